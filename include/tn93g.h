@@ -1,0 +1,129 @@
+/*
+ * tn93g.h -- C ABI of the B200 all-pairs TN93 engine (libtn93g.so).
+ *
+ * The reference (swifttn93, a drop-in for tn93 v1.1.0) has no plugin or FFI layer: its pair engine is linked
+ * into main (solver/swifttn93.cpp:2299-2301) and consumes the parsed alignment (struct SeqSet,
+ * solver/swifttn93.cpp:140-147) plus the scalar options of args_t (solver/argparse.hpp:41-65). This header is
+ * that seam made explicit: the command-line front end parses options and FASTA on the host exactly as tn93
+ * does, hands the codes to the engine, and receives the distance file bytes (in row order, through a
+ * callback) and the numbers of the JSON summary. Plain pointers and sizes only; no CUDA or C++ types.
+ *
+ * Errors: every function returns TN93G_OK (0) or a negative TN93G_E* code; tn93g_strerror names it. Nothing
+ * here exits the process. Threading: one host thread uses a context at a time.
+ */
+#ifndef TN93G_H
+#define TN93G_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TN93G_OK 0
+#define TN93G_EINVAL (-1)   /* bad argument (null pointer, bad size, bad option value) */
+#define TN93G_ECUDA (-2)    /* a CUDA runtime call failed (see tn93g_last_cuda_error) */
+#define TN93G_ENOMEM (-3)   /* device or pinned host memory exhausted, or over the context's HBM budget */
+#define TN93G_ESINK (-4)    /* the output callback returned non-zero */
+#define TN93G_ENODEV (-5)   /* no usable CUDA device */
+#define TN93G_ETIMEOUT (-6) /* a bounded device wait gave up (device error word set) */
+#define TN93G_ETOOBIG (-7)  /* alignment too long for the 32-bit x16 count lanes (L >= 2^25) */
+
+/* Ambiguity modes, numbered as tn93's RESOLVE/AVERAGE/SKIP/GAPMM/SUBSET (solver/refkernel.h:14-18). */
+#define TN93G_RESOLVE 0
+#define TN93G_AVERAGE 1
+#define TN93G_SKIP 2
+#define TN93G_GAPMM 3
+#define TN93G_SUBSET 4
+
+/* Output formats, numbered as tn93's format_t (solver/argparse.hpp:25-30). */
+#define TN93G_CSV 0
+#define TN93G_CSVN 1
+#define TN93G_HYPHY 2
+
+/* Options of one run; the fields are args_t's (solver/argparse.hpp:46-63) after main's derivations
+ * (solver/swifttn93.cpp:2256-2257, 2275-2294). */
+typedef struct tn93g_opts {
+  int mode;                    /* TN93G_RESOLVE .. TN93G_SUBSET (-a) */
+  double threshold;            /* -t: a pair is reported when min_distance <= d <= threshold */
+  double min_distance;         /* -w (default -1e-10) */
+  double resolve_fraction;     /* -g (default 1.0) */
+  long min_overlap;            /* -l, as the long tn93 passes to computeTN93 */
+  int format;                  /* TN93G_CSV, TN93G_CSVN or TN93G_HYPHY (-f) */
+  char delimiter;              /* -D (default ',') */
+  int report_self;             /* -0, already combined with "one input file and not -c" */
+  int count_only;              /* -c: no pair lines, only counts */
+  int do_fst;                  /* -m with a second file: all pairs over both files, three histograms */
+  unsigned char subset[18];    /* -a LIST: codes (index in "ACGTURYSWKMBDHVN?-") resolved under SUBSET */
+} tn93g_opts;
+
+/* Receives the distance file in order, in chunks (the header line is the caller's). The bytes are valid only
+ * during the call. Return 0 to continue, non-zero to abort the run with TN93G_ESINK. */
+typedef int (*tn93g_sink)(void *user, const char *bytes, size_t n);
+
+/* The numbers of tn93's JSON summary (solver/swifttn93.cpp:2327-2330, 2914-2958). mean[] and weighted[] are
+ * the row-ordered sums, not yet divided; the caller prints them with tn93's own iostream statements. */
+typedef struct tn93g_summary {
+  unsigned long pairwise;         /* Total comparisons possible */
+  long skipped;                   /* pairs below the overlap (-l) */
+  long links;                     /* weighted count of reported pairs */
+  double max[3], mean[3], weighted[3];
+  unsigned long hist[3][200];
+  /* engine counters */
+  long pairs_replayed;            /* pairs that took the site-order (non-dyadic) path */
+  long logs_ambiguous;            /* pairs with a logarithm inside the C library's rounding band */
+  long undecided;                 /* of those, pairs whose printed bytes or decisions depend on the band */
+  size_t output_bytes;
+} tn93g_summary;
+
+typedef struct tn93g_ctx tn93g_ctx;
+typedef struct tn93g_set tn93g_set;
+
+/* Creates a context on CUDA device `device`. hbm_budget (bytes, 0 = no limit) caps the engine's device
+ * allocations. Replaces: Engine construction and its buffers (solver/swifttn93.cpp:490-569). */
+int tn93g_create(tn93g_ctx **out, int device, size_t hbm_budget);
+void tn93g_destroy(tn93g_ctx *ctx);
+const char *tn93g_strerror(int code);
+/* the message of the last failed CUDA call in this context */
+const char *tn93g_last_cuda_error(tn93g_ctx *ctx);
+
+/* Uploads an alignment: N sequences of L codes (0..17, the index of the character in "ACGTURYSWKMBDHVN?-",
+ * as read_fasta produces them, solver/swifttn93.cpp:292-406), row-major; copy numbers (>= 1, or as tn93
+ * parsed them); names as one byte buffer with per-sequence offsets and lengths (not NUL-terminated).
+ * The caller keeps ownership of its buffers; they may be freed when the call returns.
+ * Replaces: the SeqSet handed to Engine::prepare (solver/swifttn93.cpp:140-147, 2300). */
+int tn93g_upload(tn93g_ctx *ctx, tn93g_set **out, const uint8_t *codes, long N, long L, const long *copy_counts,
+                 const char *names, const size_t *name_off, const long *name_len);
+void tn93g_free_set(tn93g_ctx *ctx, tn93g_set *set);
+
+/* All pairs of one uploaded set. n1 = number of sequences that came from the first file (n1 = N for one file).
+ * When n1 < N and !opts->do_fst, only the cross pairs (rows 0..n1-1 against columns n1..N-1) are computed,
+ * as tn93's -s mode does (solver/swifttn93.cpp:2321-2322, 2392). The distance file (after the header line)
+ * is delivered to sink in order; the summary is written to *out.
+ * Replaces: the pair loop, its reductions and writer (solver/swifttn93.cpp:2339-2866). */
+int tn93g_run(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_opts *opts, tn93g_sink sink, void *user,
+              tn93g_summary *out);
+
+/* The same run with the distance file left in device memory instead of being copied to the host: *dev_out
+ * (device pointer owned by the context, valid until the next run or tn93g_destroy) receives *nbytes bytes.
+ * For consumers that post-process on the GPU, and to time the engine with its inputs and outputs in HBM. */
+int tn93g_run_to_device(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_opts *opts, void **dev_out,
+                        size_t *nbytes, tn93g_summary *out);
+
+/* The context's CUDA stream (a cudaStream_t), on which every kernel and copy of a run is issued. */
+void *tn93g_stream(tn93g_ctx *ctx);
+
+/* Number of kernel launches of the last run. */
+long tn93g_last_launches(tn93g_ctx *ctx);
+
+/* Device time of the last run's stages in milliseconds (CUDA events on the engine's stream):
+ * [0] pack, [1] pair kernel, [2] site-order replay, [3] row reductions, [4] output formatting,
+ * [5] device->host copies, [6] whole run. Returns the number of entries written (<= n). */
+int tn93g_last_timings(tn93g_ctx *ctx, double *ms, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TN93G_H */

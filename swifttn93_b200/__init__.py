@@ -1,0 +1,245 @@
+"""swifttn93_b200 -- all-pairs TN93 distances on NVIDIA B200, byte-exact with tn93 v1.1.0 / swifttn93.
+
+The engine is the shared library lib/libtn93g.so (sm_100a kernels behind the C ABI of include/tn93g.h); this
+module binds it with ctypes. There is no CPU fallback: importing works anywhere, but creating an Engine needs
+the built library and a CUDA device, and raises otherwise.
+
+    from swifttn93_b200 import Engine, Options
+    eng = Engine()
+    s = eng.upload(codes, names, counts)           # codes: uint8 [N, L] in 0..17 ("ACGTURYSWKMBDHVN?-")
+    out, summary = eng.run(s, Options(threshold=0.015, mode="resolve", resolve_fraction=0.05, min_overlap=500))
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libtn93g.so"
+CLI_PATH = PKG / "bin" / "tn93g"
+ALPHABET = b"ACGTURYSWKMBDHVN?-"
+
+MODES = {"resolve": 0, "average": 1, "skip": 2, "gapmm": 3, "subset": 4}
+FORMATS = {"csv": 0, "csvn": 1, "hyphy": 2}
+
+# symbols declared in include/tn93g.h
+EXPORTS = ("tn93g_create", "tn93g_destroy", "tn93g_strerror", "tn93g_last_cuda_error", "tn93g_upload",
+           "tn93g_free_set", "tn93g_run", "tn93g_run_to_device", "tn93g_stream", "tn93g_last_launches",
+           "tn93g_last_timings")
+
+
+class _Opts(C.Structure):
+    _fields_ = [("mode", C.c_int), ("threshold", C.c_double), ("min_distance", C.c_double),
+                ("resolve_fraction", C.c_double), ("min_overlap", C.c_long), ("format", C.c_int),
+                ("delimiter", C.c_char), ("report_self", C.c_int), ("count_only", C.c_int), ("do_fst", C.c_int),
+                ("subset", C.c_ubyte * 18)]
+
+
+class _Summary(C.Structure):
+    _fields_ = [("pairwise", C.c_ulong), ("skipped", C.c_long), ("links", C.c_long), ("max", C.c_double * 3),
+                ("mean", C.c_double * 3), ("weighted", C.c_double * 3), ("hist", (C.c_ulong * 200) * 3),
+                ("pairs_replayed", C.c_long), ("logs_ambiguous", C.c_long), ("undecided", C.c_long),
+                ("output_bytes", C.c_size_t)]
+
+
+_SINK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_char), C.c_size_t)
+
+_lib = None
+
+
+def load_library(path: Path | str = LIB_PATH):
+    """Loads libtn93g.so (raises if it was not built: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path)
+    if not p.exists():
+        raise RuntimeError(f"{p} is missing: build it with `python -m swifttn93_b200.build`")
+    lib = C.CDLL(str(p))
+    lib.tn93g_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_size_t]
+    lib.tn93g_destroy.argtypes = [C.c_void_p]
+    lib.tn93g_strerror.restype = C.c_char_p
+    lib.tn93g_strerror.argtypes = [C.c_int]
+    lib.tn93g_last_cuda_error.restype = C.c_char_p
+    lib.tn93g_last_cuda_error.argtypes = [C.c_void_p]
+    lib.tn93g_upload.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_void_p, C.c_long, C.c_long, C.c_void_p,
+                                 C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.tn93g_free_set.argtypes = [C.c_void_p, C.c_void_p]
+    lib.tn93g_run.argtypes = [C.c_void_p, C.c_void_p, C.c_long, C.POINTER(_Opts), _SINK, C.c_void_p,
+                              C.POINTER(_Summary)]
+    lib.tn93g_last_timings.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int]
+    lib.tn93g_run_to_device.argtypes = [C.c_void_p, C.c_void_p, C.c_long, C.POINTER(_Opts), C.POINTER(C.c_void_p),
+                                        C.POINTER(C.c_size_t), C.POINTER(_Summary)]
+    lib.tn93g_stream.restype = C.c_void_p
+    lib.tn93g_stream.argtypes = [C.c_void_p]
+    lib.tn93g_last_launches.restype = C.c_long
+    lib.tn93g_last_launches.argtypes = [C.c_void_p]
+    _lib = lib
+    return lib
+
+
+@dataclass
+class Options:
+    """tn93's options for one run (the -t -w -a -g -l -f -D -0 -c -m flags)."""
+    threshold: float = 0.015
+    min_distance: float = -1.e-10
+    mode: str = "resolve"        # resolve | average | skip | gapmm | an ambiguity list such as "RY"
+    resolve_fraction: float = 1.0
+    min_overlap: int = 100
+    format: str = "csv"
+    delimiter: str = ","
+    report_self: bool = False
+    count_only: bool = False
+    do_fst: bool = False
+
+    def to_c(self) -> _Opts:
+        o = _Opts()
+        if self.mode in MODES:
+            o.mode = MODES[self.mode]
+        else:
+            o.mode = MODES["subset"]
+            for ch in self.mode.upper().encode():
+                k = ALPHABET.find(bytes([ch]))
+                if k > 3:
+                    o.subset[k] = 1
+        o.threshold = self.threshold
+        o.min_distance = self.min_distance
+        o.resolve_fraction = self.resolve_fraction
+        o.min_overlap = int(self.min_overlap)
+        o.format = FORMATS[self.format]
+        o.delimiter = self.delimiter.encode()[:1]
+        o.report_self = int(self.report_self)
+        o.count_only = int(self.count_only)
+        o.do_fst = int(self.do_fst)
+        return o
+
+
+@dataclass
+class Summary:
+    pairwise: int
+    skipped: int
+    links: int
+    max: list
+    mean: list
+    weighted: list
+    hist: np.ndarray
+    pairs_replayed: int
+    logs_ambiguous: int
+    undecided: int
+    output_bytes: int
+    timings_ms: dict = field(default_factory=dict)
+
+
+class Tn93Error(RuntimeError):
+    pass
+
+
+@dataclass
+class DeviceSet:
+    """An alignment resident on the device (tn93g_upload)."""
+    handle: C.c_void_p
+    N: int
+    L: int
+
+
+class Engine:
+    """One engine context on a CUDA device (tn93g_create)."""
+
+    STAGES = ("pack", "pair", "replay", "rows", "write", "d2h", "total")
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        self.lib = load_library()
+        self.ctx = C.c_void_p()
+        self._check(self.lib.tn93g_create(C.byref(self.ctx), device, hbm_budget))
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = self.lib.tn93g_strerror(rc).decode()
+            if getattr(self, "ctx", None):
+                msg += ": " + (self.lib.tn93g_last_cuda_error(self.ctx) or b"").decode()
+            raise Tn93Error(f"tn93g error {rc}: {msg}")
+
+    def upload(self, codes: np.ndarray, names, counts=None):
+        codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        N, L = codes.shape
+        nb = [n.encode() if isinstance(n, str) else bytes(n) for n in names]
+        blob = b"".join(nb) or b"\0"
+        off = np.zeros(N, dtype=np.uint64)
+        if N > 1:
+            off[1:] = np.cumsum([len(b) for b in nb[:-1]])
+        ln = np.array([len(b) for b in nb], dtype=np.int64)
+        cnt = np.ones(N, dtype=np.int64) if counts is None else np.ascontiguousarray(counts, dtype=np.int64)
+        s = C.c_void_p()
+        self._check(self.lib.tn93g_upload(self.ctx, C.byref(s), codes.ctypes.data, N, L, cnt.ctypes.data, blob,
+                                          off.ctypes.data, ln.ctypes.data))
+        return DeviceSet(s, N, L)
+
+    def free(self, s: DeviceSet):
+        self.lib.tn93g_free_set(self.ctx, s.handle)
+        s.handle = C.c_void_p()
+
+    def run(self, s: DeviceSet, opts: Options, n1: int | None = None, sink=None):
+        """Runs all pairs of set s. sink(bytes-like memoryview) receives the distance file in order; when sink is
+        None the bytes are collected and returned."""
+        chunks = []
+
+        def _sink(_user, ptr, n):
+            try:
+                mv = C.string_at(ptr, n)
+                if sink is None:
+                    chunks.append(mv)
+                else:
+                    sink(mv)
+                return 0
+            except Exception:  # noqa: BLE001 - an exception must not unwind through C
+                return 1
+
+        cb = _SINK(_sink)
+        o = opts.to_c()
+        S = _Summary()
+        if n1 is None:
+            n1 = s.N
+        self._check(self.lib.tn93g_run(self.ctx, s.handle, int(n1), C.byref(o), cb, None, C.byref(S)))
+        return b"".join(chunks), self._summary(S)
+
+    def run_to_device(self, s: DeviceSet, opts: Options, n1: int | None = None):
+        """Runs all pairs with the distance file left in HBM; returns (device pointer, nbytes, Summary)."""
+        o = opts.to_c()
+        S = _Summary()
+        ptr, nb = C.c_void_p(), C.c_size_t()
+        self._check(self.lib.tn93g_run_to_device(self.ctx, s.handle, int(s.N if n1 is None else n1), C.byref(o),
+                                                 C.byref(ptr), C.byref(nb), C.byref(S)))
+        return ptr.value, nb.value, self._summary(S)
+
+    @property
+    def stream(self) -> int:
+        """The engine's cudaStream_t, as an integer (for torch.cuda.ExternalStream)."""
+        return self.lib.tn93g_stream(self.ctx) or 0
+
+    def last_launches(self) -> int:
+        return self.lib.tn93g_last_launches(self.ctx)
+
+    def _summary(self, S):
+        t = (C.c_double * 7)()
+        k = self.lib.tn93g_last_timings(self.ctx, t, 7)
+        summ = Summary(pairwise=S.pairwise, skipped=S.skipped, links=S.links, max=list(S.max), mean=list(S.mean),
+                       weighted=list(S.weighted), hist=np.array([[S.hist[q][k2] for k2 in range(200)]
+                                                                 for q in range(3)], dtype=np.uint64),
+                       pairs_replayed=S.pairs_replayed, logs_ambiguous=S.logs_ambiguous, undecided=S.undecided,
+                       output_bytes=S.output_bytes,
+                       timings_ms={self.STAGES[q]: t[q] for q in range(k)})
+        return summ
+
+    def close(self):
+        if self.ctx:
+            self.lib.tn93g_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass

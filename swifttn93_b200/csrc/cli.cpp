@@ -1,0 +1,439 @@
+// cli.cpp -- the tn93 v1.1.0 command line on top of the B200 engine (libtn93g.so).
+//
+// Host side, as in the reference: option parsing with tn93's semantics and messages (argparse.cpp:20-446),
+// the FASTA reader's acceptance rules and error messages (swifttn93.cpp:259-406), the unsupported-option
+// guard (swifttn93.cpp:2226-2233), the header line (swifttn93.cpp:2307-2316) and the JSON summary printed
+// with the same iostream statements as tn93 (swifttn93.cpp:2900-2963), so the bytes on stdout match. The
+// pair engine, its reductions and the distance-file text run on the GPU through include/tn93g.h.
+#include <ctype.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <iomanip>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "tn93g.h"
+
+namespace {
+
+const char kValid[] = "ACGTURYSWKMBDHVN?-";
+
+const char kUsage[] =
+    "usage: tn93 [-h] [-v] [-o OUTPUT] [-t THRESHOLD] [-w MIN_THRESHOLD] [-a AMBIGS] [-g FRACTION] [-l OVERLAP] "
+    "[-d COUNTS_IN_NAME] [-f FORMAT] [-s SECOND_FASTA] [-b] [-r] [-c] [-n] [-0] [-q] [-H] [-S] [-D DELIMITER][FASTA]\n";
+
+struct Options {
+  FILE *out = stdout, *in1 = stdin, *in2 = nullptr;
+  double distance = 0.015, min_distance = -1.e-10, resolve_fraction = 1.0, include_prob = 1.0;
+  int ambig = TN93G_RESOLVE, format = TN93G_CSV;
+  unsigned long overlap = 100;
+  bool bootstrap = false, bootstrap2 = false, count = false, quiet = false, fst = false, no_header = false,
+       report_self = false, hamming = false;
+  char counts_sep = ':', delimiter = ',';
+  std::string subset;
+};
+
+[[noreturn]] void fail(const char *fmt, ...)
+{
+  va_list ap;
+  fprintf(stderr, "%stn93: error: ", kUsage);
+  va_start(ap, fmt);
+  vfprintf(stderr, fmt, ap);
+  va_end(ap);
+  fprintf(stderr, "\n");
+  exit(1);
+}
+
+// tn93's parser: options are matched on their second character, every non-option argument but the last is
+// an error, and the last one is the input FASTA (argparse.cpp:138-226)
+Options parse(int argc, char **argv)
+{
+  Options o;
+  auto value = [&](int &i) -> const char * {
+    if (++i == argc) fail("ran out of command line arguments");
+    return argv[i];
+  };
+  auto open_in = [&](const char *v, const char *what) -> FILE * {
+    FILE *f = strcmp(v, "-") ? fopen(v, "rb") : stdin;
+    if (!f) fail("failed to open the %s %s", what, v);
+    return f;
+  };
+  for (int i = 1; i < argc; i++) {
+    const char *a = argv[i];
+    if (a[0] == '-' && a[1] == '-') {
+      const char *l = a + 2;
+      if (!strcmp(l, "help")) {
+        fprintf(stderr, "%s\n", kUsage);
+        exit(1);
+      } else if (!strcmp(l, "version")) {
+        fprintf(stderr, "v1.1.0\n");
+        exit(0);
+      } else if (!strcmp(l, "hamming-skip"))
+        o.hamming = true;
+      else if (strcmp(l, "subquadratic"))
+        fail("unknown argument: %s", a);
+      continue;
+    }
+    if (a[0] != '-') {
+      if (i != argc - 1) fail("unknown argument: %s", a);
+      o.in1 = open_in(a, "INPUT file");
+      if (o.in1 == o.in2) fail("input FASTA files must not both be stdin %s", a);
+      continue;
+    }
+    const char *v;
+    switch (a[1]) {
+      case 'h':
+        if (a[2]) fail("unknown argument: %s", a);
+        fprintf(stderr, "%s\n", kUsage);
+        exit(1);
+      case 'v': fprintf(stderr, "v1.1.0\n"); exit(0);
+      case 'o':
+        v = value(i);
+        o.out = strcmp(v, "-") ? fopen(v, "wb") : stdout;
+        if (!o.out) fail("failed to open the OUTPUT file %s", v);
+        break;
+      case 't':
+        v = value(i);
+        o.distance = atof(v);
+        if (o.distance < 0.0) fail("genetic distance threshold must be >= 0, had: %s", v);
+        break;
+      case 'w':
+        v = value(i);
+        o.min_distance = atof(v);
+        if (o.min_distance < 0.0 || o.min_distance > 1.0) fail("genetic minimum distance threshold must be >= 0, had: %s", v);
+        break;
+      case 'l':
+        v = value(i);
+        o.overlap = (unsigned long)(long)atoi(v);
+        if (o.overlap == 0) fail("overlap must be positive, had: %s", v);
+        break;
+      case 'f':
+        v = value(i);
+        if (!strcmp(v, "csv"))
+          o.format = TN93G_CSV;
+        else if (!strcmp(v, "csvn"))
+          o.format = TN93G_CSVN;
+        else if (!strcmp(v, "hyphy"))
+          o.format = TN93G_HYPHY;
+        else
+          fail("invalid output format: %s", v);
+        break;
+      case 'a':
+        v = value(i);
+        if (!strcmp(v, "resolve"))
+          o.ambig = TN93G_RESOLVE;
+        else if (!strcmp(v, "average"))
+          o.ambig = TN93G_AVERAGE;
+        else if (!strcmp(v, "skip"))
+          o.ambig = TN93G_SKIP;
+        else if (!strcmp(v, "gapmm"))
+          o.ambig = TN93G_GAPMM;
+        else {
+          o.ambig = TN93G_SUBSET;
+          o.subset = v;
+        }
+        break;
+      case 's':
+        v = value(i);
+        o.in2 = open_in(v, "second INPUT file");
+        if (o.in1 == o.in2) fail("input FASTA files must not both be stdin %s", v);
+        break;
+      case 'd':
+        v = value(i);
+        o.counts_sep = v[0];
+        if (!isprint((unsigned char)o.counts_sep)) fail("count separator must be a printable character, had: %s", v);
+        break;
+      case 'u':
+        v = value(i);
+        o.include_prob = atof(v);
+        if (o.include_prob < 0.0 || o.include_prob > 1.0) fail("sequence inclusion probability must be >= 0, had: %s", v);
+        break;
+      case 'D':
+        v = value(i);
+        if (strlen(v) != 1) fail("invalid output format: %s", v);
+        o.delimiter = v[0];
+        break;
+      case 'b': o.bootstrap = true; break;
+      case 'r': o.bootstrap2 = true; break;
+      case 'c': o.count = true; break;
+      case 'n': o.no_header = true; break;
+      case 'q': o.quiet = true; break;
+      case 'H': o.hamming = true; break;
+      case 'S': break;
+      case 'm': o.fst = true; break;
+      case '0': o.report_self = true; break;
+      case 'g':
+        v = value(i);
+        o.resolve_fraction = atof(v);
+        if (o.resolve_fraction < 0.0 || o.resolve_fraction > 1.0) fail("resolve ambigous fraction must be >= 0, had: %s", v);
+        break;
+      default: fail("unknown argument: %s", a);
+    }
+  }
+  return o;
+}
+
+// parsed alignment: codes 0..17 row-major, names, copy numbers
+struct Alignment {
+  std::vector<uint8_t> codes;
+  std::vector<char> names;
+  std::vector<size_t> name_off;
+  std::vector<long> name_len, counts;
+  long N = 0;
+};
+
+signed char g_code[256];  // code of toupper(byte), -1 for bytes the reader drops
+
+// The reader's rules (swifttn93.cpp:292-406): '>' or '#' opens a record whose name runs to the end of the
+// line; sequence bytes map through the alphabet case-insensitively, other bytes are dropped; every sequence
+// must have the first one's length. Returns false after printing tn93's message for a reader error; exits
+// with status 1 where tn93 exits.
+bool read_fasta(FILE *F, Alignment &A, long &first_len, char sep)
+{
+  std::vector<unsigned char> buf;
+  {
+    unsigned char tmp[1 << 16];
+    size_t r;
+    while ((r = fread(tmp, 1, sizeof tmp, F)) > 0) buf.insert(buf.end(), tmp, tmp + r);
+  }
+  const unsigned char *p = buf.data(), *end = p + buf.size();
+  int state = 0;
+  size_t seq_begin = A.codes.size();
+  auto close_sequence = [&]() {
+    const long len = (long)(A.codes.size() - seq_begin);
+    if (A.N == 0) {
+      first_len = len;
+      if (first_len <= 0) {
+        std::cerr << "First sequence length must be positive." << std::endl;
+        exit(1);
+      }
+    } else if (len != first_len) {
+      std::cerr << "All sequences must have the same length (" << first_len << "), but sequence '"
+                << (A.names.data() + A.name_off.back()) << "' had length " << len;
+      exit(1);
+    }
+    A.N++;
+  };
+  while (p < end) {
+    if (state == 0) {
+      while (p < end && *p != '>' && *p != '#') p++;
+      if (p == end) break;
+      p++;
+      state = 1;
+      continue;
+    }
+    if (state == 1) {
+      const unsigned char *q = p;
+      while (q < end && *q != '\n' && *q != '\r') q++;
+      const size_t begin = A.names.size();
+      A.names.insert(A.names.end(), p, q);
+      if (q == end) {
+        p = q;
+        break;
+      }
+      p = q + 1;
+      const long len = (long)(A.names.size() - begin);
+      A.names.push_back('\0');
+      if (len <= 0) {
+        std::cerr << "Sequence names must be non-empty." << std::endl;
+        return false;
+      }
+      // copy number after the last separator that is neither the name's first nor its last character
+      unsigned long count = 1;
+      if (len >= 3) {
+        const char *nm = A.names.data() + begin;
+        long k = len - 2;
+        while (k >= 1 && nm[k] != sep) k--;
+        if (k >= 1) count = (unsigned long)(long)(int)strtol(nm + k + 1, nullptr, 10);
+        if (count < 1) count = 1;
+      }
+      A.counts.push_back((long)count);
+      A.name_off.push_back(begin);
+      A.name_len.push_back(len);
+      state = 2;
+      seq_begin = A.codes.size();
+      continue;
+    }
+    while (p < end) {
+      const signed char v = g_code[*p];
+      if (v >= 0) {
+        A.codes.push_back((uint8_t)v);
+        p++;
+        continue;
+      }
+      if (*p == '>' || *p == '#') break;
+      p++;
+    }
+    if (p == end) break;
+    p++;
+    close_sequence();
+    state = 1;
+  }
+  if (state == 2) {
+    close_sequence();
+    return true;
+  }
+  std::cerr << "Unexpected end of file: state " << state << std::endl;
+  return false;
+}
+
+void dump_histogram(std::ostream *o, const char *tag, const unsigned long *hist)
+{
+  if (tag)
+    (*o) << "\t\"Histogram " << tag << "\" : [";
+  else
+    (*o) << "\t\"Histogram\" : [";
+  for (unsigned long k = 0; k < 200; k++) {
+    if (k) (*o) << ',';
+    (*o) << '[' << (k + 1.) / 200 << ',' << hist[k] << ']';
+  }
+  (*o) << "]" << std::endl;
+}
+
+int write_sink(void *user, const char *bytes, size_t n)
+{
+  FILE *f = (FILE *)user;
+  return fwrite(bytes, 1, n, f) == n ? 0 : 1;
+}
+
+}  // namespace
+
+int main(int argc, char **argv)
+{
+  Options o = parse(argc, argv);
+  if (o.bootstrap || o.bootstrap2 || o.include_prob < 1.) {
+    std::cerr << "swifttn93: -b, -r and -u (random resampling) are not supported" << std::endl;
+    return 1;
+  }
+  if (o.hamming) {
+    std::cerr << "swifttn93: -H (Hamming early exit) is not supported" << std::endl;
+    return 1;
+  }
+  for (int c = 0; c < 256; c++) g_code[c] = -1;
+  for (int c = 0; c < 256; c++) {
+    const char *f = strchr(kValid, toupper(c));
+    if (f && toupper(c)) g_code[c] = (signed char)(f - kValid);
+  }
+  unsigned char subset[18] = {0};
+  for (unsigned char ch : o.subset) {
+    const char *f = strchr(kValid, toupper(ch));
+    if (f && toupper(ch) && f - kValid > 3) subset[f - kValid] = 1;
+  }
+  Alignment A;
+  long L = 0;
+  if (!read_fasta(o.in1, A, L, o.counts_sep)) return 1;
+  const unsigned long n1 = (unsigned long)A.N;
+  unsigned long n2 = 0;
+  if (o.in2) {
+    if (!read_fasta(o.in2, A, L, o.counts_sep)) return 1;
+    n2 = (unsigned long)A.N - n1;
+  }
+  const bool fst = o.in2 && o.fst;
+  const bool report_self = !o.in2 && o.report_self && !o.count;
+  const unsigned long N = (unsigned long)A.N;
+  const unsigned long pairwise = (o.in2 && !fst) ? n2 * n1 : (N - 1) * N / 2;
+  if (!o.quiet) {
+    if (!o.in2)
+      std::cerr << "Read " << N << " sequences of length " << L << std::endl
+                << "Will perform " << pairwise << " pairwise distance calculations";
+    else {
+      std::cerr << "Read " << n1 << " sequences from file 1 and " << n2 << " sequences from file 2 of length " << L
+                << std::endl
+                << "Will perform " << pairwise << " pairwise distance calculations";
+      if (fst) std::cerr << ". Running in F_ST mode";
+    }
+  }
+  if (o.format != TN93G_HYPHY && !o.count && !o.no_header) {
+    if (o.format == TN93G_CSV)
+      fprintf(o.out, "ID1%cID2%cDistance\n", o.delimiter, o.delimiter);
+    else
+      fprintf(o.out, "Seq1%cSeq2%cDistance\n", o.delimiter, o.delimiter);
+  }
+  tn93g_ctx *ctx = nullptr;
+  int rc = tn93g_create(&ctx, 0, 0);
+  if (rc != TN93G_OK) {
+    std::cerr << "tn93g: " << tn93g_strerror(rc) << std::endl;
+    return 2;
+  }
+  tn93g_set *set = nullptr;
+  if (A.names.empty()) A.names.push_back('\0');
+  rc = tn93g_upload(ctx, &set, A.codes.data(), A.N, L, A.counts.data(), A.names.data(), A.name_off.data(),
+                    A.name_len.data());
+  if (rc != TN93G_OK) {
+    std::cerr << "tn93g: " << tn93g_strerror(rc) << " " << tn93g_last_cuda_error(ctx) << std::endl;
+    return 2;
+  }
+  tn93g_opts op;
+  memset(&op, 0, sizeof op);
+  op.mode = o.ambig;
+  op.threshold = o.distance;
+  op.min_distance = o.min_distance;
+  op.resolve_fraction = o.resolve_fraction;
+  op.min_overlap = (long)o.overlap;
+  op.format = o.format;
+  op.delimiter = o.delimiter;
+  op.report_self = report_self;
+  op.count_only = o.count;
+  op.do_fst = fst;
+  memcpy(op.subset, subset, sizeof subset);
+  tn93g_summary S;
+  rc = tn93g_run(ctx, set, (long)n1, &op, write_sink, o.out, &S);
+  if (rc != TN93G_OK) {
+    std::cerr << "tn93g: " << tn93g_strerror(rc) << " " << tn93g_last_cuda_error(ctx) << std::endl;
+    return 2;
+  }
+  if (getenv("TN93G_STATS"))
+    fprintf(stderr, "tn93g: replayed %ld, ambiguous-log pairs %ld, undecided %ld\n", S.pairs_replayed,
+            S.logs_ambiguous, S.undecided);
+  tn93g_free_set(ctx, set);
+  tn93g_destroy(ctx);
+  fflush(o.out);
+  if (!o.quiet)
+    std::cerr << std::endl << "Progress:" << std::setw(8) << 100. << "% (" << std::setw(8) << S.links
+              << " links found, " << std::setw(12) << std::setprecision(3) << (double)pairwise << " evals)";
+  std::cerr << std::endl;
+  std::ostream *os = o.out == stdout ? &std::cerr : &std::cout;
+  // tn93's summary statements (swifttn93.cpp:2914-2958)
+  (*os) << "{" << std::endl;
+  (*os) << '\t' << "\"Actual comparisons performed\" :" << pairwise - S.skipped << ',' << std::endl;
+  (*os) << "\t\"Comparisons accounting for copy numbers \" :" << (S.weighted[0] + S.weighted[1] + S.weighted[2]) << ','
+        << std::endl;
+  (*os) << "\t\"Total comparisons possible\" : " << pairwise << ',' << std::endl;
+  (*os) << "\t\"Links found\" : " << S.links << ',' << std::endl;
+  (*os) << "\t\"Maximum distance\" : " << S.max[0] << ',' << std::endl;
+  if (!o.in2) {
+    (*os) << "\t\"Sequences\" : " << N << ',' << std::endl;
+  } else {
+    (*os) << "\t\"Sequences in first file\" : " << n1 << ',' << std::endl;
+    (*os) << "\t\"Sequences in second file\" : " << n2 << ',' << std::endl;
+  }
+  if (fst) {
+    const char *keys[4] = {"File 1", "File 2", "Between", "Combined"};
+    for (int k = 0; k < 3; k++)
+      (*os) << "\t\"Mean distance " << keys[k] << "\" : " << S.mean[k] / S.weighted[k] << ',' << std::endl;
+    const double meta = (S.mean[0] + S.mean[1] + S.mean[2]) / (S.weighted[0] + S.weighted[1] + S.weighted[2]),
+                 intra = (S.mean[0] + S.mean[1]) / (S.weighted[0] + S.weighted[1]),
+                 piD = S.mean[2] / S.weighted[2] - intra;
+    (*os) << "\t\"Mean distance [intra] " << "\" : " << intra << ',' << std::endl;
+    (*os) << "\t\"Mean distance [combined]" << "\" : " << meta << ',' << std::endl;
+    (*os) << "\t\"F_ST\" : " << piD / (intra + piD) << ',' << std::endl;
+    for (int k = 0; k < 3; k++) {
+      dump_histogram(os, keys[k], S.hist[k]);
+      (*os) << ',' << std::endl;
+    }
+    for (int k = 0; k < 200; k++) S.hist[0][k] += S.hist[1][k] + S.hist[2][k];
+    dump_histogram(os, keys[3], S.hist[0]);
+  } else {
+    (*os) << "\t\"Mean distance\" : " << S.mean[0] / S.weighted[0] << ',' << std::endl;
+    dump_histogram(os, nullptr, S.hist[0]);
+  }
+  (*os) << '}' << std::endl;
+  if (o.count)
+    fprintf(o.out, "Found %ld links among %ld pairwise comparisons\n", S.links, (long)(pairwise - S.skipped));
+  if (o.out != stdout) fclose(o.out);
+  return 0;
+}

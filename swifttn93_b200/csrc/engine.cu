@@ -1,0 +1,1332 @@
+// engine.cu -- sm_100a kernels of the all-pairs TN93 engine and the C ABI of include/tn93g.h.
+//
+// One run (tn93g_run) is a pipeline over bands of rows:
+//   pack      colscan_kernel, pack_kernel, events_kernel, transpose_kernel: constant-column fold, bit planes,
+//             compressed codes and sparse event lists (replaces Engine::prepare, swifttn93.cpp:570-1044)
+//   pair      pair_kernel: per pair the clean-site counts by AND/XOR + POPC over 64-column plane words, the
+//             N-plane cross counts, the sparse ambiguity events through the x16 tables, tn93's -l / -g
+//             decisions, the TN93 formula in FP64 and the log certificate; writes the raw distance
+//             (replaces kernel8/kernel16/kernelW/sparse_*/phaseA/tail8, swifttn93.cpp:1241-2170)
+//   replay    replay_kernel: pairs with a contribution that is not a multiple of 1/16 are recomputed by a
+//             site-order walk with tn93's float sums (replaces replay/ordered, swifttn93.cpp:1050-1232)
+//   rows      rows_kernel: per row, in column order: histogram, links, skipped pairs, the FP64 row sums in
+//             tn93's order, and the byte length of the row's output (phase C, swifttn93.cpp:2479-2604)
+//   write     write_kernel: the distance-file text of the band at scanned row offsets (the ordered writer,
+//             swifttn93.cpp:2811-2858, and fastfmt)
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+#include "tn93g.h"
+
+namespace tn93 {
+void build_log_table(LogTable *T);
+}
+
+using namespace tn93;
+
+namespace {
+
+constexpr int kWarps = 8;  // warps per block of the pair / row kernels
+
+__device__ __forceinline__ int popc(uint64_t x) { return __popcll(x); }
+__device__ __forceinline__ unsigned lanemask_lt() { return (1u << (threadIdx.x & 31)) - 1u; }
+
+__device__ __forceinline__ bool sparse_code(int c, bool wplane) { return c >= 4 && c < 17 && !(wplane && c == 15); }
+
+//------------------------------------------------------------------------------------------------ pack
+// per column: the set of codes seen (bit c), per launch the number of N codes
+__global__ void colscan_kernel(const uint8_t *__restrict__ codes, long N, long L, uint32_t *seen,
+                               unsigned long long *nN)
+{
+  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long i0 = blockIdx.y * 64l, i1 = min(N, i0 + 64);
+  uint32_t m = 0;
+  unsigned cn = 0;
+  if (p < L)
+    for (long i = i0; i < i1; i++) {
+      const unsigned c = codes[i * L + p];
+      m |= 1u << c;
+      cn += c == 15;
+    }
+  if (p < L && m) atomicOr(&seen[p], m);
+  for (int o = 16; o; o >>= 1) cn += __shfl_xor_sync(0xffffffffu, cn, o);
+  if ((threadIdx.x & 31) == 0 && cn) atomicAdd(nN, (unsigned long long)cn);
+}
+
+// one warp per (sequence, 64-column word): bit planes, compressed codes, sparse event counts
+__global__ void pack_kernel(PackArgs a)
+{
+  const int lane = threadIdx.x & 31;
+  const long i = blockIdx.y * (long)kWarps + (threadIdx.x >> 5);
+  const long w = blockIdx.x;
+  if (i >= a.N) return;
+  const long k0 = w * 64 + lane, k1 = k0 + 32;
+  const int c0 = k0 < a.Lc ? a.codes[i * a.L + a.varcol[k0]] : 17;
+  const int c1 = k1 < a.Lc ? a.codes[i * a.L + a.varcol[k1]] : 17;
+  if (k0 < a.Lc) a.cc[i * a.Lc + k0] = (uint8_t)c0;
+  if (k1 < a.Lc) a.cc[i * a.Lc + k1] = (uint8_t)c1;
+  auto both = [&](bool p0, bool p1) -> uint64_t {
+    return (uint64_t)__ballot_sync(0xffffffffu, p0) | ((uint64_t)__ballot_sync(0xffffffffu, p1) << 32);
+  };
+  const uint64_t clean = both(c0 < 4, c1 < 4);
+  const uint64_t hi = both(c0 < 4 && (c0 & 1), c1 < 4 && (c1 & 1));
+  const uint64_t lo = both(c0 < 4 && (c0 & 2), c1 < 4 && (c1 & 2));
+  const bool g0 = k0 < a.Lc && c0 == 17, g1 = k1 < a.Lc && c1 == 17;
+  const uint64_t wn = a.wplane ? both(c0 == 15 || (a.gapmm && g0), c1 == 15 || (a.gapmm && g1)) : 0;
+  const uint64_t gp = a.gapmm ? both(g0, g1) : 0;
+  const uint64_t sp = both(sparse_code(c0, a.wplane), sparse_code(c1, a.wplane));
+  if (lane == 0) {
+    uint64_t *P = a.planes + (size_t)w * a.NP * a.Npad + i;
+    P[0] = hi;
+    P[a.Npad] = lo;
+    P[2 * a.Npad] = clean;
+    P[3 * a.Npad] = wn;
+    if (a.NP > 4) P[4 * a.Npad] = gp;
+    if (sp) atomicAdd(&a.evcount[i], (unsigned)popc(sp));
+  }
+}
+
+// one warp per sequence: its sparse events in site order
+__global__ void events_kernel(PackArgs a)
+{
+  const int lane = threadIdx.x & 31;
+  const long i = blockIdx.x * (long)kWarps + (threadIdx.x >> 5);
+  if (i >= a.N) return;
+  uint32_t off = a.ev_off[i];
+  const uint8_t *row = a.cc + i * a.Lc;
+  for (long w = 0; w < a.W; w++) {
+    const long k0 = w * 64 + lane, k1 = k0 + 32;
+    const int c0 = k0 < a.Lc ? row[k0] : 17, c1 = k1 < a.Lc ? row[k1] : 17;
+    const bool s0 = sparse_code(c0, a.wplane), s1 = sparse_code(c1, a.wplane);
+    const unsigned b0 = __ballot_sync(0xffffffffu, s0), b1 = __ballot_sync(0xffffffffu, s1);
+    if (s0) a.ev[off + __popc(b0 & lanemask_lt())] = ((uint32_t)k0 << 5) | (uint32_t)c0;
+    if (s1) a.ev[off + __popc(b0) + __popc(b1 & lanemask_lt())] = ((uint32_t)k1 << 5) | (uint32_t)c1;
+    off += __popc(b0) + __popc(b1);
+  }
+}
+
+// ccT[k][i] = cc[i][k] (padding sequences read as gaps)
+__global__ void transpose_kernel(const uint8_t *__restrict__ cc, uint8_t *ccT, long N, long Lc, long Npad)
+{
+  __shared__ uint8_t tile[32][33];
+  const long k0 = blockIdx.x * 32l, i0 = blockIdx.y * 32l;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int r = ty; r < 32; r += 8) {
+    const long i = i0 + r, k = k0 + tx;
+    tile[r][tx] = (i < N && k < Lc) ? cc[i * Lc + k] : (uint8_t)17;
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const long k = k0 + r, i = i0 + tx;
+    if (k < Lc && i < Npad) ccT[k * Npad + i] = tile[tx][r];
+  }
+}
+
+//------------------------------------------------------------------------------------------------ pair
+// decision-stability certificate: do the histogram bin, the link decision and the printed text agree for
+// every distance the C library's log may lead to?
+__device__ bool certified(const Dist &D, const RunConsts &rc)
+{
+  if (hist_bin(D.lo) != hist_bin(D.hi)) return false;
+  const double tlo = D.lo <= 0. ? 0. : D.lo, thi = D.hi <= 0. ? 0. : D.hi;
+  const bool llo = tlo >= rc.min_distance && tlo <= rc.threshold;
+  const bool lhi = thi >= rc.min_distance && thi <= rc.threshold;
+  if (llo != lhi) return false;
+  if (!llo && tlo < rc.min_distance && thi > rc.threshold) return false;
+  if (llo && rc.emit) {
+    char x[24], y[24];
+    const int nx = fmt_g(tlo, x), ny = fmt_g(thi, y);
+    if (nx != ny) return false;
+    for (int k = 0; k < nx; k++)
+      if (x[k] != y[k]) return false;
+  }
+  return true;
+}
+
+// formula + certificate for exact formula inputs; returns the raw distance
+__device__ double finish_distance(const LogTable &T, const RunConsts &rc, const double nf[4], double diag, double ag,
+                                  double ct, bool &amb, bool &undecided)
+{
+  const Dist D = tn93_distance(T, nf, diag, ag, ct);
+  amb = D.amb != 0;
+  undecided = amb && !certified(D, rc);
+  return D.d;
+}
+
+__device__ __forceinline__ void count_flags(unsigned long long *counters, bool amb, bool und)
+{
+  const unsigned ba = __ballot_sync(__activemask(), amb), bu = __ballot_sync(__activemask(), und);
+  const unsigned lead = __ffs(__activemask()) - 1;
+  if ((threadIdx.x & 31) == lead) {
+    if (ba) atomicAdd(&counters[0], (unsigned long long)__popc(ba));
+    if (bu) atomicAdd(&counters[1], (unsigned long long)__popc(bu));
+  }
+}
+
+// one warp = one row i against 32 consecutive columns; a block = 8 rows x 32 columns
+template <bool WPLANE, bool GAPMM>
+__global__ void __launch_bounds__(256) pair_kernel(PairArgs a)
+{
+  __shared__ AggEntry sagg[kSparseCodes * kCodes + 5];
+  for (int t = threadIdx.x; t < (kSparseCodes * kCodes + 5) * kLanes; t += blockDim.x)
+    ((int32_t *)sagg)[t] = ((const int32_t *)a.agg)[t];
+  __syncthreads();
+  const RunConsts &rc = a.rc;
+  const int lane = threadIdx.x & 31;
+  const long i = a.r0 + blockIdx.y * (long)kWarps + (threadIdx.x >> 5);
+  const long j = a.cstart + blockIdx.x * 32l + lane;
+  if (i >= a.r1) return;
+  const long lb = rc.cross ? rc.n1 : i + 1;
+  const bool valid = j >= lb && j < rc.N;
+  if (!__any_sync(0xffffffffu, valid)) return;
+  const long jj = j < rc.N ? j : rc.N - 1;
+  const long Np = rc.Npad;
+  // clean-site counts over the variable columns
+  int T = 0, MM = 0, TS = 0, CTc = 0, Y1 = 0, Y2 = 0, L1 = 0, L2 = 0, T1 = 0, T2 = 0;
+  int nWc = 0, nWh = 0, nWl = 0, nWt = 0, nWW = 0, nGG = 0;
+  const uint64_t *P = a.planes;
+  for (long w = 0; w < rc.W; w++, P += (size_t)rc.NP * Np) {
+    const uint64_t hi = __ldg(P + i), lo = __ldg(P + Np + i), ci = __ldg(P + 2 * Np + i);
+    const uint64_t hj = __ldg(P + jj), lj = __ldg(P + Np + jj), cj = __ldg(P + 2 * Np + jj);
+    const uint64_t b = ci & cj, x = hi ^ hj, y = lo ^ lj;
+    const uint64_t ts = b & ~x & y;
+    T += popc(b);
+    MM += popc(b & (x | y));
+    TS += popc(ts);
+    CTc += popc(ts & hi);
+    Y1 += popc(b & hi);
+    Y2 += popc(b & hj);
+    L1 += popc(b & lo);
+    L2 += popc(b & lj);
+    T1 += popc(b & hi & lo);
+    T2 += popc(b & hj & lj);
+    if (WPLANE) {
+      const uint64_t ni = __ldg(P + 3 * Np + i), nj = __ldg(P + 3 * Np + jj);
+      nWc += popc(ni & cj) + popc(nj & ci);
+      nWh += popc(ni & hj) + popc(nj & hi);
+      nWl += popc(ni & lj) + popc(nj & lo);
+      nWt += popc(ni & hj & lj) + popc(nj & hi & lo);
+      nWW += popc(ni & nj);
+      if (GAPMM) nGG += popc(__ldg(P + 4 * Np + i) & __ldg(P + 4 * Np + jj));
+    }
+  }
+  // sparse events: the row's (warp-uniform list, partner code from the position-major codes) ...
+  int acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const uint32_t e0 = a.ev_off[i], e1 = a.ev_off[i + 1];
+  for (uint32_t e = e0; e < e1; e++) {
+    const uint32_t v = __ldg(a.ev + e);
+    const int code = v & 31;
+    const int pc = a.ccT[(size_t)(v >> 5) * Np + jj];
+    const int32_t *t = sagg[(code - 4) * kCodes + pc].v;
+#pragma unroll
+    for (int q = 0; q < 8; q++) acc[q] += t[q];
+    acc[8] |= t[8];
+  }
+  // ... and the column's (per lane), skipping sites where the row is itself sparse (counted above)
+  const uint8_t *rowc = a.cc + (size_t)i * rc.Lc;
+  const uint32_t f0 = a.ev_off[jj], f1 = valid ? a.ev_off[jj + 1] : f0;
+  for (uint32_t e = f0; e < f1; e++) {
+    const uint32_t v = __ldg(a.ev + e);
+    const int code = v & 31;
+    const int pc = rowc[v >> 5];
+    if (sparse_code(pc, WPLANE)) continue;
+    const int32_t *t = sagg[(code - 4) * kCodes + pc].v;
+#pragma unroll
+    for (int q = 0; q < 8; q++) acc[q] += t[q];
+    acc[8] |= t[8];
+  }
+  if (!valid) return;
+  // exact x16 aggregates
+  const int D = T - MM, nfT = T1 + T2, nfC = Y1 + Y2 - nfT, nfG = L1 + L2 - nfT;
+  const int nfA = 2 * T - nfC - nfG - nfT;
+  const int base[7] = {16 * (T + (int)rc.constT), 16 * (D + (int)rc.constT), 16 * (TS - CTc), 16 * CTc,
+                       16 * (nfA + (int)rc.constNf[0]), 16 * (nfC + (int)rc.constNf[1]),
+                       16 * (nfG + (int)rc.constNf[2])};
+  int wb[4] = {0, 0, 0, 0}, nww = 0;
+  if (WPLANE) {
+    wb[3] = nWt;
+    wb[1] = nWh - nWt;
+    wb[2] = nWl - nWt;
+    wb[0] = nWc - wb[1] - wb[2] - wb[3];
+    nww = nWW - nGG;
+  }
+  const AggEntry *EW = &sagg[kSparseCodes * kCodes];
+  int ag[7];
+#pragma unroll
+  for (int q = 0; q < 7; q++) {
+    int v = base[q] + acc[q];
+    if (WPLANE) v += wb[0] * EW[0].v[q] + wb[1] * EW[1].v[q] + wb[2] * EW[2].v[q] + wb[3] * EW[3].v[q] + nww * EW[4].v[q];
+    ag[q] = v;
+  }
+  int amb = acc[7];
+  if (WPLANE) amb += wb[0] * EW[0].v[7] + wb[1] * EW[1].v[7] + wb[2] * EW[2].v[7] + wb[3] * EW[3].v[7] + nww * EW[4].v[7];
+  double *slot = a.dist + (size_t)(i - a.r0) * a.ncols + (j - a.colbase);
+  bool qamb = false, qund = false;
+  unsigned long long qentry = 0;
+  bool to_replay = false;
+  if (acc[8] & 1) {
+    to_replay = true;  // order-dependent float sums in the main mode
+  } else {
+    double tng = (double)ag[0] / 16.0;
+    bool skip = tng <= (double)rc.min_overlap;
+    if (!skip && rc.fallback_avg && tng * rc.resolve_fraction <= (double)amb) {
+      // tn93 recomputes the pair with -a average (refkernel.cpp:742-750)
+      if (acc[8] & 2) {
+        to_replay = true;
+        qentry = 1ull << 63;
+      } else {
+        int av[7];
+#pragma unroll
+        for (int q = 0; q < 7; q++) {
+          int v = base[q];
+          if (WPLANE) v += wb[0] * EW[0].v[9 + q] + wb[1] * EW[1].v[9 + q] + wb[2] * EW[2].v[9 + q] + wb[3] * EW[3].v[9 + q] + nww * EW[4].v[9 + q];
+          av[q] = v;
+        }
+        for (uint32_t e = e0; e < e1; e++) {
+          const uint32_t v = __ldg(a.ev + e);
+          const int32_t *t = sagg[((v & 31) - 4) * kCodes + a.ccT[(size_t)(v >> 5) * Np + jj]].v;
+          for (int q = 0; q < 7; q++) av[q] += t[9 + q];
+        }
+        for (uint32_t e = f0; e < f1; e++) {
+          const uint32_t v = __ldg(a.ev + e);
+          const int pc = rowc[v >> 5];
+          if (sparse_code(pc, WPLANE)) continue;
+          const int32_t *t = sagg[((v & 31) - 4) * kCodes + pc].v;
+          for (int q = 0; q < 7; q++) av[q] += t[9 + q];
+        }
+        for (int q = 0; q < 7; q++) ag[q] = av[q];
+        skip = (double)ag[0] / 16.0 <= (double)rc.min_overlap;
+      }
+    }
+    if (!to_replay) {
+      if (skip) {
+        *slot = __longlong_as_double((long long)kSkipBits);
+      } else {
+        const double nf[4] = {(double)ag[4] / 16.0, (double)ag[5] / 16.0, (double)ag[6] / 16.0,
+                              (double)(2 * ag[0] - ag[4] - ag[5] - ag[6]) / 16.0};
+        *slot = finish_distance(*a.logt, rc, nf, (double)ag[1] / 16.0, (double)ag[2] / 16.0, (double)ag[3] / 16.0,
+                                qamb, qund);
+      }
+    }
+  }
+  if (to_replay) {
+    const unsigned idx = atomicAdd(a.replay_n, 1u);
+    if (idx < a.replay_cap) a.replay_q[idx] = qentry | ((unsigned long long)i << 31) | (unsigned long long)j;
+  }
+  count_flags(a.counters, qamb, qund);
+}
+
+//------------------------------------------------------------------------------------------------ replay
+// tn93's own per-pair walk for the order-dependent pairs: every site in order, float contributions summed in
+// site order, then the c1-major merge of float and integer cells (refkernel.cpp:622-750)
+__global__ void replay_kernel(ReplayArgs a)
+{
+  const unsigned n = *a.qn;
+  const unsigned idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const unsigned long long e = a.q[idx];
+  int t = (int)(e >> 63);
+  const long i = (long)((e >> 31) & 0xFFFFFFFFull), j = (long)(e & 0x7FFFFFFFull);
+  const RunConsts &rc = a.rc;
+  const uint8_t *s1 = a.cc + (size_t)i * rc.Lc, *s2 = a.cc + (size_t)j * rc.Lc;
+  double res = 0;
+  bool qamb = false, qund = false;
+  for (;;) {
+    const SiteEntry *S = a.site + t * kCodes * kCodes;
+    double fc[16];
+    long ic[16];
+    for (int q = 0; q < 16; q++) {
+      fc[q] = 0.;
+      ic[q] = 0;
+    }
+    long amb = 0;
+    for (long k = 0; k < rc.Lc; k++) {
+      const int c1 = s1[k], c2 = s2[k];
+      if ((c1 | c2) < 4) {
+        ic[c1 * 4 + c2]++;
+        continue;
+      }
+      const SiteEntry &s = S[c1 * kCodes + c2];
+      for (int q = 0; q < 16; q++)
+        if (s.fc[q] != 0.) fc[q] = __dadd_rn(fc[q], s.fc[q]);
+      ic[0] += s.icd[0];
+      ic[5] += s.icd[1];
+      ic[10] += s.icd[2];
+      ic[15] += s.icd[3];
+      amb += s.amb;
+    }
+    for (int x = 0; x < 4; x++) ic[x * 5] += rc.constCnt[x];
+    double tot = 0., nf[4] = {0., 0., 0., 0.};
+    for (int c1 = 0; c1 < 4; c1++)
+      for (int c2 = 0; c2 < 4; c2++) {
+        const double pc = fc[c1 * 4 + c2] = __dadd_rn(fc[c1 * 4 + c2], (double)ic[c1 * 4 + c2]);
+        tot = __dadd_rn(tot, pc);
+        nf[c1] = __dadd_rn(nf[c1], pc);
+        nf[c2] = __dadd_rn(nf[c2], pc);
+      }
+    if (tot <= (double)rc.min_overlap) {
+      res = __longlong_as_double((long long)kSkipBits);
+      break;
+    }
+    if (t == 0 && rc.fallback_avg && __dmul_rn(tot, rc.resolve_fraction) <= (double)(unsigned long)amb) {
+      t = 1;
+      continue;
+    }
+    const double diag = __dadd_rn(__dadd_rn(__dadd_rn(fc[0], fc[5]), fc[10]), fc[15]);
+    res = finish_distance(*a.logt, rc, nf, diag, __dadd_rn(fc[2], fc[8]), __dadd_rn(fc[7], fc[13]), qamb, qund);
+    break;
+  }
+  a.dist[(size_t)(i - a.r0) * a.ncols + (j - a.colbase)] = res;
+  count_flags(a.counters, qamb, qund);
+}
+
+//------------------------------------------------------------------------------------------------ rows
+__device__ __forceinline__ int digits_of(long v)
+{
+  int n = 1;
+  while (v >= 10) {
+    v /= 10;
+    n++;
+  }
+  return n;
+}
+
+struct PairView {
+  bool valid, computed, linked, counted;  // counted: contributes to the sums (not a -l skip)
+  int bin, hb;
+  long w;
+  double thisD;
+};
+
+__device__ __forceinline__ PairView view_pair(const RowArgs &a, long i, long j, long cnt_i)
+{
+  const RunConsts &rc = a.rc;
+  PairView v;
+  v.valid = j < rc.N;
+  v.computed = v.linked = v.counted = false;
+  v.bin = 0;
+  v.hb = 0;
+  v.w = 0;
+  v.thisD = -1.0;
+  if (!v.valid) return v;
+  const double raw = a.dist[(size_t)(i - a.r0) * a.ncols + (j - a.colbase)];
+  v.w = cnt_i * a.counts[j];
+  if (rc.fst) v.bin = i < rc.n1 ? (j >= rc.n1 ? 2 : 0) : 1;
+  if ((uint64_t)__double_as_longlong(raw) != kSkipBits) {
+    v.computed = true;
+    v.hb = hist_bin(raw);
+    v.thisD = raw <= 0. ? 0. : raw;
+  }
+  v.linked = v.thisD >= rc.min_distance && v.thisD <= rc.threshold;
+  v.counted = !(v.thisD <= -0.5);
+  return v;
+}
+
+__device__ __forceinline__ int line_len(const RowArgs &a, long i, long j, double thisD, int name_i)
+{
+  char g[24];
+  const int gl = fmt_g(thisD, g);
+  if (a.rc.format == 0) return name_i + a.name_len[j] + gl + 3;
+  return digits_of(i) + digits_of(j) + gl + 3;
+}
+
+__device__ __forceinline__ int self_len(const RowArgs &a, long i)
+{
+  if (!a.rc.report_self || a.rc.cross) return 0;
+  if (a.rc.format == 0) return 2 * a.name_len[i] + 4;
+  if (a.rc.format == 1) return 2 * digits_of(i) + 4;
+  return 0;
+}
+
+// one warp per row: histogram, links, skips, column-order sums, byte count
+__global__ void __launch_bounds__(256) rows_kernel(RowArgs a)
+{
+  __shared__ unsigned long long sh[3 * kHistBins];
+  for (int t = threadIdx.x; t < 3 * kHistBins; t += blockDim.x) sh[t] = 0;
+  __syncthreads();
+  const RunConsts &rc = a.rc;
+  const int lane = threadIdx.x & 31;
+  const long i = a.r0 + blockIdx.x * (long)kWarps + (threadIdx.x >> 5);
+  if (i < a.r1) {
+    const long cnt_i = a.counts[i];
+    const int nli = a.name_len[i];
+    double s0 = 0., s1 = 0., s2 = 0., w0 = 0., w1 = 0., w2 = 0.;
+    double m0 = 0., m1 = 0., m2 = 0.;
+    long long links = 0, skipped = 0;
+    unsigned long long bytes = 0;
+    if (!rc.cross) {
+      if (cnt_i > 1 && lane == 0) {
+        const unsigned long long svs = (unsigned long long)(cnt_i * (cnt_i - 1l)) >> 1;
+        if (i < rc.n1) {
+          w0 += (double)svs;
+          atomicAdd(&sh[0], svs);
+        } else {
+          w1 += (double)svs;
+          atomicAdd(&sh[kHistBins], svs);
+        }
+      }
+      if (lane == 0 && rc.emit) bytes += self_len(a, i);
+    }
+    const long lb = rc.cross ? rc.n1 : i + 1;
+    for (long j0 = lb; j0 < rc.N; j0 += 32) {
+      const long j = j0 + lane;
+      const PairView v = view_pair(a, i, j, cnt_i);
+      if (v.computed) atomicAdd(&sh[v.bin * kHistBins + v.hb], (unsigned long long)v.w);
+      if (v.valid && v.linked) {
+        links += v.w;
+        if (rc.emit) {
+          if (rc.format != 2)
+            bytes += line_len(a, i, j, v.thisD, nli);
+          else {
+            a.hy[(size_t)i * rc.N + j] = v.thisD;
+            a.hy[(size_t)j * rc.N + i] = v.thisD;
+          }
+        }
+      }
+      const bool inc = v.valid && v.counted;
+      if (v.valid && !v.counted) skipped++;
+      const double term = inc ? __dmul_rn(v.thisD, (double)v.w) : 0.;
+      if (inc) {
+        if (v.bin == 0) m0 = v.thisD > m0 ? v.thisD : m0;
+        else if (v.bin == 1) m1 = v.thisD > m1 ? v.thisD : m1;
+        else m2 = v.thisD > m2 ? v.thisD : m2;
+      }
+      // tn93 sums each row in column order (swifttn93.cpp:2594-2602): lane 0 adds the 32 terms in order
+      const unsigned incm = __ballot_sync(0xffffffffu, inc);
+      for (int l = 0; l < 32; l++) {
+        const double t = __shfl_sync(0xffffffffu, term, l);
+        const double wl = __shfl_sync(0xffffffffu, (double)v.w, l);
+        const int bl = __shfl_sync(0xffffffffu, v.bin, l);
+        if (lane == 0 && (incm >> l & 1)) {
+          if (bl == 0) {
+            s0 = __dadd_rn(s0, t);
+            w0 = __dadd_rn(w0, wl);
+          } else if (bl == 1) {
+            s1 = __dadd_rn(s1, t);
+            w1 = __dadd_rn(w1, wl);
+          } else {
+            s2 = __dadd_rn(s2, t);
+            w2 = __dadd_rn(w2, wl);
+          }
+        }
+      }
+    }
+    for (int o = 16; o; o >>= 1) {
+      links += __shfl_xor_sync(0xffffffffu, links, o);
+      skipped += __shfl_xor_sync(0xffffffffu, skipped, o);
+      bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+      m0 = fmax(m0, __shfl_xor_sync(0xffffffffu, m0, o));
+      m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+      m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+    }
+    if (lane == 0) {
+      const long r = i - a.r0;
+      a.row_bytes[r] = bytes;
+      a.row_sum[r * 3] = s0;
+      a.row_sum[r * 3 + 1] = s1;
+      a.row_sum[r * 3 + 2] = s2;
+      a.row_w[r * 3] = w0;
+      a.row_w[r * 3 + 1] = w1;
+      a.row_w[r * 3 + 2] = w2;
+      a.row_max[r * 3] = m0;
+      a.row_max[r * 3 + 1] = m1;
+      a.row_max[r * 3 + 2] = m2;
+      a.row_links[r] = links;
+      a.row_skipped[r] = skipped;
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < 3 * kHistBins; t += blockDim.x)
+    if (sh[t]) atomicAdd(&a.hist[t], sh[t]);
+}
+
+__device__ __forceinline__ char *put_bytes(char *o, const char *s, int n)
+{
+  for (int k = 0; k < n; k++) o[k] = s[k];
+  return o + n;
+}
+
+// one warp per row: the row's text at its scanned offset
+__global__ void __launch_bounds__(256) write_kernel(RowArgs a)
+{
+  const RunConsts &rc = a.rc;
+  const int lane = threadIdx.x & 31;
+  const long i = a.r0 + blockIdx.x * (long)kWarps + (threadIdx.x >> 5);
+  if (i >= a.r1) return;
+  const long cnt_i = a.counts[i];
+  const int nli = a.name_len[i];
+  const char *ni = a.names + a.name_off[i];
+  char *out = a.out + a.row_off[i - a.r0];
+  if (!rc.cross && rc.report_self) {
+    if (lane == 0) {
+      char *o = out;
+      if (rc.format == 0) {
+        o = put_bytes(o, ni, nli);
+        *o++ = rc.delim;
+        o = put_bytes(o, ni, nli);
+        *o++ = rc.delim;
+      } else {
+        char t[24];
+        const int n = fmt_long(i, t);
+        o = put_bytes(o, t, n);
+        *o++ = rc.delim;
+        o = put_bytes(o, t, n);
+        *o++ = rc.delim;
+      }
+      *o++ = '0';
+      *o++ = '\n';
+    }
+    out += self_len(a, i);
+  }
+  const long lb = rc.cross ? rc.n1 : i + 1;
+  for (long j0 = lb; j0 < rc.N; j0 += 32) {
+    const long j = j0 + lane;
+    const PairView v = view_pair(a, i, j, cnt_i);
+    const bool put = v.valid && v.linked;
+    char g[24];
+    int gl = 0, len = 0;
+    if (put) {
+      gl = fmt_g(v.thisD, g);
+      len = rc.format == 0 ? nli + a.name_len[j] + gl + 3 : digits_of(i) + digits_of(j) + gl + 3;
+    }
+    int pre = len;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, pre, o);
+      if (lane >= o) pre += t;
+    }
+    const int total = __shfl_sync(0xffffffffu, pre, 31);
+    if (put) {
+      char *o = out + (pre - len);
+      if (rc.format == 0) {
+        o = put_bytes(o, ni, nli);
+        *o++ = rc.delim;
+        o = put_bytes(o, a.names + a.name_off[j], a.name_len[j]);
+        *o++ = rc.delim;
+      } else {
+        char t[24];
+        int n = fmt_long(i, t);
+        o = put_bytes(o, t, n);
+        *o++ = rc.delim;
+        n = fmt_long(j, t);
+        o = put_bytes(o, t, n);
+        *o++ = rc.delim;
+      }
+      o = put_bytes(o, g, gl);
+      *o = '\n';
+    }
+    out += total;
+  }
+}
+
+// -f hyphy: per matrix row the byte count, then the text: "\n{" d(r,0) "," ... "}" with 0 on the diagonal, the
+// reported distance where the pair was reported and 100 elsewhere (swifttn93.cpp:2869-2897)
+__device__ __forceinline__ int hy_entry(const double *hy, long N, long r, long c, char *buf)
+{
+  if (c == r) {
+    buf[0] = '0';
+    return 1;
+  }
+  const double d = hy[(size_t)r * N + c];
+  if (d != d) {
+    buf[0] = '1';
+    buf[1] = '0';
+    buf[2] = '0';
+    return 3;
+  }
+  return fmt_g(d, buf);
+}
+
+__global__ void hy_len_kernel(const double *hy, long N, unsigned long long *row_bytes)
+{
+  const int lane = threadIdx.x & 31;
+  const long r = blockIdx.x * (long)kWarps + (threadIdx.x >> 5);
+  if (r >= N) return;
+  unsigned long long b = 0;
+  for (long c = lane; c < N; c += 32) {
+    char t[24];
+    b += hy_entry(hy, N, r, c, t) + (c ? 1 : 0);
+  }
+  for (int o = 16; o; o >>= 1) b += __shfl_xor_sync(0xffffffffu, b, o);
+  if (lane == 0) row_bytes[r] = b + 3;  // "\n{" and "}"
+}
+
+__global__ void hy_write_kernel(const double *hy, long N, const unsigned long long *row_off, char *out)
+{
+  const int lane = threadIdx.x & 31;
+  const long r = blockIdx.x * (long)kWarps + (threadIdx.x >> 5);
+  if (r >= N) return;
+  char *o = out + row_off[r];
+  if (lane == 0) {
+    o[0] = '\n';
+    o[1] = '{';
+  }
+  o += 2;
+  for (long c0 = 0; c0 < N; c0 += 32) {
+    const long c = c0 + lane;
+    char t[24];
+    int len = 0;
+    if (c < N) len = hy_entry(hy, N, r, c, t) + (c ? 1 : 0);
+    int pre = len;
+    for (int s = 1; s < 32; s <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, pre, s);
+      if (lane >= s) pre += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, pre, 31);
+    if (c < N) {
+      char *p = o + (pre - len);
+      if (c) *p++ = ',';
+      put_bytes(p, t, len - (c ? 1 : 0));
+    }
+    o += total;
+  }
+  if (lane == 0) *o = '}';
+}
+
+__global__ void fill_nan_kernel(double *p, size_t n)
+{
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    p[k] = __longlong_as_double(0x7FF8000000000000ll);
+}
+
+}  // namespace
+
+//================================================================================================== host side
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t n = 0;
+};
+
+struct tn93g_set {
+  long N = 0, L = 0;
+  uint8_t *d_codes = nullptr;
+  long *d_counts = nullptr;
+  char *d_names = nullptr;
+  uint64_t *d_name_off = nullptr;
+  int32_t *d_name_len = nullptr;
+  std::vector<long> counts, name_len;
+};
+
+struct tn93g_ctx {
+  int device = 0;
+  size_t budget = 0, used = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  LogTable *d_logt = nullptr;
+  Tables *h_tab = nullptr;
+  DevBuf seen, nN, varcol, planes, cc, ccT, evcount, evoff, ev, agg, site, dist, rq, rqn, counters, rbytes, rsum, rw,
+      rmax, rlinks, rskip, hist, roff, out, hy;
+  void *pinned = nullptr;
+  size_t pinned_n = 0;
+  cudaEvent_t evs[16];
+  double timings[8] = {0};
+  long launches = 0;
+  size_t dev_out_n = 0;
+};
+
+namespace {
+
+#define CU(call)                                                                      \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) {                                                          \
+      ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);                  \
+      return e_ == cudaErrorMemoryAllocation ? TN93G_ENOMEM : TN93G_ECUDA;            \
+    }                                                                                 \
+  } while (0)
+
+int ensure(tn93g_ctx *ctx, DevBuf &b, size_t bytes)
+{
+  if (bytes <= b.n && b.p) return TN93G_OK;
+  if (b.p) {
+    cudaFree(b.p);
+    ctx->used -= b.n;
+    b.p = nullptr;
+    b.n = 0;
+  }
+  bytes = std::max<size_t>(bytes, 256);
+  if (ctx->budget && ctx->used + bytes > ctx->budget) {
+    ctx->err = "over the context's HBM budget";
+    return TN93G_ENOMEM;
+  }
+  CU(cudaMalloc(&b.p, bytes));
+  b.n = bytes;
+  ctx->used += bytes;
+  return TN93G_OK;
+}
+
+int ensure_pinned(tn93g_ctx *ctx, size_t bytes)
+{
+  if (bytes <= ctx->pinned_n) return TN93G_OK;
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  ctx->pinned = nullptr;
+  ctx->pinned_n = 0;
+  bytes = std::max<size_t>(bytes + bytes / 4, 1 << 20);
+  CU(cudaHostAlloc(&ctx->pinned, bytes, cudaHostAllocDefault));
+  ctx->pinned_n = bytes;
+  return TN93G_OK;
+}
+
+// grows b to `bytes`, keeping its first `keep` bytes (stream-ordered copy)
+int ensure_keep(tn93g_ctx *ctx, DevBuf &b, size_t bytes, size_t keep)
+{
+  if (bytes <= b.n && b.p) return TN93G_OK;
+  bytes = std::max<size_t>(bytes + bytes / 2, 1 << 20);
+  if (ctx->budget && ctx->used + bytes > ctx->budget) {
+    ctx->err = "over the context's HBM budget";
+    return TN93G_ENOMEM;
+  }
+  void *p = nullptr;
+  CU(cudaMalloc(&p, bytes));
+  if (keep && b.p) CU(cudaMemcpyAsync(p, b.p, keep, cudaMemcpyDeviceToDevice, ctx->stream));
+  if (b.p) {
+    CU(cudaStreamSynchronize(ctx->stream));
+    cudaFree(b.p);
+    ctx->used -= b.n;
+  }
+  b.p = p;
+  b.n = bytes;
+  ctx->used += bytes;
+  return TN93G_OK;
+}
+
+#define TRY(x)                   \
+  do {                           \
+    int r_ = (x);                \
+    if (r_ != TN93G_OK) return r_; \
+  } while (0)
+
+}  // namespace
+
+extern "C" {
+
+const char *tn93g_strerror(int code)
+{
+  switch (code) {
+    case TN93G_OK: return "ok";
+    case TN93G_EINVAL: return "invalid argument";
+    case TN93G_ECUDA: return "CUDA runtime error";
+    case TN93G_ENOMEM: return "out of device or pinned memory";
+    case TN93G_ESINK: return "output callback aborted the run";
+    case TN93G_ENODEV: return "no usable CUDA device";
+    case TN93G_ETIMEOUT: return "device wait timed out";
+    case TN93G_ETOOBIG: return "alignment too long (L >= 2^25)";
+    default: return "unknown error";
+  }
+}
+
+const char *tn93g_last_cuda_error(tn93g_ctx *ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+int tn93g_create(tn93g_ctx **out, int device, size_t hbm_budget)
+{
+  if (!out) return TN93G_EINVAL;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) return TN93G_ENODEV;
+  tn93g_ctx *ctx = new tn93g_ctx();
+  ctx->device = device;
+  ctx->budget = hbm_budget;
+  int rc = TN93G_OK;
+  do {
+    if (cudaSetDevice(device) != cudaSuccess) {
+      rc = TN93G_ENODEV;
+      break;
+    }
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      rc = TN93G_ECUDA;
+      break;
+    }
+    for (auto &e : ctx->evs)
+      if (cudaEventCreate(&e) != cudaSuccess) rc = TN93G_ECUDA;
+    LogTable h;
+    build_log_table(&h);
+    if (cudaMalloc(&ctx->d_logt, sizeof(LogTable)) != cudaSuccess ||
+        cudaMemcpy(ctx->d_logt, &h, sizeof h, cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = TN93G_ECUDA;
+    ctx->h_tab = new Tables();
+  } while (0);
+  if (rc != TN93G_OK) {
+    tn93g_destroy(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return TN93G_OK;
+}
+
+void tn93g_destroy(tn93g_ctx *ctx)
+{
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  DevBuf *bufs[] = {&ctx->seen, &ctx->nN, &ctx->varcol, &ctx->planes, &ctx->cc, &ctx->ccT, &ctx->evcount,
+                    &ctx->evoff, &ctx->ev, &ctx->agg, &ctx->site, &ctx->dist, &ctx->rq, &ctx->rqn, &ctx->counters,
+                    &ctx->rbytes, &ctx->rsum, &ctx->rw, &ctx->rmax, &ctx->rlinks, &ctx->rskip, &ctx->hist,
+                    &ctx->roff, &ctx->out, &ctx->hy};
+  for (DevBuf *b : bufs)
+    if (b->p) cudaFree(b->p);
+  if (ctx->d_logt) cudaFree(ctx->d_logt);
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  for (auto &e : ctx->evs)
+    if (e) cudaEventDestroy(e);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx->h_tab;
+  delete ctx;
+}
+
+int tn93g_upload(tn93g_ctx *ctx, tn93g_set **out, const uint8_t *codes, long N, long L, const long *copy_counts,
+                 const char *names, const size_t *name_off, const long *name_len)
+{
+  if (!ctx || !out || !codes || N <= 0 || L <= 0 || !copy_counts || !names || !name_off || !name_len)
+    return TN93G_EINVAL;
+  if (L >= (1l << 25)) return TN93G_ETOOBIG;
+  cudaSetDevice(ctx->device);
+  tn93g_set *s = new tn93g_set();
+  s->N = N;
+  s->L = L;
+  s->counts.assign(copy_counts, copy_counts + N);
+  s->name_len.assign(name_len, name_len + N);
+  size_t nbytes = 0;
+  for (long i = 0; i < N; i++) nbytes = std::max(nbytes, name_off[i] + (size_t)name_len[i]);
+  std::vector<uint64_t> off(name_off, name_off + N);
+  std::vector<int32_t> nl(N);
+  for (long i = 0; i < N; i++) nl[i] = (int32_t)name_len[i];
+  auto fail = [&](cudaError_t e) {
+    ctx->err = cudaGetErrorString(e);
+    tn93g_free_set(ctx, s);
+    return e == cudaErrorMemoryAllocation ? TN93G_ENOMEM : TN93G_ECUDA;
+  };
+  cudaError_t e;
+  if ((e = cudaMalloc(&s->d_codes, (size_t)N * L)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&s->d_counts, N * sizeof(long))) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&s->d_names, nbytes + 1)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&s->d_name_off, N * sizeof(uint64_t))) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&s->d_name_len, N * sizeof(int32_t))) != cudaSuccess) return fail(e);
+  if ((e = cudaMemcpyAsync(s->d_codes, codes, (size_t)N * L, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+    return fail(e);
+  if ((e = cudaMemcpyAsync(s->d_counts, copy_counts, N * sizeof(long), cudaMemcpyHostToDevice, ctx->stream)) !=
+      cudaSuccess)
+    return fail(e);
+  if (nbytes && (e = cudaMemcpyAsync(s->d_names, names, nbytes, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+    return fail(e);
+  if ((e = cudaMemcpyAsync(s->d_name_off, off.data(), N * sizeof(uint64_t), cudaMemcpyHostToDevice, ctx->stream)) !=
+      cudaSuccess)
+    return fail(e);
+  if ((e = cudaMemcpyAsync(s->d_name_len, nl.data(), N * sizeof(int32_t), cudaMemcpyHostToDevice, ctx->stream)) !=
+      cudaSuccess)
+    return fail(e);
+  if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(e);
+  *out = s;
+  return TN93G_OK;
+}
+
+void tn93g_free_set(tn93g_ctx *ctx, tn93g_set *s)
+{
+  if (!s) return;
+  if (ctx) cudaSetDevice(ctx->device);
+  cudaFree(s->d_codes);
+  cudaFree(s->d_counts);
+  cudaFree(s->d_names);
+  cudaFree(s->d_name_off);
+  cudaFree(s->d_name_len);
+  delete s;
+}
+
+int tn93g_last_timings(tn93g_ctx *ctx, double *ms, int n)
+{
+  if (!ctx || !ms) return 0;
+  const int k = std::min(n, 7);
+  for (int q = 0; q < k; q++) ms[q] = ctx->timings[q];
+  return k;
+}
+
+void *tn93g_stream(tn93g_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+long tn93g_last_launches(tn93g_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_opts *opts, tn93g_sink sink, void *user,
+                    tn93g_summary *sum, bool to_device);
+
+int tn93g_run(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_opts *opts, tn93g_sink sink, void *user,
+              tn93g_summary *sum)
+{
+  return run_impl(ctx, set, n1, opts, sink, user, sum, false);
+}
+
+int tn93g_run_to_device(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_opts *opts, void **dev_out,
+                        size_t *nbytes, tn93g_summary *sum)
+{
+  if (!dev_out || !nbytes) return TN93G_EINVAL;
+  const int rc = run_impl(ctx, set, n1, opts, nullptr, nullptr, sum, true);
+  *dev_out = rc == TN93G_OK ? ctx->out.p : nullptr;
+  *nbytes = rc == TN93G_OK ? ctx->dev_out_n : 0;
+  return rc;
+}
+
+static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_opts *opts, tn93g_sink sink, void *user,
+                    tn93g_summary *sum, bool to_device)
+{
+  if (!ctx || !set || !opts || !sum || n1 <= 0 || n1 > set->N) return TN93G_EINVAL;
+  if (opts->mode < 0 || opts->mode > 4 || opts->format < 0 || opts->format > 2) return TN93G_EINVAL;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const long N = set->N, L = set->L;
+  memset(sum, 0, sizeof *sum);
+  for (double &t : ctx->timings) t = 0;
+  ctx->launches = 0;
+  ctx->dev_out_n = 0;
+  size_t dev_off = 0;  // to_device: bytes of the distance file already in ctx->out
+  RunConsts rc;
+  memset(&rc, 0, sizeof rc);
+  rc.N = N;
+  rc.n1 = n1;
+  rc.mode = opts->mode;
+  rc.gapmm = opts->mode == TN93G_GAPMM;
+  rc.fst = n1 < N && opts->do_fst;
+  rc.cross = n1 < N && !opts->do_fst;
+  rc.fallback_avg = (opts->mode == TN93G_RESOLVE || opts->mode == TN93G_SUBSET) && opts->resolve_fraction < 1.;
+  rc.emit = !opts->count_only;
+  rc.format = opts->format;
+  rc.delim = opts->delimiter;
+  rc.report_self = opts->report_self && !rc.cross && n1 == N && rc.emit;
+  rc.threshold = opts->threshold;
+  rc.min_distance = opts->min_distance;
+  rc.resolve_fraction = opts->resolve_fraction;
+  rc.min_overlap = opts->min_overlap;
+  const bool hyphy = rc.emit && opts->format == TN93G_HYPHY;
+  cudaEvent_t *E = ctx->evs;
+  CU(cudaEventRecord(E[0], st));
+
+  //------------------------------------------------------------------ pack
+  TRY(ensure(ctx, ctx->seen, L * sizeof(uint32_t)));
+  TRY(ensure(ctx, ctx->nN, sizeof(unsigned long long)));
+  CU(cudaMemsetAsync(ctx->seen.p, 0, L * sizeof(uint32_t), st));
+  CU(cudaMemsetAsync(ctx->nN.p, 0, sizeof(unsigned long long), st));
+  {
+    dim3 g((unsigned)((L + 255) / 256), (unsigned)((N + 63) / 64));
+    colscan_kernel<<<g, 256, 0, st>>>(set->d_codes, N, L, (uint32_t *)ctx->seen.p, (unsigned long long *)ctx->nN.p);
+    CU(cudaGetLastError());
+    ctx->launches++;
+  }
+  std::vector<uint32_t> seen(L);
+  unsigned long long nN = 0;
+  CU(cudaMemcpyAsync(seen.data(), ctx->seen.p, L * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(&nN, ctx->nN.p, sizeof nN, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  // a column is constant when every sequence has the same clean base there: each pair gets (b, b)
+  std::vector<int32_t> varcol;
+  varcol.reserve(L);
+  for (long p = 0; p < L; p++) {
+    const uint32_t m = seen[p];
+    if (m && !(m & (m - 1)) && m < 16) {
+      const int b = __builtin_ctz(m);
+      rc.constT++;
+      rc.constNf[b] += 2;
+      rc.constCnt[b]++;
+    } else
+      varcol.push_back((int32_t)p);
+  }
+  const long Lc = (long)varcol.size();
+  const long W = (Lc + 63) / 64;
+  const long Npad = (N + 31) / 32 * 32;
+  rc.Lc = Lc;
+  rc.W = W;
+  rc.Npad = Npad;
+  // N gets its own bit plane when frequent (more than 16 per sequence); gapmm always (gaps join it)
+  rc.wplane = rc.gapmm || nN > 16ull * (unsigned long long)N;
+  rc.NP = rc.gapmm ? 5 : 4;
+  TRY(ensure(ctx, ctx->varcol, std::max<long>(Lc, 1) * sizeof(int32_t)));
+  TRY(ensure(ctx, ctx->planes, (size_t)std::max<long>(W, 1) * rc.NP * Npad * sizeof(uint64_t)));
+  TRY(ensure(ctx, ctx->cc, (size_t)N * std::max<long>(Lc, 1)));
+  TRY(ensure(ctx, ctx->ccT, (size_t)std::max<long>(Lc, 1) * Npad));
+  TRY(ensure(ctx, ctx->evcount, N * sizeof(uint32_t)));
+  TRY(ensure(ctx, ctx->evoff, (N + 1) * sizeof(uint32_t)));
+  if (Lc) CU(cudaMemcpyAsync(ctx->varcol.p, varcol.data(), Lc * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  CU(cudaMemsetAsync(ctx->planes.p, 0, (size_t)std::max<long>(W, 1) * rc.NP * Npad * sizeof(uint64_t), st));
+  CU(cudaMemsetAsync(ctx->evcount.p, 0, N * sizeof(uint32_t), st));
+  PackArgs pa;
+  pa.codes = set->d_codes;
+  pa.N = N;
+  pa.L = L;
+  pa.Lc = Lc;
+  pa.W = W;
+  pa.Npad = Npad;
+  pa.varcol = (const int32_t *)ctx->varcol.p;
+  pa.NP = rc.NP;
+  pa.wplane = rc.wplane;
+  pa.gapmm = rc.gapmm;
+  pa.planes = (uint64_t *)ctx->planes.p;
+  pa.cc = (uint8_t *)ctx->cc.p;
+  pa.evcount = (uint32_t *)ctx->evcount.p;
+  pa.ev_off = (const uint32_t *)ctx->evoff.p;
+  if (W) {
+    pack_kernel<<<dim3((unsigned)W, (unsigned)((N + kWarps - 1) / kWarps)), 256, 0, st>>>(pa);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    transpose_kernel<<<dim3((unsigned)((Lc + 31) / 32), (unsigned)(Npad / 32)), dim3(32, 8), 0, st>>>(
+        (const uint8_t *)ctx->cc.p, (uint8_t *)ctx->ccT.p, N, Lc, Npad);
+    CU(cudaGetLastError());
+    ctx->launches++;
+  }
+  std::vector<uint32_t> evc(N), evoff(N + 1);
+  CU(cudaMemcpyAsync(evc.data(), ctx->evcount.p, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  evoff[0] = 0;
+  for (long i = 0; i < N; i++) evoff[i + 1] = evoff[i] + evc[i];
+  TRY(ensure(ctx, ctx->ev, std::max<size_t>(evoff[N], 1) * sizeof(uint32_t)));
+  CU(cudaMemcpyAsync(ctx->evoff.p, evoff.data(), (N + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  pa.ev = (uint32_t *)ctx->ev.p;
+  if (W && evoff[N]) {
+    events_kernel<<<(unsigned)((N + kWarps - 1) / kWarps), 256, 0, st>>>(pa);
+    CU(cudaGetLastError());
+    ctx->launches++;
+  }
+  // tables of this mode
+  build_tables(ctx->h_tab, opts->mode, opts->subset);
+  const size_t agg_n = kSparseCodes * kCodes + 5;
+  TRY(ensure(ctx, ctx->agg, agg_n * sizeof(AggEntry)));
+  TRY(ensure(ctx, ctx->site, sizeof(ctx->h_tab->site)));
+  CU(cudaMemcpyAsync(ctx->agg.p, ctx->h_tab->ev, agg_n * sizeof(AggEntry), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(ctx->site.p, ctx->h_tab->site, sizeof(ctx->h_tab->site), cudaMemcpyHostToDevice, st));
+  CU(cudaEventRecord(E[1], st));
+
+  //------------------------------------------------------------------ bands
+  const long upper = rc.cross ? n1 : N;
+  const long colbase = rc.cross ? n1 : 0;
+  const long ncols = N - colbase;
+  sum->pairwise = rc.cross ? (unsigned long)(N - n1) * (unsigned long)n1 : (unsigned long)(N - 1) * (unsigned long)N / 2;
+  // rows per band: about 64 M pair slots (512 MB of distances)
+  long band = std::max<long>(kWarps, std::min<long>(upper, (64l << 20) / std::max<long>(ncols, 1)));
+  band = (band + kWarps - 1) / kWarps * kWarps;
+  if (hyphy) {
+    TRY(ensure(ctx, ctx->hy, (size_t)N * N * sizeof(double)));
+    fill_nan_kernel<<<1024, 256, 0, st>>>((double *)ctx->hy.p, (size_t)N * N);
+    CU(cudaGetLastError());
+    ctx->launches++;
+  }
+  TRY(ensure(ctx, ctx->dist, (size_t)band * ncols * sizeof(double)));
+  TRY(ensure(ctx, ctx->rq, (size_t)band * ncols * sizeof(unsigned long long)));
+  TRY(ensure(ctx, ctx->rqn, sizeof(unsigned)));
+  TRY(ensure(ctx, ctx->counters, 4 * sizeof(unsigned long long)));
+  TRY(ensure(ctx, ctx->rbytes, band * sizeof(unsigned long long)));
+  TRY(ensure(ctx, ctx->roff, band * sizeof(unsigned long long)));
+  TRY(ensure(ctx, ctx->rsum, band * 3 * sizeof(double)));
+  TRY(ensure(ctx, ctx->rw, band * 3 * sizeof(double)));
+  TRY(ensure(ctx, ctx->rmax, band * 3 * sizeof(double)));
+  TRY(ensure(ctx, ctx->rlinks, band * sizeof(long long)));
+  TRY(ensure(ctx, ctx->rskip, band * sizeof(long long)));
+  TRY(ensure(ctx, ctx->hist, 3 * kHistBins * sizeof(unsigned long long)));
+  CU(cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(unsigned long long), st));
+  CU(cudaMemsetAsync(ctx->hist.p, 0, 3 * kHistBins * sizeof(unsigned long long), st));
+  std::vector<unsigned long long> rbytes(band), roff(band);
+  std::vector<double> rsum(band * 3), rw(band * 3), rmax(band * 3);
+  std::vector<long long> rlinks(band), rskip(band);
+  double max_[3] = {0, 0, 0}, mean[3] = {0, 0, 0}, wc[3] = {0, 0, 0};
+  long links = 0, skipped = 0;
+  float ms = 0;
+  for (long r0 = 0; r0 < upper; r0 += band) {
+    const long r1 = std::min(upper, r0 + band), nr = r1 - r0;
+    CU(cudaEventRecord(E[2], st));
+    CU(cudaMemsetAsync(ctx->rqn.p, 0, sizeof(unsigned), st));
+    PairArgs A;
+    A.rc = rc;
+    A.planes = (const uint64_t *)ctx->planes.p;
+    A.cc = (const uint8_t *)ctx->cc.p;
+    A.ccT = (const uint8_t *)ctx->ccT.p;
+    A.ev_off = (const uint32_t *)ctx->evoff.p;
+    A.ev = (const uint32_t *)ctx->ev.p;
+    A.agg = (const AggEntry *)ctx->agg.p;
+    A.r0 = r0;
+    A.r1 = r1;
+    A.ncols = ncols;
+    A.colbase = colbase;
+    A.dist = (double *)ctx->dist.p;
+    A.replay_q = (unsigned long long *)ctx->rq.p;
+    A.replay_n = (unsigned *)ctx->rqn.p;
+    A.replay_cap = (unsigned long long)band * ncols;
+    A.counters = (unsigned long long *)ctx->counters.p;
+    A.logt = ctx->d_logt;
+    // columns: the smallest lower bound of the band's rows onwards
+    const long cstart = rc.cross ? n1 : r0 + 1;
+    const long cblk0 = (cstart - colbase) / 32;
+    const long cblks = (ncols + 31) / 32 - cblk0;
+    if (cblks > 0) {
+      A.cstart = colbase + cblk0 * 32;
+      dim3 g((unsigned)cblks, (unsigned)((nr + kWarps - 1) / kWarps));
+      if (rc.wplane) {
+        if (rc.gapmm)
+          pair_kernel<true, true><<<g, 256, 0, st>>>(A);
+        else
+          pair_kernel<true, false><<<g, 256, 0, st>>>(A);
+      } else
+        pair_kernel<false, false><<<g, 256, 0, st>>>(A);
+      CU(cudaGetLastError());
+    ctx->launches++;
+    }
+    CU(cudaEventRecord(E[3], st));
+    unsigned nq = 0;
+    CU(cudaMemcpyAsync(&nq, ctx->rqn.p, sizeof nq, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    if (nq) {
+      ReplayArgs R;
+      R.rc = rc;
+      R.cc = (const uint8_t *)ctx->cc.p;
+      R.site = (const SiteEntry *)ctx->site.p;
+      R.q = (const unsigned long long *)ctx->rq.p;
+      R.qn = (const unsigned *)ctx->rqn.p;
+      R.r0 = r0;
+      R.ncols = ncols;
+      R.colbase = colbase;
+      R.dist = (double *)ctx->dist.p;
+      R.counters = (unsigned long long *)ctx->counters.p;
+      R.logt = ctx->d_logt;
+      replay_kernel<<<(nq + 127) / 128, 128, 0, st>>>(R);
+      CU(cudaGetLastError());
+    ctx->launches++;
+      sum->pairs_replayed += nq;
+    }
+    CU(cudaEventRecord(E[4], st));
+    RowArgs RA;
+    RA.rc = rc;
+    RA.dist = (const double *)ctx->dist.p;
+    RA.r0 = r0;
+    RA.r1 = r1;
+    RA.ncols = ncols;
+    RA.colbase = colbase;
+    RA.counts = set->d_counts;
+    RA.name_len = set->d_name_len;
+    RA.name_off = set->d_name_off;
+    RA.names = set->d_names;
+    RA.row_bytes = (unsigned long long *)ctx->rbytes.p;
+    RA.row_sum = (double *)ctx->rsum.p;
+    RA.row_w = (double *)ctx->rw.p;
+    RA.row_max = (double *)ctx->rmax.p;
+    RA.row_links = (long long *)ctx->rlinks.p;
+    RA.row_skipped = (long long *)ctx->rskip.p;
+    RA.hist = (unsigned long long *)ctx->hist.p;
+    RA.row_off = (const unsigned long long *)ctx->roff.p;
+    RA.hy = (double *)ctx->hy.p;
+    const unsigned rblocks = (unsigned)((nr + kWarps - 1) / kWarps);
+    rows_kernel<<<rblocks, 256, 0, st>>>(RA);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    CU(cudaEventRecord(E[5], st));
+    CU(cudaMemcpyAsync(rbytes.data(), ctx->rbytes.p, nr * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(rsum.data(), ctx->rsum.p, nr * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(rw.data(), ctx->rw.p, nr * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(rmax.data(), ctx->rmax.p, nr * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(rlinks.data(), ctx->rlinks.p, nr * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(rskip.data(), ctx->rskip.p, nr * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    CU(cudaEventElapsedTime(&ms, E[2], E[3]));
+    ctx->timings[1] += ms;
+    CU(cudaEventElapsedTime(&ms, E[3], E[4]));
+    ctx->timings[2] += ms;
+    CU(cudaEventElapsedTime(&ms, E[4], E[5]));
+    ctx->timings[3] += ms;
+    // rows in order (swifttn93.cpp:2838-2848)
+    unsigned long long tot = 0;
+    for (long r = 0; r < nr; r++) {
+      roff[r] = tot;
+      tot += rbytes[r];
+      links += rlinks[r];
+      skipped += rskip[r];
+      for (int q = 0; q < 3; q++) {
+        if (rmax[r * 3 + q] > max_[q]) max_[q] = rmax[r * 3 + q];
+        mean[q] += rsum[r * 3 + q];
+        wc[q] += rw[r * 3 + q];
+      }
+    }
+    if (rc.emit && !hyphy && tot) {
+      if (to_device) {
+        TRY(ensure_keep(ctx, ctx->out, dev_off + tot, dev_off));
+      } else {
+        TRY(ensure(ctx, ctx->out, tot));
+        TRY(ensure_pinned(ctx, tot));
+      }
+      CU(cudaMemcpyAsync(ctx->roff.p, roff.data(), nr * sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
+      RA.out = (char *)ctx->out.p + (to_device ? dev_off : 0);
+      CU(cudaEventRecord(E[6], st));
+      write_kernel<<<rblocks, 256, 0, st>>>(RA);
+      CU(cudaGetLastError());
+    ctx->launches++;
+      CU(cudaEventRecord(E[7], st));
+      if (!to_device) CU(cudaMemcpyAsync(ctx->pinned, ctx->out.p, tot, cudaMemcpyDeviceToHost, st));
+      CU(cudaEventRecord(E[8], st));
+      CU(cudaStreamSynchronize(st));
+      CU(cudaEventElapsedTime(&ms, E[6], E[7]));
+      ctx->timings[4] += ms;
+      CU(cudaEventElapsedTime(&ms, E[7], E[8]));
+      ctx->timings[5] += ms;
+      sum->output_bytes += tot;
+      dev_off += tot;
+      if (!to_device && sink && sink(user, (const char *)ctx->pinned, tot)) return TN93G_ESINK;
+    }
+  }
+  if (hyphy) {
+    TRY(ensure(ctx, ctx->rbytes, N * sizeof(unsigned long long)));
+    TRY(ensure(ctx, ctx->roff, N * sizeof(unsigned long long)));
+    const unsigned blocks = (unsigned)((N + kWarps - 1) / kWarps);
+    CU(cudaEventRecord(E[6], st));
+    hy_len_kernel<<<blocks, 256, 0, st>>>((const double *)ctx->hy.p, N, (unsigned long long *)ctx->rbytes.p);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    std::vector<unsigned long long> hb(N), ho(N);
+    CU(cudaMemcpyAsync(hb.data(), ctx->rbytes.p, N * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    unsigned long long tot = 1;  // leading "{"
+    for (long r = 0; r < N; r++) {
+      ho[r] = tot;
+      tot += hb[r];
+    }
+    tot += 2;  // "\n}"
+    TRY(ensure(ctx, ctx->out, tot));
+    if (!to_device) TRY(ensure_pinned(ctx, tot));
+    CU(cudaMemcpyAsync(ctx->roff.p, ho.data(), N * sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(ctx->out.p, "{", 1, cudaMemcpyHostToDevice, st));
+    hy_write_kernel<<<blocks, 256, 0, st>>>((const double *)ctx->hy.p, N, (const unsigned long long *)ctx->roff.p,
+                                            (char *)ctx->out.p);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    CU(cudaMemcpyAsync((char *)ctx->out.p + tot - 2, "\n}", 2, cudaMemcpyHostToDevice, st));
+    CU(cudaEventRecord(E[7], st));
+    if (!to_device) CU(cudaMemcpyAsync(ctx->pinned, ctx->out.p, tot, cudaMemcpyDeviceToHost, st));
+    CU(cudaEventRecord(E[8], st));
+    CU(cudaStreamSynchronize(st));
+    CU(cudaEventElapsedTime(&ms, E[6], E[7]));
+    ctx->timings[4] += ms;
+    CU(cudaEventElapsedTime(&ms, E[7], E[8]));
+    ctx->timings[5] += ms;
+    sum->output_bytes += tot;
+    dev_off = tot;
+    if (!to_device && sink && sink(user, (const char *)ctx->pinned, tot)) return TN93G_ESINK;
+  }
+  unsigned long long hist[3 * kHistBins], counters[4];
+  CU(cudaMemcpyAsync(hist, ctx->hist.p, sizeof hist, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(counters, ctx->counters.p, sizeof counters, cudaMemcpyDeviceToHost, st));
+  CU(cudaEventRecord(E[9], st));
+  CU(cudaStreamSynchronize(st));
+  CU(cudaEventElapsedTime(&ms, E[0], E[1]));
+  ctx->timings[0] = ms;
+  CU(cudaEventElapsedTime(&ms, E[0], E[9]));
+  ctx->timings[6] = ms;
+  for (int q = 0; q < 3; q++) {
+    sum->max[q] = max_[q];
+    sum->mean[q] = mean[q];
+    sum->weighted[q] = wc[q];
+    for (int k = 0; k < kHistBins; k++) sum->hist[q][k] = hist[q * kHistBins + k];
+  }
+  sum->links = links;
+  sum->skipped = skipped;
+  sum->logs_ambiguous = (long)counters[0];
+  sum->undecided = (long)counters[1];
+  ctx->dev_out_n = dev_off;
+  return TN93G_OK;
+}
+
+}  // extern "C"

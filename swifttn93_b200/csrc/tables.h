@@ -1,0 +1,46 @@
+// tables.h -- per-site contribution tables of tn93's ambiguity semantics, built on the host once per run and
+// uploaded to the device.
+#pragma once
+#include <stdint.h>
+
+namespace tn93 {
+
+constexpr int kCodes = 18;   // "ACGTURYSWKMBDHVN?-"
+constexpr int kGap = 17;
+constexpr int kN = 15;
+constexpr int kSparse0 = 4;  // first non-clean code
+constexpr int kSparseCodes = 13;  // codes 4..16
+
+// Lanes of an aggregate entry (x16 integers, exact while every contribution is a multiple of 1/16):
+//   0 T (total), 1 D (diagonal), 2 AG (A<->G), 3 CT (C<->T), 4 nfA, 5 nfC, 6 nfG  -- the main mode
+//   7 ambiguity count (resolved events, for the -g test)
+//   8 flags: bit 0 = a main-mode contribution is not a multiple of 1/16, bit 1 = the same in AVERAGE mode
+//   9..15 lanes 0..6 in AVERAGE mode (the -g fallback)
+constexpr int kLanes = 16;
+struct AggEntry {
+  int32_t v[kLanes];
+};
+
+// One site of the site-order replay: the float contributions of tn93's handler to the 4x4 table (row = code of
+// the first sequence), its integer diagonal increments and its ambiguity count.
+struct SiteEntry {
+  double fc[16];
+  int32_t icd[4];
+  int32_t amb;
+  int32_t pad[3];
+};
+
+struct Tables {
+  AggEntry ev[kSparseCodes * kCodes];  // [c - 4][o]: a sparse code c of one sequence facing code o
+  AggEntry ew[4];                      // N (or, under gapmm, a gap) facing clean base b
+  AggEntry eww;                        // N facing N
+  SiteEntry site[2][kCodes * kCodes];  // [0 main mode, 1 AVERAGE][c1 * 18 + c2]
+};
+
+// mode: 0 resolve, 1 average, 2 skip, 3 gapmm, 4 subset; subset[c] = 1 for codes listed in -a LIST
+void build_tables(Tables *T, int mode, const unsigned char subset[kCodes]);
+
+// true if code c is a "sparse event" code: not clean, not a gap, and not N when N has its own plane
+inline bool is_sparse_code(int c, bool w_plane) { return c >= kSparse0 && c < kGap && !(w_plane && c == kN); }
+
+}  // namespace tn93
