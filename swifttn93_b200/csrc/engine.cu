@@ -64,9 +64,9 @@ __global__ void colscan_kernel(const uint8_t *__restrict__ codes, long N, long L
 __global__ void pack_kernel(PackArgs a)
 {
   const int lane = threadIdx.x & 31;
-  const long i = blockIdx.y * (long)kWarps + (threadIdx.x >> 5);
-  const long w = blockIdx.x;
+  const long i = blockIdx.x * (long)kWarps + (threadIdx.x >> 5);
   if (i >= a.N) return;
+  for (long w = blockIdx.y; w < a.W; w += gridDim.y) {
   const long k0 = w * 64 + lane, k1 = k0 + 32;
   const int c0 = k0 < a.Lc ? a.codes[i * a.L + a.varcol[k0]] : 17;
   const int c1 = k1 < a.Lc ? a.codes[i * a.L + a.varcol[k1]] : 17;
@@ -90,6 +90,7 @@ __global__ void pack_kernel(PackArgs a)
     P[3 * a.Npad] = wn;
     if (a.NP > 4) P[4 * a.Npad] = gp;
     if (sp) atomicAdd(&a.evcount[i], (unsigned)popc(sp));
+  }
   }
 }
 
@@ -328,7 +329,7 @@ __global__ void __launch_bounds__(256) pair_kernel(PairArgs a)
 // site order, then the c1-major merge of float and integer cells (refkernel.cpp:622-750)
 __global__ void replay_kernel(ReplayArgs a)
 {
-  const unsigned n = *a.qn;
+  const unsigned long long n = min((unsigned long long)*a.qn, a.qcap);
   const unsigned idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
   const unsigned long long e = a.q[idx];
@@ -1065,7 +1066,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   pa.evcount = (uint32_t *)ctx->evcount.p;
   pa.ev_off = (const uint32_t *)ctx->evoff.p;
   if (W) {
-    pack_kernel<<<dim3((unsigned)W, (unsigned)((N + kWarps - 1) / kWarps)), 256, 0, st>>>(pa);
+    pack_kernel<<<dim3((unsigned)((N + kWarps - 1) / kWarps), (unsigned)std::min<long>(W, 65535)), 256, 0, st>>>(pa);
     CU(cudaGetLastError());
     ctx->launches++;
     transpose_kernel<<<dim3((unsigned)((Lc + 31) / 32), (unsigned)(Npad / 32)), dim3(32, 8), 0, st>>>(
@@ -1102,7 +1103,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   sum->pairwise = rc.cross ? (unsigned long)(N - n1) * (unsigned long)n1 : (unsigned long)(N - 1) * (unsigned long)N / 2;
   // rows per band: about 64 M pair slots (512 MB of distances)
   long band = std::max<long>(kWarps, std::min<long>(upper, (64l << 20) / std::max<long>(ncols, 1)));
-  band = (band + kWarps - 1) / kWarps * kWarps;
+  band = std::min<long>((band + kWarps - 1) / kWarps * kWarps, 65535l * kWarps);
   if (hyphy) {
     TRY(ensure(ctx, ctx->hy, (size_t)N * N * sizeof(double)));
     fill_nan_kernel<<<1024, 256, 0, st>>>((double *)ctx->hy.p, (size_t)N * N);
@@ -1179,6 +1180,8 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
       R.site = (const SiteEntry *)ctx->site.p;
       R.q = (const unsigned long long *)ctx->rq.p;
       R.qn = (const unsigned *)ctx->rqn.p;
+      R.qcap = (unsigned long long)band * ncols;
+      nq = (unsigned)std::min<unsigned long long>(nq, R.qcap);
       R.r0 = r0;
       R.ncols = ncols;
       R.colbase = colbase;

@@ -69,6 +69,7 @@ struct ReplayArgs {
   const SiteEntry *site;  // [2][18*18]
   const unsigned long long *q;
   const unsigned int *qn;
+  unsigned long long qcap;
   long r0, ncols, colbase;
   double *dist;
   unsigned long long *counters;
