@@ -1,0 +1,316 @@
+#!/usr/bin/env python3
+"""Throughput of the all-pairs TN93 path: pairwise distances per second, including the byte-exact text.
+
+Workload (one step): the benchmark-shaped alignment of 6,700 sequences x 1,500 columns (seeded synthetic data,
+swifttn93_b200.synth.hiv_bench: coalescent background at 6% divergence, 40 transmission clusters, 1% IUPAC
+ambiguity with 4% of sequences at 3-5%, gap runs and ragged ends), run once each with -a resolve, -a average and
+-a gapmm at -t 1000 -g 0.05 -l 500 -f csv, so every one of the 3 x 22,441,650 pairs is written.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value  : pairs/s with the alignment resident in HBM and the distance file left in HBM (tn93g_run_to_device),
+         device-timed with CUDA events on the engine's stream, L2 flushed between steps (outside the events).
+e2e    : pairs/s through the C ABI from host buffers: every step uploads the codes from pinned host memory and
+         copies the distance file back to pinned host memory (tn93g_upload + tn93g_run).
+--impl reference: the reference swifttn93 built from its own sources (oracle/_ref) on the host cores, same
+         workload and options, output to a tmpfs file, wall clock.
+Multi-GPU (torchrun): every rank runs its own replica of the workload (pairs are independent; no collective on
+the data path), value = pairs of all ranks / max over ranks of the device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "pairwise distances/sec (incl. byte-exact formatting) on 1 B200 vs host-CPU swifttn93"
+MODES = ("resolve", "average", "gapmm")
+FLAGS = dict(threshold=1000.0, resolve_fraction=0.05, min_overlap=500, format="csv")
+WORKLOAD = "hiv_bench 6700x1500, -t 1000 -g 0.05 -l 500 -f csv, -a resolve/average/gapmm (all pairs written)"
+
+
+def peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return dict(hbm=d["hbm_gbs"], bf16=d["bf16_tflops"], src="measured")
+    return dict(hbm=6650.0, bf16=1590.0, src="fallback")
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index=0):
+        self.index, self.samples, self._stop = index, [], threading.Event()
+
+    def __enter__(self):
+        def run():
+            q = ("index,clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    r = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                        "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                    if r.returncode == 0 and r.stdout.strip():
+                        self.samples.append([x.strip() for x in r.stdout.strip().split(",")])
+                except Exception:  # noqa: BLE001
+                    pass
+                self._stop.wait(0.2)
+
+        self.t = threading.Thread(target=run, daemon=True)
+        self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self.t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 4 + k and "Active" in s[4 + k]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def workload():
+    from swifttn93_b200 import synth
+
+    names, codes = synth.hiv_bench()
+    return names, codes
+
+
+def variable_columns(codes):
+    """Columns that are not the same clean base in every sequence (what the engine counts over)."""
+    first = codes[0]
+    const = (first < 4) & np.all(codes == first[None, :], axis=0)
+    return int((~const).sum())
+
+
+def reference_binary():
+    flags = set(open("/proc/cpuinfo").read().split()) if os.path.exists("/proc/cpuinfo") else set()
+    need = {"avx512f", "avx512dq", "avx512bw", "avx512vl", "avx512vbmi", "avx512_vbmi2", "avx512ifma",
+            "avx512_vpopcntdq", "avx512_bitalg", "avx512_vnni", "gfni", "vaes", "vpclmulqdq"}
+    for name, ok in (("swifttn93", need <= flags), ("swifttn93_libm", True)):
+        p = REPO / "oracle" / "_ref" / name
+        if p.exists() and ok:
+            return p
+    return None
+
+
+def run_reference(names, codes, steps, warmup, sample_modes=MODES):
+    """Wall time of the reference binary on all host cores over the workload; returns (pairs/s, detail)."""
+    from swifttn93_b200 import synth
+
+    ref = reference_binary()
+    if ref is None:
+        return None, "reference binary not built (oracle/build_ref.sh needs the reference sources)"
+    tmpdir = Path("/dev/shm") if Path("/dev/shm").is_dir() else Path(tempfile.gettempdir())
+    td = Path(tempfile.mkdtemp(dir=tmpdir))
+    try:
+        inp = td / "hiv_bench.fa"
+        inp.write_bytes(synth.to_fasta(names, codes))
+        n = codes.shape[0]
+        pairs = n * (n - 1) // 2
+        env = {**os.environ, "OMP_NUM_THREADS": str(os.cpu_count())}
+        times = []
+        for it in range(warmup + steps):
+            t0 = time.perf_counter()
+            for m in sample_modes:
+                out = td / "out.csv"
+                r = subprocess.run([str(ref), "-q", "-t", "1000", "-a", m, "-g", "0.05", "-l", "500", "-f", "csv",
+                                    "-o", str(out), str(inp)], stdout=subprocess.DEVNULL, env=env)
+                if r.returncode != 0:
+                    return None, f"reference exited {r.returncode}"
+                out.unlink()
+            if it >= warmup:
+                times.append(time.perf_counter() - t0)
+        per_step = float(np.mean(times))
+        return pairs * len(sample_modes) / per_step, dict(binary=ref.name, cores=os.cpu_count(), step_s=per_step)
+    finally:
+        shutil.rmtree(td, ignore_errors=True)
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    return ws, int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--n", type=int, default=0, help="use the first N sequences only (profiling runs)")
+    args = ap.parse_args()
+    ws, rank, local = dist_init()
+    names, codes = workload()
+    if args.n:
+        names, codes = names[:args.n], np.ascontiguousarray(codes[:args.n])
+    n = codes.shape[0]
+    pairs_step = len(MODES) * n * (n - 1) // 2
+    config = {"workload": WORKLOAD, "sequences": n, "columns": int(codes.shape[1]), "pairs_per_step": pairs_step,
+              "l2": "flushed between steps (256 MiB write), outside the timed events"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        v, det = run_reference(names, codes, args.steps, max(1, args.warmup))
+        if v is None:
+            print(json.dumps({"impl": "reference", "unavailable": det}))
+            return
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "pairs/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": det["step_s"] * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config,
+                "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": det["cores"], "kind": "reference",
+                                 "sample": f"full step ({len(MODES)} modes x {n*(n-1)//2} pairs), {det['binary']}, "
+                                           "output to tmpfs"},
+                "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+
+    from swifttn93_b200 import Engine, Options
+
+    torch.cuda.set_device(local)
+    eng = Engine(device=local)
+    stream = torch.cuda.ExternalStream(eng.stream, device=local)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=f"cuda:{local}")
+    opts = [Options(mode=m, **FLAGS) for m in MODES]
+    Lc = variable_columns(codes)
+
+    # ---- value: inputs and outputs resident in HBM
+    s = eng.upload(codes, names)
+    step_ms, stage_ms, launches, out_bytes = [], {}, 0, 0
+    clocks = Clocks(local)
+    for it in range(args.warmup + args.steps):
+        timed = it >= args.warmup
+        if timed and it == args.warmup:
+            if ws > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            clocks.__enter__()
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        summ = []
+        for o in opts:
+            ptr, nb, sm = eng.run_to_device(s, o)
+            summ.append(sm)
+            if timed:
+                launches += eng.last_launches()
+                out_bytes += nb
+                for k, v in sm.timings_ms.items():
+                    stage_ms[k] = stage_ms.get(k, 0.0) + v
+        ev1.record(stream)
+        ev1.synchronize()
+        if timed:
+            step_ms.append(ev0.elapsed_time(ev1))
+    torch.cuda.synchronize()
+    clocks.__exit__()
+    if ws > 1:
+        torch.distributed.barrier()
+    total_ms = float(np.sum(step_ms))
+    if ws > 1:
+        t = torch.tensor([total_ms], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = pairs_step * args.steps * ws / (total_ms / 1e3)
+
+    # ---- e2e: host buffers in, host bytes out, through the C ABI
+    pinned = torch.empty(codes.shape, dtype=torch.uint8).pin_memory()
+    pinned.numpy()[:] = codes
+    pin_np = pinned.numpy()
+    e2e_ms, h2d, d2h = [], 0, 0
+    for it in range(0 if args.no_e2e else args.warmup + args.steps):
+        timed = it >= args.warmup
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        nbytes = 0
+        for o in opts:
+            s2 = eng.upload(pin_np, names)
+            _, sm = eng.run(s2, o, sink="discard")
+            nbytes += sm.output_bytes
+            eng.free(s2)
+        torch.cuda.synchronize()
+        if timed:
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+            h2d = len(MODES) * (codes.nbytes + sum(len(x) for x in names) + 24 * n)
+            d2h = nbytes
+    e2e = pairs_step * ws / (float(np.mean(e2e_ms)) / 1e3) if e2e_ms else None
+
+    # ---- roofline of the dominant stage
+    P = peaks()
+    stages = {k: v for k, v in stage_ms.items() if k in ("pair", "replay", "rows", "write")}
+    dom = max(stages, key=stages.get)
+    per_launch_ms = stages[dom] / (args.steps * len(MODES))
+    pairs_run = n * (n - 1) // 2
+    if dom == "pair":
+        classes = 5  # the N/gap plane is active under gapmm; use the larger unit count throughout
+        work = pairs_run * classes * classes * Lc * 2  # INT8 one-hot MAC equivalents (x2 ops)
+        achieved = work / (per_launch_ms / 1e3) / 1e12
+        roof = {"kernel": "pair_kernel", "bound": "tensor", "achieved": achieved, "peak": 2 * P["bf16"],
+                "unit": "TFLOP/s", "frac": achieved / (2 * P["bf16"]), "traffic": None,
+                "peak_note": f"dense INT8 = 2 x {P['src']} bf16 ({P['bf16']} TF/s)",
+                "work_note": f"{classes}x{classes}xLc INT8 MACs per pair, Lc={Lc}"}
+    else:
+        bpp = {"write": out_bytes / (args.steps * len(MODES)) / pairs_run + 8, "rows": 8 + 8, "replay": 8}[dom]
+        achieved = pairs_run * bpp / (per_launch_ms / 1e3) / 1e9
+        roof = {"kernel": f"{dom}_kernel", "bound": "hbm", "achieved": achieved, "peak": P["hbm"], "unit": "GB/s",
+                "frac": achieved / P["hbm"], "traffic": None, "peak_note": f"{P['src']} HBM copy bandwidth",
+                "work_note": f"{bpp:.1f} algorithmic bytes per pair"}
+
+    line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+            "e2e": {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": roof, "gpu_launches": launches, "clocks": clocks.summary(),
+            "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()},
+            "engine": {"Lc": Lc, "ambiguous_log_pairs": int(sum(x.logs_ambiguous for x in summ)),
+                       "undecided": int(sum(x.undecided for x in summ)),
+                       "replayed": int(sum(x.pairs_replayed for x in summ))}}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        v, det = run_reference(names, codes, 1, 1)
+        if v is not None:
+            line["cpu_baseline"] = {"value": v, "unit": "pairs/s", "cores": det["cores"], "kind": "reference",
+                                    "sample": f"one full step ({len(MODES)} x {pairs_run} pairs), {det['binary']}, "
+                                              "output to tmpfs"}
+    eng.free(s)
+    eng.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -182,8 +182,8 @@ class Engine:
         s.handle = C.c_void_p()
 
     def run(self, s: DeviceSet, opts: Options, n1: int | None = None, sink=None):
-        """Runs all pairs of set s. sink(bytes-like memoryview) receives the distance file in order; when sink is
-        None the bytes are collected and returned."""
+        """Runs all pairs of set s. sink(bytes) receives the distance file in order; when sink is None the bytes are
+        collected and returned; sink="discard" leaves them in the engine's pinned host buffer (no callback)."""
         chunks = []
 
         def _sink(_user, ptr, n):
@@ -197,7 +197,7 @@ class Engine:
             except Exception:  # noqa: BLE001 - an exception must not unwind through C
                 return 1
 
-        cb = _SINK(_sink)
+        cb = None if (isinstance(sink, str) and sink == "discard") else _SINK(_sink)
         o = opts.to_c()
         S = _Summary()
         if n1 is None:
