@@ -84,7 +84,7 @@ class Clocks:
         sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
         mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 4 + k and "Active" in s[4 + k]})
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if len(s) > 4 + k and s[4 + k] == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.samples)}
 

@@ -197,7 +197,7 @@ class Engine:
             except Exception:  # noqa: BLE001 - an exception must not unwind through C
                 return 1
 
-        cb = None if (isinstance(sink, str) and sink == "discard") else _SINK(_sink)
+        cb = _SINK() if (isinstance(sink, str) and sink == "discard") else _SINK(_sink)
         o = opts.to_c()
         S = _Summary()
         if n1 is None:
