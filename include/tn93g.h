@@ -29,6 +29,7 @@ extern "C" {
 #define TN93G_ENODEV (-5)   /* no usable CUDA device */
 #define TN93G_ETIMEOUT (-6) /* a bounded device wait gave up (device error word set) */
 #define TN93G_ETOOBIG (-7)  /* alignment too long for the 32-bit x16 count lanes (L >= 2^25) */
+#define TN93G_ESCRATCH (-8) /* input beyond the fixed limits of tn93g_pair_distances_noalloc */
 
 /* Ambiguity modes, numbered as tn93's RESOLVE/AVERAGE/SKIP/GAPMM/SUBSET (solver/refkernel.h:14-18). */
 #define TN93G_RESOLVE 0
@@ -121,6 +122,28 @@ long tn93g_last_launches(tn93g_ctx *ctx);
  * [0] pack, [1] pair kernel, [2] site-order replay, [3] row reductions, [4] output formatting,
  * [5] device->host copies, [6] whole run. Returns the number of entries written (<= n). */
 int tn93g_last_timings(tn93g_ctx *ctx, double *ms, int n);
+
+/* Allocation-free pair distances. This entry point has no counterpart in the reference; it exists for callers
+ * that cannot allocate device memory -- code running while a CUDA graph is being captured, plugin hosts whose
+ * own allocator owns the whole device, or latency-critical loops that must not enter the driver's allocator.
+ * It runs the same pack, pair and site-order replay kernels as tn93g_run on one alignment, but every
+ * intermediate buffer lives in one fixed array inside this library (about 16 MB of device memory, held on
+ * every GPU that loads the library until the process exits), so it calls no cudaMalloc, cudaFree or other
+ * allocating routine. Limits: N <= 512 sequences, L <= 4096 columns; larger inputs return TN93G_ESCRATCH.
+ *   d_codes  device pointer, N x L codes 0..17 (row-major), the caller's
+ *   d_dist   device pointer, N x N doubles (row-major), the caller's; for every j > i, d_dist[i*N + j] receives
+ *            the raw distance of pair (i, j) as tn93g_run computes it (before tn93's "<= 0 -> 0"), or the bit
+ *            pattern 0x7FF4000000000BAD for a pair below the overlap (-l); other entries are not written
+ *   stream   a cudaStream_t, or NULL for the default stream; the call returns after the stream is synchronised
+ * The first call on a device (with that device current) looks up the array's device address and writes its
+ * logarithm table; make that first call before any stream capture. All calls share the array and it keeps
+ * the last call's contents (each call clears what must start at zero), so two calls whose GPU work overlaps
+ * would race: the library serialises calls from one process with a lock and returns only after the stream
+ * has drained; do not overlap them by other means. */
+int tn93g_pair_distances_noalloc(const uint8_t *d_codes, long N, long L, const tn93g_opts *opts, double *d_dist,
+                                 void *stream);
+/* message of the last failure of tn93g_pair_distances_noalloc */
+const char *tn93g_noalloc_last_error(void);
 
 #ifdef __cplusplus
 }

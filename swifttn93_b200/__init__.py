@@ -28,7 +28,7 @@ FORMATS = {"csv": 0, "csvn": 1, "hyphy": 2}
 # symbols declared in include/tn93g.h
 EXPORTS = ("tn93g_create", "tn93g_destroy", "tn93g_strerror", "tn93g_last_cuda_error", "tn93g_upload",
            "tn93g_free_set", "tn93g_run", "tn93g_run_to_device", "tn93g_stream", "tn93g_last_launches",
-           "tn93g_last_timings")
+           "tn93g_last_timings", "tn93g_pair_distances_noalloc", "tn93g_noalloc_last_error")
 
 
 class _Opts(C.Structure):

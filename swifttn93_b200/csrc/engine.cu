@@ -19,6 +19,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -819,6 +820,7 @@ const char *tn93g_strerror(int code)
     case TN93G_ENODEV: return "no usable CUDA device";
     case TN93G_ETIMEOUT: return "device wait timed out";
     case TN93G_ETOOBIG: return "alignment too long (L >= 2^25)";
+    case TN93G_ESCRATCH: return "alignment exceeds the allocation-free entry point's limits (N <= 512, L <= 4096)";
     default: return "unknown error";
   }
 }
@@ -1331,5 +1333,256 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   ctx->dev_out_n = dev_off;
   return TN93G_OK;
 }
+
+}  // extern "C"
+
+//================================================================================================== allocation-free entry point
+// tn93g_pair_distances_noalloc: the pack -> pair -> site-order replay pipeline of tn93g_run for one alignment,
+// with every intermediate buffer carved out of one fixed file-scope device array instead of cudaMalloc, for
+// callers that must not allocate device memory. Inputs and outputs are the caller's device buffers.
+namespace {
+
+constexpr long kNaMaxN = 512;   // sequences
+constexpr long kNaMaxL = 4096;  // columns
+constexpr long kNaW = (kNaMaxL + 63) / 64;
+constexpr size_t na_al(size_t x) { return (x + 255) / 256 * 256; }
+constexpr size_t kNaLog = 0;
+constexpr size_t kNaAgg = kNaLog + na_al(sizeof(LogTable));
+constexpr size_t kNaSite = kNaAgg + na_al((kSparseCodes * kCodes + 5) * sizeof(AggEntry));
+constexpr size_t kNaSeen = kNaSite + na_al(2 * kCodes * kCodes * sizeof(SiteEntry));
+constexpr size_t kNaNN = kNaSeen + na_al(kNaMaxL * sizeof(uint32_t));
+constexpr size_t kNaVarcol = kNaNN + na_al(sizeof(unsigned long long));
+constexpr size_t kNaPlanes = kNaVarcol + na_al(kNaMaxL * sizeof(int32_t));
+constexpr size_t kNaCC = kNaPlanes + na_al((size_t)kNaW * 5 * kNaMaxN * sizeof(uint64_t));
+constexpr size_t kNaCCT = kNaCC + na_al((size_t)kNaMaxN * kNaMaxL);
+constexpr size_t kNaEvcount = kNaCCT + na_al((size_t)kNaMaxL * kNaMaxN);
+constexpr size_t kNaEvoff = kNaEvcount + na_al(kNaMaxN * sizeof(uint32_t));
+constexpr size_t kNaEv = kNaEvoff + na_al((kNaMaxN + 1) * sizeof(uint32_t));
+constexpr size_t kNaRq = kNaEv + na_al((size_t)kNaMaxN * kNaMaxL * sizeof(uint32_t));
+constexpr size_t kNaRqn = kNaRq + na_al((size_t)kNaMaxN * kNaMaxN * sizeof(unsigned long long));
+constexpr size_t kNaCounters = kNaRqn + na_al(sizeof(unsigned));
+constexpr size_t kNaBytes = kNaCounters + na_al(4 * sizeof(unsigned long long));  // about 15.6 MB
+
+// The scratch. Every GPU that loads this library holds it until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+// Per device: the scratch's device address (cudaGetSymbolAddress, taken with that device current) and whether
+// the log table has been written into it. Host code must never pass the symbol itself to a kernel.
+constexpr int kNaMaxDevices = 64;
+std::mutex g_na_mu;
+unsigned char *g_na_base[kNaMaxDevices];
+
+// message of the last failure (written with g_na_mu held)
+char g_na_err[256];
+
+void na_error(const char *what, cudaError_t e)
+{
+  snprintf(g_na_err, sizeof g_na_err, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// caller holds g_na_mu
+int noalloc_setup(int dev, unsigned char **base)
+{
+  if (dev < 0 || dev >= kNaMaxDevices) return TN93G_ENODEV;
+  if (g_na_base[dev]) {
+    *base = g_na_base[dev];
+    return TN93G_OK;
+  }
+  unsigned char *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    na_error("cudaGetSymbolAddress", e);
+    return TN93G_ECUDA;
+  }
+  LogTable h;
+  build_log_table(&h);
+  e = cudaMemcpy(p + kNaLog, &h, sizeof h, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    na_error("cudaMemcpy", e);
+    return TN93G_ECUDA;
+  }
+  g_na_base[dev] = p;
+  *base = p;
+  return TN93G_OK;
+}
+
+Tables g_na_tables;  // host staging of the contribution tables (static storage; used with g_na_mu held)
+
+// caller holds g_na_mu
+int noalloc_run(const uint8_t *d_codes, long N, long L, const tn93g_opts *opts, double *d_dist, cudaStream_t st)
+{
+#define NA(call)                  \
+  do {                            \
+    cudaError_t e_ = (call);      \
+    if (e_ != cudaSuccess) {      \
+      na_error(#call, e_);        \
+      return TN93G_ECUDA;         \
+    }                             \
+  } while (0)
+  int dev = 0;
+  NA(cudaGetDevice(&dev));
+  unsigned char *S = nullptr;
+  const int src = noalloc_setup(dev, &S);
+  if (src != TN93G_OK) return src;
+  RunConsts rc;
+  memset(&rc, 0, sizeof rc);
+  rc.N = N;
+  rc.n1 = N;
+  rc.mode = opts->mode;
+  rc.gapmm = opts->mode == TN93G_GAPMM;
+  rc.fallback_avg = (opts->mode == TN93G_RESOLVE || opts->mode == TN93G_SUBSET) && opts->resolve_fraction < 1.;
+  rc.emit = !opts->count_only;
+  rc.format = opts->format;
+  rc.delim = opts->delimiter;
+  rc.threshold = opts->threshold;
+  rc.min_distance = opts->min_distance;
+  rc.resolve_fraction = opts->resolve_fraction;
+  rc.min_overlap = opts->min_overlap;
+  uint32_t *seen = (uint32_t *)(S + kNaSeen);
+  unsigned long long *nN = (unsigned long long *)(S + kNaNN);
+  NA(cudaMemsetAsync(seen, 0, L * sizeof(uint32_t), st));
+  NA(cudaMemsetAsync(nN, 0, sizeof(unsigned long long), st));
+  colscan_kernel<<<dim3((unsigned)((L + 255) / 256), (unsigned)((N + 63) / 64)), 256, 0, st>>>(d_codes, N, L, seen, nN);
+  NA(cudaGetLastError());
+  uint32_t h_seen[kNaMaxL];
+  int32_t h_varcol[kNaMaxL];
+  unsigned long long h_nN = 0;
+  NA(cudaMemcpyAsync(h_seen, seen, L * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  NA(cudaMemcpyAsync(&h_nN, nN, sizeof h_nN, cudaMemcpyDeviceToHost, st));
+  NA(cudaStreamSynchronize(st));
+  long Lc = 0;
+  for (long p = 0; p < L; p++) {
+    const uint32_t m = h_seen[p];
+    if (m && !(m & (m - 1)) && m < 16) {
+      const int b = __builtin_ctz(m);
+      rc.constT++;
+      rc.constNf[b] += 2;
+      rc.constCnt[b]++;
+    } else
+      h_varcol[Lc++] = (int32_t)p;
+  }
+  const long W = (Lc + 63) / 64, Npad = (N + 31) / 32 * 32;
+  rc.Lc = Lc;
+  rc.W = W;
+  rc.Npad = Npad;
+  rc.wplane = rc.gapmm || h_nN > 16ull * (unsigned long long)N;
+  rc.NP = rc.gapmm ? 5 : 4;
+  PackArgs pa;
+  pa.codes = d_codes;
+  pa.N = N;
+  pa.L = L;
+  pa.Lc = Lc;
+  pa.W = W;
+  pa.Npad = Npad;
+  pa.varcol = (const int32_t *)(S + kNaVarcol);
+  pa.NP = rc.NP;
+  pa.wplane = rc.wplane;
+  pa.gapmm = rc.gapmm;
+  pa.planes = (uint64_t *)(S + kNaPlanes);
+  pa.cc = S + kNaCC;
+  pa.evcount = (uint32_t *)(S + kNaEvcount);
+  pa.ev_off = (const uint32_t *)(S + kNaEvoff);
+  pa.ev = (uint32_t *)(S + kNaEv);
+  if (Lc) NA(cudaMemcpyAsync(S + kNaVarcol, h_varcol, Lc * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  NA(cudaMemsetAsync(pa.planes, 0, (size_t)std::max<long>(W, 1) * rc.NP * Npad * sizeof(uint64_t), st));
+  NA(cudaMemsetAsync(pa.evcount, 0, N * sizeof(uint32_t), st));
+  if (W) {
+    pack_kernel<<<dim3((unsigned)((N + kWarps - 1) / kWarps), (unsigned)W), 256, 0, st>>>(pa);
+    NA(cudaGetLastError());
+    transpose_kernel<<<dim3((unsigned)((Lc + 31) / 32), (unsigned)(Npad / 32)), dim3(32, 8), 0, st>>>(
+        pa.cc, S + kNaCCT, N, Lc, Npad);
+    NA(cudaGetLastError());
+  }
+  uint32_t h_evc[kNaMaxN], h_evoff[kNaMaxN + 1];
+  NA(cudaMemcpyAsync(h_evc, pa.evcount, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  NA(cudaStreamSynchronize(st));
+  h_evoff[0] = 0;
+  for (long i = 0; i < N; i++) h_evoff[i + 1] = h_evoff[i] + h_evc[i];
+  NA(cudaMemcpyAsync(S + kNaEvoff, h_evoff, (N + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  if (W && h_evoff[N]) {
+    events_kernel<<<(unsigned)((N + kWarps - 1) / kWarps), 256, 0, st>>>(pa);
+    NA(cudaGetLastError());
+  }
+  build_tables(&g_na_tables, opts->mode, opts->subset);
+  NA(cudaMemcpyAsync(S + kNaAgg, g_na_tables.ev, (kSparseCodes * kCodes + 5) * sizeof(AggEntry),
+                     cudaMemcpyHostToDevice, st));
+  NA(cudaMemcpyAsync(S + kNaSite, g_na_tables.site, sizeof(g_na_tables.site), cudaMemcpyHostToDevice, st));
+  unsigned *rqn = (unsigned *)(S + kNaRqn);
+  unsigned long long *counters = (unsigned long long *)(S + kNaCounters);
+  NA(cudaMemsetAsync(rqn, 0, sizeof(unsigned), st));
+  NA(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), st));
+  PairArgs A;
+  A.rc = rc;
+  A.planes = pa.planes;
+  A.cc = pa.cc;
+  A.ccT = S + kNaCCT;
+  A.ev_off = pa.ev_off;
+  A.ev = pa.ev;
+  A.agg = (const AggEntry *)(S + kNaAgg);
+  A.r0 = 0;
+  A.r1 = N;
+  A.ncols = N;
+  A.colbase = 0;
+  A.cstart = 0;
+  A.dist = d_dist;
+  A.replay_q = (unsigned long long *)(S + kNaRq);
+  A.replay_n = rqn;
+  A.replay_cap = (unsigned long long)kNaMaxN * kNaMaxN;
+  A.counters = counters;
+  A.logt = (const LogTable *)(S + kNaLog);
+  dim3 g((unsigned)((N + 31) / 32), (unsigned)((N + kWarps - 1) / kWarps));
+  if (rc.wplane) {
+    if (rc.gapmm)
+      pair_kernel<true, true><<<g, 256, 0, st>>>(A);
+    else
+      pair_kernel<true, false><<<g, 256, 0, st>>>(A);
+  } else
+    pair_kernel<false, false><<<g, 256, 0, st>>>(A);
+  NA(cudaGetLastError());
+  unsigned nq = 0;
+  NA(cudaMemcpyAsync(&nq, rqn, sizeof nq, cudaMemcpyDeviceToHost, st));
+  NA(cudaStreamSynchronize(st));
+  if (nq) {
+    ReplayArgs R;
+    R.rc = rc;
+    R.cc = pa.cc;
+    R.site = (const SiteEntry *)(S + kNaSite);
+    R.q = A.replay_q;
+    R.qn = rqn;
+    R.qcap = A.replay_cap;
+    R.r0 = 0;
+    R.ncols = N;
+    R.colbase = 0;
+    R.dist = d_dist;
+    R.counters = counters;
+    R.logt = A.logt;
+    replay_kernel<<<(nq + 127) / 128, 128, 0, st>>>(R);
+    NA(cudaGetLastError());
+  }
+  NA(cudaStreamSynchronize(st));
+  return TN93G_OK;
+#undef NA
+}
+
+}  // namespace
+
+extern "C" {
+
+int tn93g_pair_distances_noalloc(const uint8_t *d_codes, long N, long L, const tn93g_opts *opts, double *d_dist,
+                                 void *stream)
+{
+  if (!d_codes || !opts || !d_dist || N <= 0 || L <= 0) return TN93G_EINVAL;
+  if (opts->mode < 0 || opts->mode > 4) return TN93G_EINVAL;
+  std::lock_guard<std::mutex> g(g_na_mu);
+  if (N > kNaMaxN || L > kNaMaxL) {
+    snprintf(g_na_err, sizeof g_na_err,
+             "alignment of %ld x %ld exceeds the fixed scratch of the allocation-free entry point (N <= %ld, L <= %ld)",
+             N, L, kNaMaxN, kNaMaxL);
+    return TN93G_ESCRATCH;
+  }
+  return noalloc_run(d_codes, N, L, opts, d_dist, (cudaStream_t)stream);
+}
+
+const char *tn93g_noalloc_last_error(void) { return g_na_err; }
 
 }  // extern "C"
