@@ -114,7 +114,7 @@ def reference_binary():
     return None
 
 
-def run_reference(names, codes, steps, warmup, sample_modes=MODES):
+def run_reference(names, codes, steps, warmup, sample_modes=MODES, tflag="1000"):
     """Wall time of the reference binary on all host cores over the workload; returns (pairs/s, detail)."""
     from swifttn93_b200 import synth
 
@@ -134,7 +134,7 @@ def run_reference(names, codes, steps, warmup, sample_modes=MODES):
             t0 = time.perf_counter()
             for m in sample_modes:
                 out = td / "out.csv"
-                r = subprocess.run([str(ref), "-q", "-t", "1000", "-a", m, "-g", "0.05", "-l", "500", "-f", "csv",
+                r = subprocess.run([str(ref), "-q", "-t", tflag, "-a", m, "-g", "0.05", "-l", "500", "-f", "csv",
                                     "-o", str(out), str(inp)], stdout=subprocess.DEVNULL, env=env)
                 if r.returncode != 0:
                     return None, f"reference exited {r.returncode}"
@@ -249,6 +249,7 @@ def main():
     pinned.numpy()[:] = codes
     pin_np = pinned.numpy()
     e2e_ms, h2d, d2h = [], 0, 0
+    e2e_parts = {"upload": 0.0, "run": 0.0, "free": 0.0, "d2h_device": 0.0, "write_device": 0.0}
     for it in range(0 if args.no_e2e else args.warmup + args.steps):
         timed = it >= args.warmup
         with torch.cuda.stream(stream):
@@ -257,10 +258,20 @@ def main():
         t0 = time.perf_counter()
         nbytes = 0
         for o in opts:
+            ta = time.perf_counter()
             s2 = eng.upload(pin_np, names)
+            tb = time.perf_counter()
             _, sm = eng.run(s2, o, sink="discard")
+            tc = time.perf_counter()
             nbytes += sm.output_bytes
             eng.free(s2)
+            td = time.perf_counter()
+            if timed:
+                e2e_parts["upload"] += (tb - ta) * 1e3 / args.steps
+                e2e_parts["run"] += (tc - tb) * 1e3 / args.steps
+                e2e_parts["free"] += (td - tc) * 1e3 / args.steps
+                e2e_parts["d2h_device"] += sm.timings_ms.get("d2h", 0.0) / args.steps
+                e2e_parts["write_device"] += sm.timings_ms.get("write", 0.0) / args.steps
         torch.cuda.synchronize()
         if timed:
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
@@ -295,15 +306,45 @@ def main():
             "e2e": {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roof, "gpu_launches": launches, "clocks": clocks.summary(),
             "stage_ms_per_step": {k: v / args.steps for k, v in stage_ms.items()},
+            "e2e_ms_per_step_parts": e2e_parts,
             "engine": {"Lc": Lc, "ambiguous_log_pairs": int(sum(x.logs_ambiguous for x in summ)),
                        "undecided": int(sum(x.undecided for x in summ)),
                        "replayed": int(sum(x.pairs_replayed for x in summ))}}
+    # the compute-bound variant (HIV-TRACE flags: -t 0.015 -a resolve -g 0.05 -l 500): few pairs are written
+    if not args.no_e2e:
+        o15 = Options(mode="resolve", threshold=0.015, resolve_fraction=0.05, min_overlap=500, format="csv")
+        vt, et = [], []
+        for it in range(args.warmup + args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            eng.run_to_device(s, o15)
+            ev1.record(stream)
+            ev1.synchronize()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s3 = eng.upload(pin_np, names)
+            _, sm15 = eng.run(s3, o15, sink="discard")
+            eng.free(s3)
+            torch.cuda.synchronize()
+            if it >= args.warmup:
+                vt.append(ev0.elapsed_time(ev1))
+                et.append((time.perf_counter() - t0) * 1e3)
+        pr = n * (n - 1) // 2
+        line["variant_hivtrace_t0.015"] = {"value": pr / (np.mean(vt) / 1e3), "e2e": pr / (np.mean(et) / 1e3),
+                                            "unit": "pairs/s", "links": sm15.links,
+                                            "flags": "-t 0.015 -a resolve -g 0.05 -l 500 -f csv"}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         v, det = run_reference(names, codes, 1, 1)
         if v is not None:
             line["cpu_baseline"] = {"value": v, "unit": "pairs/s", "cores": det["cores"], "kind": "reference",
                                     "sample": f"one full step ({len(MODES)} x {pairs_run} pairs), {det['binary']}, "
                                               "output to tmpfs"}
+        if "variant_hivtrace_t0.015" in line:
+            v15, _ = run_reference(names, codes, 1, 1, sample_modes=("resolve",), tflag="0.015")
+            if v15 is not None:
+                line["variant_hivtrace_t0.015"]["reference"] = v15
     eng.free(s)
     eng.close()
     if rank == 0:

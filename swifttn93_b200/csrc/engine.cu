@@ -9,13 +9,14 @@
 //             (replaces kernel8/kernel16/kernelW/sparse_*/phaseA/tail8, swifttn93.cpp:1241-2170)
 //   replay    replay_kernel: pairs with a contribution that is not a multiple of 1/16 are recomputed by a
 //             site-order walk with tn93's float sums (replaces replay/ordered, swifttn93.cpp:1050-1232)
-//   rows      rows_kernel: per row, in column order: histogram, links, skipped pairs, the FP64 row sums in
-//             tn93's order, and the byte length of the row's output (phase C, swifttn93.cpp:2479-2604)
-//   write     write_kernel: the distance-file text of the band at scanned row offsets (the ordered writer,
+//   rows      stats_kernel (per row segment: histogram, links, skipped pairs, maxima, text length) and
+//             sum_kernel (per row, the FP64 sums in tn93's column order) (phase C, swifttn93.cpp:2479-2604)
+//   write     write_kernel: the distance-file text of the band at scanned segment offsets (the ordered writer,
 //             swifttn93.cpp:2811-2858, and fastfmt)
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -132,6 +133,29 @@ __global__ void transpose_kernel(const uint8_t *__restrict__ cc, uint8_t *ccT, l
 }
 
 //------------------------------------------------------------------------------------------------ pair
+// powers of ten for the certificate's fast test
+__device__ __constant__ double kP10[12] = {1e-5, 1e-4, 1e-3, 1e-2, 1e-1, 1e0, 1e1, 1e2, 1e3, 1e4, 1e5, 1e6};
+__device__ __constant__ double kScale[11] = {1e10, 1e9, 1e8, 1e7, 1e6, 1e5, 1e4, 1e3, 1e2, 1e1, 1e0};
+
+// Do lo <= hi print the same six significant digits? Fast test: scale both into [1e5, 1e6) and require the same
+// integer part with both fractions clear of 1/2 by 1e-4 (the scaled doubles are within 1e-9 of the exact scaled
+// values). Returns -1 when the test cannot decide (then the caller compares the printed strings).
+__device__ __forceinline__ int same_g_fast(double lo, double hi)
+{
+  if (!(lo >= 1e-5 && hi < 1e5)) return -1;
+  int X = 0;
+#pragma unroll
+  for (int k = 1; k < 10; k++) X += lo >= kP10[k];
+  const double s = kScale[X];
+  const double ta = __dmul_rn(lo, s), tb = __dmul_rn(hi, s);
+  if (!(ta >= 1e5 && tb < 1e6)) return -1;
+  const double fa = floor(ta), fb = floor(tb);
+  if (fa != fb) return -1;
+  const double ra = ta - fa, rb = tb - fb;
+  if (rb < 0.4999 || ra > 0.5001) return 1;
+  return -1;
+}
+
 // decision-stability certificate: do the histogram bin, the link decision and the printed text agree for
 // every distance the C library's log may lead to?
 __device__ bool certified(const Dist &D, const RunConsts &rc)
@@ -142,7 +166,9 @@ __device__ bool certified(const Dist &D, const RunConsts &rc)
   const bool lhi = thi >= rc.min_distance && thi <= rc.threshold;
   if (llo != lhi) return false;
   if (!llo && tlo < rc.min_distance && thi > rc.threshold) return false;
-  if (llo && rc.emit) {
+  if (llo && rc.emit && tlo != thi) {
+    const int f = same_g_fast(tlo, thi);
+    if (f >= 0) return f == 1;
     char x[24], y[24];
     const int nx = fmt_g(tlo, x), ny = fmt_g(thi, y);
     if (nx != ny) return false;
@@ -162,102 +188,59 @@ __device__ double finish_distance(const LogTable &T, const RunConsts &rc, const 
   return D.d;
 }
 
-__device__ __forceinline__ void count_flags(unsigned long long *counters, bool amb, bool und)
+// warp-level total of the per-lane counts, one atomic per warp (all 32 lanes must call it)
+__device__ __forceinline__ void count_flags(unsigned long long *counters, int namb, int nund)
 {
-  const unsigned ba = __ballot_sync(__activemask(), amb), bu = __ballot_sync(__activemask(), und);
-  const unsigned lead = __ffs(__activemask()) - 1;
-  if ((threadIdx.x & 31) == lead) {
-    if (ba) atomicAdd(&counters[0], (unsigned long long)__popc(ba));
-    if (bu) atomicAdd(&counters[1], (unsigned long long)__popc(bu));
+  for (int o = 16; o; o >>= 1) {
+    namb += __shfl_xor_sync(0xffffffffu, namb, o);
+    nund += __shfl_xor_sync(0xffffffffu, nund, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (namb) atomicAdd(&counters[0], (unsigned long long)namb);
+    if (nund) atomicAdd(&counters[1], (unsigned long long)nund);
   }
 }
 
-// one warp = one row i against 32 consecutive columns; a block = 8 rows x 32 columns
-template <bool WPLANE, bool GAPMM>
-__global__ void __launch_bounds__(256) pair_kernel(PairArgs a)
+__device__ __forceinline__ void add_entry(int acc[9], const int32_t *t)
 {
-  __shared__ AggEntry sagg[kSparseCodes * kCodes + 5];
-  for (int t = threadIdx.x; t < (kSparseCodes * kCodes + 5) * kLanes; t += blockDim.x)
-    ((int32_t *)sagg)[t] = ((const int32_t *)a.agg)[t];
-  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 8; q++) acc[q] += t[q];
+  acc[8] |= t[8];
+}
+
+// Block tile of the pair kernel: 32 rows x 32 columns, 8 warps. Column-side sparse events are summed with the
+// lanes over the tile's rows (warp-uniform event lists, coalesced position-major partner codes) into shared
+// memory; then each warp takes 4 of the tile's rows, one at a time, with the lanes over the columns: clean-site
+// counts, row-side events (warp-uniform list) and the epilogue.
+constexpr int kTile = 32;
+constexpr int kRowsPerWarp = kTile / kWarps;
+constexpr int kColAccStride = kTile * 9 + 1;  // ints per tile row (+1: conflict-free in both phases)
+constexpr int kAggInts = (kSparseCodes * kCodes + 5) * kLanes;
+constexpr size_t kPairSmem = (size_t)kAggInts * 4 + (size_t)kTile * kColAccStride * 4;
+
+struct Counts {
+  int T, MM, TS, CT, Y1, Y2, L1, L2, T1, T2;
+  int nWc, nWh, nWl, nWt, nWW, nGG;
+};
+
+// the per-pair epilogue: exact x16 aggregates, tn93's -l / -g / order decisions, formula, certificate
+template <bool WPLANE>
+__device__ __forceinline__ void pair_epilogue(const PairArgs &a, const AggEntry *sagg, const Counts &c, const int acc[9],
+                                              long i, long j, int &namb, int &nund)
+{
   const RunConsts &rc = a.rc;
-  const int lane = threadIdx.x & 31;
-  const long i = a.r0 + blockIdx.y * (long)kWarps + (threadIdx.x >> 5);
-  const long j = a.cstart + blockIdx.x * 32l + lane;
-  if (i >= a.r1) return;
-  const long lb = rc.cross ? rc.n1 : i + 1;
-  const bool valid = j >= lb && j < rc.N;
-  if (!__any_sync(0xffffffffu, valid)) return;
-  const long jj = j < rc.N ? j : rc.N - 1;
-  const long Np = rc.Npad;
-  // clean-site counts over the variable columns
-  int T = 0, MM = 0, TS = 0, CTc = 0, Y1 = 0, Y2 = 0, L1 = 0, L2 = 0, T1 = 0, T2 = 0;
-  int nWc = 0, nWh = 0, nWl = 0, nWt = 0, nWW = 0, nGG = 0;
-  const uint64_t *P = a.planes;
-  for (long w = 0; w < rc.W; w++, P += (size_t)rc.NP * Np) {
-    const uint64_t hi = __ldg(P + i), lo = __ldg(P + Np + i), ci = __ldg(P + 2 * Np + i);
-    const uint64_t hj = __ldg(P + jj), lj = __ldg(P + Np + jj), cj = __ldg(P + 2 * Np + jj);
-    const uint64_t b = ci & cj, x = hi ^ hj, y = lo ^ lj;
-    const uint64_t ts = b & ~x & y;
-    T += popc(b);
-    MM += popc(b & (x | y));
-    TS += popc(ts);
-    CTc += popc(ts & hi);
-    Y1 += popc(b & hi);
-    Y2 += popc(b & hj);
-    L1 += popc(b & lo);
-    L2 += popc(b & lj);
-    T1 += popc(b & hi & lo);
-    T2 += popc(b & hj & lj);
-    if (WPLANE) {
-      const uint64_t ni = __ldg(P + 3 * Np + i), nj = __ldg(P + 3 * Np + jj);
-      nWc += popc(ni & cj) + popc(nj & ci);
-      nWh += popc(ni & hj) + popc(nj & hi);
-      nWl += popc(ni & lj) + popc(nj & lo);
-      nWt += popc(ni & hj & lj) + popc(nj & hi & lo);
-      nWW += popc(ni & nj);
-      if (GAPMM) nGG += popc(__ldg(P + 4 * Np + i) & __ldg(P + 4 * Np + jj));
-    }
-  }
-  // sparse events: the row's (warp-uniform list, partner code from the position-major codes) ...
-  int acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  const uint32_t e0 = a.ev_off[i], e1 = a.ev_off[i + 1];
-  for (uint32_t e = e0; e < e1; e++) {
-    const uint32_t v = __ldg(a.ev + e);
-    const int code = v & 31;
-    const int pc = a.ccT[(size_t)(v >> 5) * Np + jj];
-    const int32_t *t = sagg[(code - 4) * kCodes + pc].v;
-#pragma unroll
-    for (int q = 0; q < 8; q++) acc[q] += t[q];
-    acc[8] |= t[8];
-  }
-  // ... and the column's (per lane), skipping sites where the row is itself sparse (counted above)
-  const uint8_t *rowc = a.cc + (size_t)i * rc.Lc;
-  const uint32_t f0 = a.ev_off[jj], f1 = valid ? a.ev_off[jj + 1] : f0;
-  for (uint32_t e = f0; e < f1; e++) {
-    const uint32_t v = __ldg(a.ev + e);
-    const int code = v & 31;
-    const int pc = rowc[v >> 5];
-    if (sparse_code(pc, WPLANE)) continue;
-    const int32_t *t = sagg[(code - 4) * kCodes + pc].v;
-#pragma unroll
-    for (int q = 0; q < 8; q++) acc[q] += t[q];
-    acc[8] |= t[8];
-  }
-  if (!valid) return;
-  // exact x16 aggregates
-  const int D = T - MM, nfT = T1 + T2, nfC = Y1 + Y2 - nfT, nfG = L1 + L2 - nfT;
-  const int nfA = 2 * T - nfC - nfG - nfT;
-  const int base[7] = {16 * (T + (int)rc.constT), 16 * (D + (int)rc.constT), 16 * (TS - CTc), 16 * CTc,
+  const int D = c.T - c.MM, nfT = c.T1 + c.T2, nfC = c.Y1 + c.Y2 - nfT, nfG = c.L1 + c.L2 - nfT;
+  const int nfA = 2 * c.T - nfC - nfG - nfT;
+  const int base[7] = {16 * (c.T + (int)rc.constT), 16 * (D + (int)rc.constT), 16 * (c.TS - c.CT), 16 * c.CT,
                        16 * (nfA + (int)rc.constNf[0]), 16 * (nfC + (int)rc.constNf[1]),
                        16 * (nfG + (int)rc.constNf[2])};
   int wb[4] = {0, 0, 0, 0}, nww = 0;
   if (WPLANE) {
-    wb[3] = nWt;
-    wb[1] = nWh - nWt;
-    wb[2] = nWl - nWt;
-    wb[0] = nWc - wb[1] - wb[2] - wb[3];
-    nww = nWW - nGG;
+    wb[3] = c.nWt;
+    wb[1] = c.nWh - c.nWt;
+    wb[2] = c.nWl - c.nWt;
+    wb[0] = c.nWc - wb[1] - wb[2] - wb[3];
+    nww = c.nWW - c.nGG;
   }
   const AggEntry *EW = &sagg[kSparseCodes * kCodes];
   int ag[7];
@@ -270,123 +253,276 @@ __global__ void __launch_bounds__(256) pair_kernel(PairArgs a)
   int amb = acc[7];
   if (WPLANE) amb += wb[0] * EW[0].v[7] + wb[1] * EW[1].v[7] + wb[2] * EW[2].v[7] + wb[3] * EW[3].v[7] + nww * EW[4].v[7];
   double *slot = a.dist + (size_t)(i - a.r0) * a.ncols + (j - a.colbase);
-  bool qamb = false, qund = false;
   unsigned long long qentry = 0;
   bool to_replay = false;
   if (acc[8] & 1) {
     to_replay = true;  // order-dependent float sums in the main mode
   } else {
-    double tng = (double)ag[0] / 16.0;
-    bool skip = tng <= (double)rc.min_overlap;
-    if (!skip && rc.fallback_avg && tng * rc.resolve_fraction <= (double)amb) {
-      // tn93 recomputes the pair with -a average (refkernel.cpp:742-750)
-      if (acc[8] & 2) {
-        to_replay = true;
-        qentry = 1ull << 63;
-      } else {
-        int av[7];
-#pragma unroll
-        for (int q = 0; q < 7; q++) {
-          int v = base[q];
-          if (WPLANE) v += wb[0] * EW[0].v[9 + q] + wb[1] * EW[1].v[9 + q] + wb[2] * EW[2].v[9 + q] + wb[3] * EW[3].v[9 + q] + nww * EW[4].v[9 + q];
-          av[q] = v;
-        }
-        for (uint32_t e = e0; e < e1; e++) {
-          const uint32_t v = __ldg(a.ev + e);
-          const int32_t *t = sagg[((v & 31) - 4) * kCodes + a.ccT[(size_t)(v >> 5) * Np + jj]].v;
-          for (int q = 0; q < 7; q++) av[q] += t[9 + q];
-        }
-        for (uint32_t e = f0; e < f1; e++) {
-          const uint32_t v = __ldg(a.ev + e);
-          const int pc = rowc[v >> 5];
-          if (sparse_code(pc, WPLANE)) continue;
-          const int32_t *t = sagg[((v & 31) - 4) * kCodes + pc].v;
-          for (int q = 0; q < 7; q++) av[q] += t[9 + q];
-        }
-        for (int q = 0; q < 7; q++) ag[q] = av[q];
-        skip = (double)ag[0] / 16.0 <= (double)rc.min_overlap;
-      }
-    }
-    if (!to_replay) {
-      if (skip) {
-        *slot = __longlong_as_double((long long)kSkipBits);
-      } else {
-        const double nf[4] = {(double)ag[4] / 16.0, (double)ag[5] / 16.0, (double)ag[6] / 16.0,
-                              (double)(2 * ag[0] - ag[4] - ag[5] - ag[6]) / 16.0};
-        *slot = finish_distance(*a.logt, rc, nf, (double)ag[1] / 16.0, (double)ag[2] / 16.0, (double)ag[3] / 16.0,
-                                qamb, qund);
-      }
+    const double tng = (double)ag[0] / 16.0;
+    if (tng <= (double)rc.min_overlap) {
+      *slot = __longlong_as_double((long long)kSkipBits);
+    } else if (rc.fallback_avg && tng * rc.resolve_fraction <= (double)amb) {
+      // tn93 recomputes the pair with -a average (refkernel.cpp:742-750): the site-order path does that exactly
+      to_replay = true;
+      qentry = 1ull << 63;
+    } else {
+      const double nf[4] = {(double)ag[4] / 16.0, (double)ag[5] / 16.0, (double)ag[6] / 16.0,
+                            (double)(2 * ag[0] - ag[4] - ag[5] - ag[6]) / 16.0};
+      bool qa, qu;
+      *slot = finish_distance(*a.logt, rc, nf, (double)ag[1] / 16.0, (double)ag[2] / 16.0, (double)ag[3] / 16.0, qa, qu);
+      namb += qa;
+      nund += qu;
     }
   }
   if (to_replay) {
     const unsigned idx = atomicAdd(a.replay_n, 1u);
     if (idx < a.replay_cap) a.replay_q[idx] = qentry | ((unsigned long long)i << 31) | (unsigned long long)j;
   }
-  count_flags(a.counters, qamb, qund);
+}
+
+template <bool WPLANE, bool GAPMM, int MINB>
+__global__ void __launch_bounds__(256, MINB) pair_kernel(PairArgs a)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  AggEntry *sagg = reinterpret_cast<AggEntry *>(smem_raw);
+  int *colacc = reinterpret_cast<int *>(smem_raw + (size_t)kAggInts * 4);
+  const RunConsts &rc = a.rc;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long i0 = a.r0 + blockIdx.y * (long)kTile;
+  const long j0 = a.cstart + blockIdx.x * (long)kTile;
+  // block-uniform exits: no valid pair in the tile
+  if (i0 >= a.r1 || j0 >= rc.N) return;
+  if (!rc.cross && j0 + kTile - 1 <= i0) return;
+  for (int t = threadIdx.x; t < kAggInts; t += blockDim.x) ((int32_t *)sagg)[t] = ((const int32_t *)a.agg)[t];
+  __syncthreads();
+  const long Np = rc.Npad;
+  // ---- column-side sparse events: lane = tile row, warp-uniform column; skipped where the row is sparse too
+  {
+    const long ib = min(i0 + lane, rc.N - 1);
+    for (int cl = warp; cl < kTile; cl += kWarps) {
+      const long j = j0 + cl;
+      int acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      if (j < rc.N) {
+        const uint32_t f0 = a.ev_off[j], f1 = a.ev_off[j + 1];
+        for (uint32_t e = f0; e < f1; e++) {
+          const uint32_t v = __ldg(a.ev + e);
+          const int pc = a.ccT[(size_t)(v >> 5) * Np + ib];
+          if (sparse_code(pc, WPLANE)) continue;
+          add_entry(acc, sagg[((v & 31) - 4) * kCodes + pc].v);
+        }
+      }
+      int *dst = colacc + lane * kColAccStride + cl * 9;
+#pragma unroll
+      for (int q = 0; q < 9; q++) dst[q] = acc[q];
+    }
+  }
+  __syncthreads();
+  // ---- per row of this warp (4 rows, one at a time): clean-site counts against lane = column, the row-side
+  // sparse events (warp-uniform list), then the epilogue
+  const long j = j0 + lane;
+  const long jj = j < rc.N ? j : rc.N - 1;
+  int namb = 0, nund = 0;
+#pragma unroll 1
+  for (int r = 0; r < kRowsPerWarp; r++) {
+    const long i = i0 + warp + kWarps * r;
+    if (i >= a.r1) break;
+    const long lb = rc.cross ? rc.n1 : i + 1;
+    const bool valid = j >= lb && j < rc.N;
+    if (!__any_sync(0xffffffffu, valid)) continue;
+    Counts c = Counts{0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const uint64_t *P = a.planes;
+    for (long w = 0; w < rc.W; w++, P += (size_t)rc.NP * Np) {
+      const uint64_t hj = __ldg(P + jj), lj = __ldg(P + Np + jj), cj = __ldg(P + 2 * Np + jj);
+      const uint64_t hi = __ldg(P + i), lo = __ldg(P + Np + i), ci = __ldg(P + 2 * Np + i);
+      const uint64_t b = ci & cj, x = hi ^ hj, y = lo ^ lj;
+      const uint64_t ts = b & ~x & y;
+      c.T += popc(b);
+      c.MM += popc(b & (x | y));
+      c.TS += popc(ts);
+      c.CT += popc(ts & hi);
+      c.Y1 += popc(b & hi);
+      c.Y2 += popc(b & hj);
+      c.L1 += popc(b & lo);
+      c.L2 += popc(b & lj);
+      c.T1 += popc(b & hi & lo);
+      c.T2 += popc(b & hj & lj);
+      if (WPLANE) {
+        const uint64_t ni = __ldg(P + 3 * Np + i), nj = __ldg(P + 3 * Np + jj);
+        c.nWc += popc(ni & cj) + popc(nj & ci);
+        c.nWh += popc(ni & hj) + popc(nj & hi);
+        c.nWl += popc(ni & lj) + popc(nj & lo);
+        c.nWt += popc(ni & hj & lj) + popc(nj & hi & lo);
+        c.nWW += popc(ni & nj);
+        if (GAPMM) c.nGG += popc(__ldg(P + 4 * Np + i) & __ldg(P + 4 * Np + jj));
+      }
+    }
+    int acc[9];
+    const int *src = colacc + (int)(i - i0) * kColAccStride + lane * 9;
+#pragma unroll
+    for (int q = 0; q < 9; q++) acc[q] = src[q];
+    const uint32_t e0 = a.ev_off[i], e1 = a.ev_off[i + 1];
+    for (uint32_t e = e0; e < e1; e++) {
+      const uint32_t v = __ldg(a.ev + e);
+      const int pc = a.ccT[(size_t)(v >> 5) * Np + jj];
+      add_entry(acc, sagg[((v & 31) - 4) * kCodes + pc].v);
+    }
+    if (valid) pair_epilogue<WPLANE>(a, sagg, c, acc, i, j, namb, nund);
+  }
+  count_flags(a.counters, namb, nund);
 }
 
 //------------------------------------------------------------------------------------------------ replay
-// tn93's own per-pair walk for the order-dependent pairs: every site in order, float contributions summed in
-// site order, then the c1-major merge of float and integer cells (refkernel.cpp:622-750)
-__global__ void replay_kernel(ReplayArgs a)
+// position of the n-th set bit (0-based) of x; x has more than n set bits
+__device__ __forceinline__ int nth_bit32(unsigned x, int n)
 {
-  const unsigned long long n = min((unsigned long long)*a.qn, a.qcap);
-  const unsigned idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n) return;
-  const unsigned long long e = a.q[idx];
-  int t = (int)(e >> 63);
-  const long i = (long)((e >> 31) & 0xFFFFFFFFull), j = (long)(e & 0x7FFFFFFFull);
-  const RunConsts &rc = a.rc;
-  const uint8_t *s1 = a.cc + (size_t)i * rc.Lc, *s2 = a.cc + (size_t)j * rc.Lc;
-  double res = 0;
-  bool qamb = false, qund = false;
-  for (;;) {
-    const SiteEntry *S = a.site + t * kCodes * kCodes;
-    double fc[16];
-    long ic[16];
-    for (int q = 0; q < 16; q++) {
-      fc[q] = 0.;
-      ic[q] = 0;
+  int pos = 0;
+#pragma unroll
+  for (int s = 16; s; s >>= 1) {
+    const int c = __popc(x & ((1u << s) - 1u));
+    if (n >= c) {
+      n -= c;
+      x >>= s;
+      pos += s;
     }
-    long amb = 0;
-    for (long k = 0; k < rc.Lc; k++) {
-      const int c1 = s1[k], c2 = s2[k];
-      if ((c1 | c2) < 4) {
-        ic[c1 * 4 + c2]++;
-        continue;
-      }
-      const SiteEntry &s = S[c1 * kCodes + c2];
-      for (int q = 0; q < 16; q++)
-        if (s.fc[q] != 0.) fc[q] = __dadd_rn(fc[q], s.fc[q]);
-      ic[0] += s.icd[0];
-      ic[5] += s.icd[1];
-      ic[10] += s.icd[2];
-      ic[15] += s.icd[3];
-      amb += s.amb;
-    }
-    for (int x = 0; x < 4; x++) ic[x * 5] += rc.constCnt[x];
-    double tot = 0., nf[4] = {0., 0., 0., 0.};
-    for (int c1 = 0; c1 < 4; c1++)
-      for (int c2 = 0; c2 < 4; c2++) {
-        const double pc = fc[c1 * 4 + c2] = __dadd_rn(fc[c1 * 4 + c2], (double)ic[c1 * 4 + c2]);
-        tot = __dadd_rn(tot, pc);
-        nf[c1] = __dadd_rn(nf[c1], pc);
-        nf[c2] = __dadd_rn(nf[c2], pc);
-      }
-    if (tot <= (double)rc.min_overlap) {
-      res = __longlong_as_double((long long)kSkipBits);
-      break;
-    }
-    if (t == 0 && rc.fallback_avg && __dmul_rn(tot, rc.resolve_fraction) <= (double)(unsigned long)amb) {
-      t = 1;
-      continue;
-    }
-    const double diag = __dadd_rn(__dadd_rn(__dadd_rn(fc[0], fc[5]), fc[10]), fc[15]);
-    res = finish_distance(*a.logt, rc, nf, diag, __dadd_rn(fc[2], fc[8]), __dadd_rn(fc[7], fc[13]), qamb, qund);
-    break;
   }
-  a.dist[(size_t)(i - a.r0) * a.ncols + (j - a.colbase)] = res;
-  count_flags(a.counters, qamb, qund);
+  return pos;
+}
+
+// tn93's own per-pair computation for the order-dependent pairs (refkernel.cpp:622-750), one warp per pair:
+//   * clean/clean cells: the 4x4 table from the bit planes (lanes over 64-column words);
+//   * every other site in site order: per word, the lanes fetch the codes of the word's non-clean sites (in
+//     order) and lane q adds the site's contribution to float cell q, so each cell is summed in site order as
+//     tn93 does; lanes 16..19 add the integer diagonal resolutions, lane 20 the ambiguity count;
+//   * lane 0: tn93's c1-major merge of float and integer cells, the -l / -g tests and the formula.
+__global__ void __launch_bounds__(256) replay_kernel(ReplayArgs a)
+{
+  __shared__ unsigned char sc1[kWarps][64], sc2[kWarps][64];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned long long n = min((unsigned long long)*a.qn, a.qcap);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && n) atomicAdd(&a.counters[2], n);
+  const RunConsts &rc = a.rc;
+  const long Np = rc.Npad;
+  const uint64_t last_valid = (rc.Lc & 63) ? ((1ull << (rc.Lc & 63)) - 1ull) : ~0ull;
+  for (unsigned long long idx = (unsigned long long)blockIdx.x * kWarps + warp; idx < n;
+       idx += (unsigned long long)gridDim.x * kWarps) {
+    const unsigned long long e = a.q[idx];
+    int t = (int)(e >> 63);
+    const long i = (long)((e >> 31) & 0xFFFFFFFFull), j = (long)(e & 0x7FFFFFFFull);
+    const uint8_t *s1 = a.cc + (size_t)i * rc.Lc, *s2 = a.cc + (size_t)j * rc.Lc;
+    // clean/clean 4x4 counts (the same in every mode)
+    int cnt[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) cnt[q] = 0;
+    for (long w = lane; w < rc.W; w += 32) {
+      const uint64_t *P = a.planes + (size_t)w * rc.NP * Np;
+      const uint64_t hi = P[i], lo = P[Np + i], ci = P[2 * Np + i];
+      const uint64_t hj = P[j], lj = P[Np + j], cj = P[2 * Np + j];
+      const uint64_t xi[4] = {ci & ~hi & ~lo, ci & hi & ~lo, ci & ~hi & lo, ci & hi & lo};
+      const uint64_t xj[4] = {cj & ~hj & ~lj, cj & hj & ~lj, cj & ~hj & lj, cj & hj & lj};
+#pragma unroll
+      for (int x = 0; x < 4; x++)
+#pragma unroll
+        for (int y = 0; y < 4; y++) cnt[x * 4 + y] += popc(xi[x] & xj[y]);
+    }
+#pragma unroll
+    for (int q = 0; q < 16; q++)
+      for (int o = 16; o; o >>= 1) cnt[q] += __shfl_xor_sync(0xffffffffu, cnt[q], o);
+    double res = 0;
+    bool qamb = false, qund = false;
+    for (;;) {
+      const SiteEntry *S = a.site + t * kCodes * kCodes;
+      double acc = 0.;  // lane q < 16: float cell q
+      long iacc = 0;    // lanes 16..19: diagonal resolutions, lane 20: ambiguity count
+      for (long w = 0; w < rc.W; w++) {
+        const uint64_t *P = a.planes + (size_t)w * rc.NP * Np;
+        uint64_t E = ~(P[2 * Np + i] & P[2 * Np + j]);
+        if (w == rc.W - 1) E &= last_valid;
+        if (!E) continue;
+        const int ne = __popcll(E), nlo = __popc((unsigned)E);
+        for (int rk = lane; rk < ne; rk += 32) {
+          const int bit = rk < nlo ? nth_bit32((unsigned)E, rk) : 32 + nth_bit32((unsigned)(E >> 32), rk - nlo);
+          const long k = w * 64 + bit;
+          sc1[warp][rk] = s1[k];
+          sc2[warp][rk] = s2[k];
+        }
+        __syncwarp();
+        if (lane < 16) {
+          for (int l = 0; l < ne; l++) {
+            const double v = S[sc1[warp][l] * kCodes + sc2[warp][l]].fc[lane];
+            if (v != 0.) acc = __dadd_rn(acc, v);
+          }
+        } else if (lane < 20) {
+          for (int l = 0; l < ne; l++) iacc += S[sc1[warp][l] * kCodes + sc2[warp][l]].icd[lane - 16];
+        } else if (lane == 20) {
+          for (int l = 0; l < ne; l++) iacc += S[sc1[warp][l] * kCodes + sc2[warp][l]].amb;
+        }
+        __syncwarp();
+      }
+      // lane 0: gather the cells, then tn93's merge and decisions
+      double fc[16];
+      long icd[4];
+#pragma unroll
+      for (int q = 0; q < 16; q++) fc[q] = __shfl_sync(0xffffffffu, acc, q);
+#pragma unroll
+      for (int q = 0; q < 4; q++) icd[q] = __shfl_sync(0xffffffffu, iacc, 16 + q);
+      const long amb = __shfl_sync(0xffffffffu, iacc, 20);
+      int next = 0;  // 0 done, 1 recompute with -a average
+      if (lane == 0) {
+        long ic[16];
+        for (int q = 0; q < 16; q++) ic[q] = cnt[q];
+        for (int x = 0; x < 4; x++) ic[x * 5] += icd[x] + rc.constCnt[x];
+        double tot = 0., nf[4] = {0., 0., 0., 0.};
+        for (int c1 = 0; c1 < 4; c1++)
+          for (int c2 = 0; c2 < 4; c2++) {
+            const double pc = fc[c1 * 4 + c2] = __dadd_rn(fc[c1 * 4 + c2], (double)ic[c1 * 4 + c2]);
+            tot = __dadd_rn(tot, pc);
+            nf[c1] = __dadd_rn(nf[c1], pc);
+            nf[c2] = __dadd_rn(nf[c2], pc);
+          }
+        if (tot <= (double)rc.min_overlap) {
+          res = __longlong_as_double((long long)kSkipBits);
+        } else if (t == 0 && rc.fallback_avg && __dmul_rn(tot, rc.resolve_fraction) <= (double)(unsigned long)amb) {
+          next = 1;
+        } else {
+          const double diag = __dadd_rn(__dadd_rn(__dadd_rn(fc[0], fc[5]), fc[10]), fc[15]);
+          res = finish_distance(*a.logt, rc, nf, diag, __dadd_rn(fc[2], fc[8]), __dadd_rn(fc[7], fc[13]), qamb, qund);
+        }
+      }
+      next = __shfl_sync(0xffffffffu, next, 0);
+      if (!next) break;
+      t = 1;
+    }
+    if (lane == 0) {
+      a.dist[(size_t)(i - a.r0) * a.ncols + (j - a.colbase)] = res;
+      if (qamb) atomicAdd(&a.counters[0], 1ull);
+      if (qund) atomicAdd(&a.counters[1], 1ull);
+    }
+  }
+}
+
+// exclusive scan of a band's segment byte counts (one block), and the band total
+__global__ void __launch_bounds__(1024) scan_kernel(const unsigned long long *in, unsigned long long *out, long n,
+                                                   unsigned long long *total)
+{
+  __shared__ unsigned long long part[1024];
+  const long per = (n + 1023) / 1024;
+  const long b = threadIdx.x * per, e = min(n, b + per);
+  unsigned long long s = 0;
+  for (long k = b; k < e; k++) s += in[k];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {
+    const unsigned long long v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  unsigned long long run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+  for (long k = b; k < e; k++) {
+    out[k] = run;
+    run += in[k];
+  }
+  if (threadIdx.x == 1023) *total = part[1023];
 }
 
 //------------------------------------------------------------------------------------------------ rows
@@ -431,14 +567,6 @@ __device__ __forceinline__ PairView view_pair(const RowArgs &a, long i, long j, 
   return v;
 }
 
-__device__ __forceinline__ int line_len(const RowArgs &a, long i, long j, double thisD, int name_i)
-{
-  char g[24];
-  const int gl = fmt_g(thisD, g);
-  if (a.rc.format == 0) return name_i + a.name_len[j] + gl + 3;
-  return digits_of(i) + digits_of(j) + gl + 3;
-}
-
 __device__ __forceinline__ int self_len(const RowArgs &a, long i)
 {
   if (!a.rc.report_self || a.rc.cross) return 0;
@@ -447,77 +575,66 @@ __device__ __forceinline__ int self_len(const RowArgs &a, long i)
   return 0;
 }
 
-// one warp per row: histogram, links, skips, column-order sums, byte count
-__global__ void __launch_bounds__(256) rows_kernel(RowArgs a)
+// Columns per segment of the stats and write kernels: a warp handles one (row, segment), so a band of a few
+// long rows still fills the GPU.
+constexpr int kSeg = 1024;
+
+// one warp per (row, segment): histogram, links, skips, maxima and the byte count of the segment's text
+__global__ void __launch_bounds__(256) stats_kernel(RowArgs a)
 {
   __shared__ unsigned long long sh[3 * kHistBins];
   for (int t = threadIdx.x; t < 3 * kHistBins; t += blockDim.x) sh[t] = 0;
   __syncthreads();
   const RunConsts &rc = a.rc;
-  const int lane = threadIdx.x & 31;
-  const long i = a.r0 + blockIdx.x * (long)kWarps + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long i = a.r0 + blockIdx.x * (long)kWarps + warp;
+  const int sg = blockIdx.y;
   if (i < a.r1) {
+    const long r = i - a.r0, slot = r * a.maxseg + sg;
+    const long lb = rc.cross ? rc.n1 : i + 1;
+    const long c0 = lb + (long)sg * kSeg, c1 = min(rc.N, c0 + kSeg);
     const long cnt_i = a.counts[i];
     const int nli = a.name_len[i];
-    double s0 = 0., s1 = 0., s2 = 0., w0 = 0., w1 = 0., w2 = 0.;
+    const int dli = rc.format == 1 ? digits_of(i) : 0;
     double m0 = 0., m1 = 0., m2 = 0.;
     long long links = 0, skipped = 0;
     unsigned long long bytes = 0;
-    if (!rc.cross) {
+    if (sg == 0 && !rc.cross) {
       if (cnt_i > 1 && lane == 0) {
         const unsigned long long svs = (unsigned long long)(cnt_i * (cnt_i - 1l)) >> 1;
-        if (i < rc.n1) {
-          w0 += (double)svs;
-          atomicAdd(&sh[0], svs);
-        } else {
-          w1 += (double)svs;
-          atomicAdd(&sh[kHistBins], svs);
-        }
+        atomicAdd(&sh[i < rc.n1 ? 0 : kHistBins], svs);
       }
       if (lane == 0 && rc.emit) bytes += self_len(a, i);
     }
-    const long lb = rc.cross ? rc.n1 : i + 1;
-    for (long j0 = lb; j0 < rc.N; j0 += 32) {
+    for (long j0 = c0; j0 < c1; j0 += 32) {
       const long j = j0 + lane;
-      const PairView v = view_pair(a, i, j, cnt_i);
-      if (v.computed) atomicAdd(&sh[v.bin * kHistBins + v.hb], (unsigned long long)v.w);
+      PairView v = view_pair(a, i, j, cnt_i);
+      if (j >= c1) v.valid = v.computed = v.linked = false;
+      // histogram: lanes with the same bin add once (their weights summed when all are 1)
+      const int key = v.computed ? v.bin * kHistBins + v.hb : -1;
+      const unsigned peers = __match_any_sync(0xffffffffu, key);
+      if (__all_sync(0xffffffffu, !v.computed || v.w == 1)) {
+        if (v.computed && lane == __ffs(peers) - 1) atomicAdd(&sh[key], (unsigned long long)__popc(peers));
+      } else if (v.computed) {
+        atomicAdd(&sh[key], (unsigned long long)v.w);
+      }
       if (v.valid && v.linked) {
         links += v.w;
         if (rc.emit) {
-          if (rc.format != 2)
-            bytes += line_len(a, i, j, v.thisD, nli);
-          else {
+          if (rc.format != 2) {
+            const int gl = fmt_g_len(v.thisD);
+            bytes += rc.format == 0 ? nli + a.name_len[j] + gl + 3 : dli + digits_of(j) + gl + 3;
+          } else {
             a.hy[(size_t)i * rc.N + j] = v.thisD;
             a.hy[(size_t)j * rc.N + i] = v.thisD;
           }
         }
       }
-      const bool inc = v.valid && v.counted;
       if (v.valid && !v.counted) skipped++;
-      const double term = inc ? __dmul_rn(v.thisD, (double)v.w) : 0.;
-      if (inc) {
+      if (v.valid && v.counted) {
         if (v.bin == 0) m0 = v.thisD > m0 ? v.thisD : m0;
         else if (v.bin == 1) m1 = v.thisD > m1 ? v.thisD : m1;
         else m2 = v.thisD > m2 ? v.thisD : m2;
-      }
-      // tn93 sums each row in column order (swifttn93.cpp:2594-2602): lane 0 adds the 32 terms in order
-      const unsigned incm = __ballot_sync(0xffffffffu, inc);
-      for (int l = 0; l < 32; l++) {
-        const double t = __shfl_sync(0xffffffffu, term, l);
-        const double wl = __shfl_sync(0xffffffffu, (double)v.w, l);
-        const int bl = __shfl_sync(0xffffffffu, v.bin, l);
-        if (lane == 0 && (incm >> l & 1)) {
-          if (bl == 0) {
-            s0 = __dadd_rn(s0, t);
-            w0 = __dadd_rn(w0, wl);
-          } else if (bl == 1) {
-            s1 = __dadd_rn(s1, t);
-            w1 = __dadd_rn(w1, wl);
-          } else {
-            s2 = __dadd_rn(s2, t);
-            w2 = __dadd_rn(w2, wl);
-          }
-        }
       }
     }
     for (int o = 16; o; o >>= 1) {
@@ -529,24 +646,95 @@ __global__ void __launch_bounds__(256) rows_kernel(RowArgs a)
       m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
     }
     if (lane == 0) {
-      const long r = i - a.r0;
-      a.row_bytes[r] = bytes;
-      a.row_sum[r * 3] = s0;
-      a.row_sum[r * 3 + 1] = s1;
-      a.row_sum[r * 3 + 2] = s2;
-      a.row_w[r * 3] = w0;
-      a.row_w[r * 3 + 1] = w1;
-      a.row_w[r * 3 + 2] = w2;
-      a.row_max[r * 3] = m0;
-      a.row_max[r * 3 + 1] = m1;
-      a.row_max[r * 3 + 2] = m2;
-      a.row_links[r] = links;
-      a.row_skipped[r] = skipped;
+      a.seg_bytes[slot] = bytes;
+      a.seg_links[slot] = links;
+      a.seg_skip[slot] = skipped;
+      a.seg_max[slot * 3] = m0;
+      a.seg_max[slot * 3 + 1] = m1;
+      a.seg_max[slot * 3 + 2] = m2;
     }
   }
   __syncthreads();
   for (int t = threadIdx.x; t < 3 * kHistBins; t += blockDim.x)
     if (sh[t]) atomicAdd(&a.hist[t], sh[t]);
+}
+
+// one warp per row: tn93's row sums in column order (swifttn93.cpp:2594-2602); lane 0 adds each chunk's terms in
+// order. The self-pair weights come first, as tn93 adds them when the row starts (swifttn93.cpp:2405-2415).
+__global__ void __launch_bounds__(256) sum_kernel(RowArgs a)
+{
+  __shared__ double sterm[kWarps][32], sw[kWarps][32];
+  __shared__ unsigned char sbin[kWarps][32];
+  const RunConsts &rc = a.rc;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long i = a.r0 + blockIdx.x * (long)kWarps + warp;
+  if (i >= a.r1) return;
+  const long cnt_i = a.counts[i];
+  double s0 = 0., s1 = 0., s2 = 0., w0 = 0., w1 = 0., w2 = 0.;
+  if (!rc.cross && cnt_i > 1) {
+    const unsigned long long svs = (unsigned long long)(cnt_i * (cnt_i - 1l)) >> 1;
+    if (i < rc.n1)
+      w0 += (double)svs;
+    else
+      w1 += (double)svs;
+  }
+  const long lb = rc.cross ? rc.n1 : i + 1;
+  const double *drow = a.dist + (size_t)(i - a.r0) * a.ncols - a.colbase;
+  for (long j0 = lb; j0 < rc.N; j0 += 32) {
+    const long j = j0 + lane;
+    bool inc = false;
+    double term = 0., wl = 0.;
+    int bin = 0;
+    if (j < rc.N) {
+      const double raw = drow[j];
+      if ((uint64_t)__double_as_longlong(raw) != kSkipBits) {
+        const double t = raw <= 0. ? 0. : raw;
+        const long w = cnt_i * a.counts[j];
+        if (rc.fst) bin = i < rc.n1 ? (j >= rc.n1 ? 2 : 0) : 1;
+        inc = true;
+        term = __dmul_rn(t, (double)w);
+        wl = (double)w;
+      }
+    }
+    sterm[warp][lane] = term;
+    sw[warp][lane] = wl;
+    sbin[warp][lane] = inc ? (unsigned char)bin : (unsigned char)255;
+    __syncwarp();
+    if (lane == 0) {
+      const int n = (int)min(32l, rc.N - j0);
+      if (!rc.fst) {
+        for (int l = 0; l < n; l++)
+          if (sbin[warp][l] == 0) {
+            s0 = __dadd_rn(s0, sterm[warp][l]);
+            w0 = __dadd_rn(w0, sw[warp][l]);
+          }
+      } else {
+        for (int l = 0; l < n; l++) {
+          const int bl = sbin[warp][l];
+          if (bl == 0) {
+            s0 = __dadd_rn(s0, sterm[warp][l]);
+            w0 = __dadd_rn(w0, sw[warp][l]);
+          } else if (bl == 1) {
+            s1 = __dadd_rn(s1, sterm[warp][l]);
+            w1 = __dadd_rn(w1, sw[warp][l]);
+          } else if (bl == 2) {
+            s2 = __dadd_rn(s2, sterm[warp][l]);
+            w2 = __dadd_rn(w2, sw[warp][l]);
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+  if (lane == 0) {
+    const long r = i - a.r0;
+    a.row_sum[r * 3] = s0;
+    a.row_sum[r * 3 + 1] = s1;
+    a.row_sum[r * 3 + 2] = s2;
+    a.row_w[r * 3] = w0;
+    a.row_w[r * 3 + 1] = w1;
+    a.row_w[r * 3 + 2] = w2;
+  }
 }
 
 __device__ __forceinline__ char *put_bytes(char *o, const char *s, int n)
@@ -555,20 +743,91 @@ __device__ __forceinline__ char *put_bytes(char *o, const char *s, int n)
   return o + n;
 }
 
-// one warp per row: the row's text at its scanned offset
-__global__ void __launch_bounds__(256) write_kernel(RowArgs a)
+// the text of one reported pair at o (generic pointer: shared staging or global)
+__device__ __forceinline__ void put_line(char *o, const RowArgs &a, long i, long j, const char *ni, int nli,
+                                         const char *g, int gl)
 {
   const RunConsts &rc = a.rc;
-  const int lane = threadIdx.x & 31;
-  const long i = a.r0 + blockIdx.x * (long)kWarps + (threadIdx.x >> 5);
+  if (rc.format == 0) {
+    o = put_bytes(o, ni, nli);
+    *o++ = rc.delim;
+    o = put_bytes(o, a.names + a.name_off[j], a.name_len[j]);
+    *o++ = rc.delim;
+  } else {
+    char t[24];
+    int n = fmt_long(i, t);
+    o = put_bytes(o, t, n);
+    *o++ = rc.delim;
+    n = fmt_long(j, t);
+    o = put_bytes(o, t, n);
+    *o++ = rc.delim;
+  }
+  o = put_bytes(o, g, gl);
+  *o = '\n';
+}
+
+// Output staging: each warp assembles its lines in shared memory at the same offset modulo 16 as their
+// destination, then stores whole 16-byte blocks (edges byte by byte), so global writes are coalesced. Nothing is
+// written at or past the end of the counted range.
+constexpr int kStage = 4096;
+
+struct Stager {
+  char *buf;       // this warp's staging buffer (16-byte aligned)
+  uintptr_t gpos;  // global address of the first staged byte
+  uintptr_t gend;  // end of the counted range
+  int head, fill;  // buf[head .. head + fill) holds global [gpos, gpos + fill)
+  bool over;       // the text ran past its counted length (reported as an internal error)
+  __device__ void flush(int lane)
+  {
+    const uintptr_t g0 = gpos - (uintptr_t)head;
+    if (gpos + fill > gend) over = true;
+    const int end = (int)min((uintptr_t)(head + fill), gend > g0 ? gend - g0 : 0), nblk = (end + 15) >> 4;
+    for (int b = lane; b < nblk; b += 32) {
+      const int lo = b << 4, hi = lo + 16;
+      if (lo >= head && hi <= end)
+        *reinterpret_cast<uint4 *>(g0 + lo) = *reinterpret_cast<const uint4 *>(buf + lo);
+      else
+        for (int k = max(lo, head); k < min(hi, end); k++) *reinterpret_cast<char *>(g0 + k) = buf[k];
+    }
+    __syncwarp();
+    gpos += fill;
+    head = (int)(gpos & 15);
+    fill = 0;
+  }
+};
+
+// one warp per (row, segment): the segment's text at its scanned offset (the row's self line in segment 0)
+__global__ void __launch_bounds__(256) write_kernel(RowArgs a)
+{
+  __shared__ __align__(16) char stage[kWarps][kStage];
+  const RunConsts &rc = a.rc;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long i = a.r0 + blockIdx.x * (long)kWarps + warp;
+  const int sg = blockIdx.y;
   if (i >= a.r1) return;
+  const long slot = (i - a.r0) * a.maxseg + sg;
+  if (a.seg_bytes[slot] == 0) return;
+  const long lb = rc.cross ? rc.n1 : i + 1;
+  const long c0 = lb + (long)sg * kSeg, c1 = min(rc.N, c0 + kSeg);
   const long cnt_i = a.counts[i];
   const int nli = a.name_len[i];
   const char *ni = a.names + a.name_off[i];
-  char *out = a.out + a.row_off[i - a.r0];
-  if (!rc.cross && rc.report_self) {
+  Stager S;
+  S.buf = stage[warp];
+  S.gpos = (uintptr_t)(a.out + a.seg_off[slot]);
+  S.gend = S.gpos + a.seg_bytes[slot];
+  S.head = (int)(S.gpos & 15);
+  S.fill = 0;
+  S.over = false;
+  const int sl = sg == 0 ? self_len(a, i) : 0;
+  if (sl) {
+    const bool direct = S.head + sl > kStage;
+    if (direct && S.gpos + sl > S.gend) {
+      if (lane == 0) atomicAdd(a.err, 1ull);
+      return;
+    }
     if (lane == 0) {
-      char *o = out;
+      char *o = direct ? (char *)S.gpos : S.buf + S.head;
       if (rc.format == 0) {
         o = put_bytes(o, ni, nli);
         *o++ = rc.delim;
@@ -583,20 +842,25 @@ __global__ void __launch_bounds__(256) write_kernel(RowArgs a)
         *o++ = rc.delim;
       }
       *o++ = '0';
-      *o++ = '\n';
+      *o = '\n';
     }
-    out += self_len(a, i);
+    __syncwarp();
+    if (direct) {
+      S.gpos += sl;
+      S.head = (int)(S.gpos & 15);
+    } else
+      S.fill = sl;
   }
-  const long lb = rc.cross ? rc.n1 : i + 1;
-  for (long j0 = lb; j0 < rc.N; j0 += 32) {
+  const int dli = rc.format == 1 ? digits_of(i) : 0;
+  for (long j0 = c0; j0 < c1; j0 += 32) {
     const long j = j0 + lane;
     const PairView v = view_pair(a, i, j, cnt_i);
-    const bool put = v.valid && v.linked;
+    const bool put = j < c1 && v.valid && v.linked;
     char g[24];
     int gl = 0, len = 0;
     if (put) {
       gl = fmt_g(v.thisD, g);
-      len = rc.format == 0 ? nli + a.name_len[j] + gl + 3 : digits_of(i) + digits_of(j) + gl + 3;
+      len = rc.format == 0 ? nli + a.name_len[j] + gl + 3 : dli + digits_of(j) + gl + 3;
     }
     int pre = len;
     for (int o = 1; o < 32; o <<= 1) {
@@ -604,27 +868,26 @@ __global__ void __launch_bounds__(256) write_kernel(RowArgs a)
       if (lane >= o) pre += t;
     }
     const int total = __shfl_sync(0xffffffffu, pre, 31);
-    if (put) {
-      char *o = out + (pre - len);
-      if (rc.format == 0) {
-        o = put_bytes(o, ni, nli);
-        *o++ = rc.delim;
-        o = put_bytes(o, a.names + a.name_off[j], a.name_len[j]);
-        *o++ = rc.delim;
-      } else {
-        char t[24];
-        int n = fmt_long(i, t);
-        o = put_bytes(o, t, n);
-        *o++ = rc.delim;
-        n = fmt_long(j, t);
-        o = put_bytes(o, t, n);
-        *o++ = rc.delim;
+    if (total == 0) continue;
+    if (S.head + S.fill + total > kStage) S.flush(lane);
+    if (S.head + total > kStage) {
+      // a chunk larger than the staging buffer (very long names): write it in place
+      if (S.gpos + total > S.gend) {
+        S.over = true;
+        break;
       }
-      o = put_bytes(o, g, gl);
-      *o = '\n';
+      if (put) put_line((char *)(S.gpos + pre - len), a, i, j, ni, nli, g, gl);
+      __syncwarp();
+      S.gpos += total;
+      S.head = (int)(S.gpos & 15);
+    } else {
+      if (put) put_line(S.buf + S.head + S.fill + (pre - len), a, i, j, ni, nli, g, gl);
+      __syncwarp();
+      S.fill += total;
     }
-    out += total;
   }
+  S.flush(lane);
+  if (S.over && lane == 0) atomicAdd(a.err, 1ull);
 }
 
 // -f hyphy: per matrix row the byte count, then the text: "\n{" d(r,0) "," ... "}" with 0 on the diagonal, the
@@ -697,6 +960,46 @@ __global__ void fill_nan_kernel(double *p, size_t n)
     p[k] = __longlong_as_double(0x7FF8000000000000ll);
 }
 
+// pair kernel launch (dynamic shared memory above the 48 KB default needs the opt-in attribute once). Two
+// register budgets are built: 2 blocks per SM (128 registers, no spills) and 3 (80 registers, some spills);
+// TN93G_PAIR_BLOCKS=3 selects the second. They measured the same on the benchmark workload.
+template <int MINB>
+cudaError_t launch_pair_t(const PairArgs &A, dim3 g, cudaStream_t st)
+{
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(pair_kernel<false, false, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kPairSmem)) != cudaSuccess)
+      return e;
+    if ((e = cudaFuncSetAttribute(pair_kernel<true, false, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kPairSmem)) != cudaSuccess)
+      return e;
+    if ((e = cudaFuncSetAttribute(pair_kernel<true, true, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kPairSmem)) != cudaSuccess)
+      return e;
+    attr_done = true;
+  }
+  if (A.rc.wplane) {
+    if (A.rc.gapmm)
+      pair_kernel<true, true, MINB><<<g, 256, kPairSmem, st>>>(A);
+    else
+      pair_kernel<true, false, MINB><<<g, 256, kPairSmem, st>>>(A);
+  } else
+    pair_kernel<false, false, MINB><<<g, 256, kPairSmem, st>>>(A);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pair(const PairArgs &A, long ncolblocks, long nrows, cudaStream_t st)
+{
+  static const int minb = [] {
+    const char *e = getenv("TN93G_PAIR_BLOCKS");
+    return (e && atoi(e) == 3) ? 3 : 2;
+  }();
+  dim3 g((unsigned)ncolblocks, (unsigned)((nrows + kTile - 1) / kTile));
+  return minb == 3 ? launch_pair_t<3>(A, g, st) : launch_pair_t<2>(A, g, st);
+}
+
 }  // namespace
 
 //================================================================================================== host side
@@ -708,6 +1011,7 @@ struct DevBuf {
 
 struct tn93g_set {
   long N = 0, L = 0;
+  size_t cap[5] = {0, 0, 0, 0, 0};  // bytes of d_codes, d_counts, d_names, d_name_off, d_name_len
   uint8_t *d_codes = nullptr;
   long *d_counts = nullptr;
   char *d_names = nullptr;
@@ -728,6 +1032,16 @@ struct tn93g_ctx {
   void *pinned = nullptr;
   size_t pinned_n = 0;
   cudaEvent_t evs[16];
+  cudaStream_t copy_stream = nullptr;  // device->host copies of finished bands
+  cudaEvent_t evw0[2], evw1[2], evc0[2], evc1[2];
+  cudaEvent_t evk[2][5];  // per band parity: start, after pair, after replay, after stats+sums+scan, stats on host
+  DevBuf out2[2], total;
+  void *pin2[2] = {nullptr, nullptr};
+  size_t pin2_n[2] = {0, 0};
+  void *pstats = nullptr;
+  size_t pstats_n = 0;
+  // device buffers of freed sets, kept for the next upload (repeated upload/free skips the allocator)
+  std::vector<std::pair<void *, size_t>> set_pool;
   double timings[8] = {0};
   long launches = 0;
   size_t dev_out_n = 0;
@@ -773,6 +1087,18 @@ int ensure_pinned(tn93g_ctx *ctx, size_t bytes)
   bytes = std::max<size_t>(bytes + bytes / 4, 1 << 20);
   CU(cudaHostAlloc(&ctx->pinned, bytes, cudaHostAllocDefault));
   ctx->pinned_n = bytes;
+  return TN93G_OK;
+}
+
+int ensure_pinned_at(tn93g_ctx *ctx, void *&p, size_t &n, size_t bytes)
+{
+  if (bytes <= n && p) return TN93G_OK;
+  if (p) cudaFreeHost(p);
+  p = nullptr;
+  n = 0;
+  bytes = std::max<size_t>(bytes + bytes / 4, 1 << 20);
+  CU(cudaHostAlloc(&p, bytes, cudaHostAllocDefault));
+  n = bytes;
   return TN93G_OK;
 }
 
@@ -848,6 +1174,14 @@ int tn93g_create(tn93g_ctx **out, int device, size_t hbm_budget)
     }
     for (auto &e : ctx->evs)
       if (cudaEventCreate(&e) != cudaSuccess) rc = TN93G_ECUDA;
+    for (int q = 0; q < 2; q++) {
+      if (cudaEventCreate(&ctx->evw0[q]) != cudaSuccess || cudaEventCreate(&ctx->evw1[q]) != cudaSuccess ||
+          cudaEventCreate(&ctx->evc0[q]) != cudaSuccess || cudaEventCreate(&ctx->evc1[q]) != cudaSuccess)
+        rc = TN93G_ECUDA;
+      for (auto &e : ctx->evk[q])
+        if (cudaEventCreate(&e) != cudaSuccess) rc = TN93G_ECUDA;
+    }
+    if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) rc = TN93G_ECUDA;
     LogTable h;
     build_log_table(&h);
     if (cudaMalloc(&ctx->d_logt, sizeof(LogTable)) != cudaSuccess ||
@@ -875,6 +1209,18 @@ void tn93g_destroy(tn93g_ctx *ctx)
     if (b->p) cudaFree(b->p);
   if (ctx->d_logt) cudaFree(ctx->d_logt);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  for (int q = 0; q < 2; q++) {
+    if (ctx->out2[q].p) cudaFree(ctx->out2[q].p);
+    if (ctx->pin2[q]) cudaFreeHost(ctx->pin2[q]);
+    for (cudaEvent_t e : {ctx->evw0[q], ctx->evw1[q], ctx->evc0[q], ctx->evc1[q]})
+      if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->evk[q])
+      if (e) cudaEventDestroy(e);
+  }
+  if (ctx->total.p) cudaFree(ctx->total.p);
+  for (auto &b : ctx->set_pool) cudaFree(b.first);
+  if (ctx->pstats) cudaFreeHost(ctx->pstats);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   for (auto &e : ctx->evs)
     if (e) cudaEventDestroy(e);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -905,11 +1251,27 @@ int tn93g_upload(tn93g_ctx *ctx, tn93g_set **out, const uint8_t *codes, long N, 
     return e == cudaErrorMemoryAllocation ? TN93G_ENOMEM : TN93G_ECUDA;
   };
   cudaError_t e;
-  if ((e = cudaMalloc(&s->d_codes, (size_t)N * L)) != cudaSuccess) return fail(e);
-  if ((e = cudaMalloc(&s->d_counts, N * sizeof(long))) != cudaSuccess) return fail(e);
-  if ((e = cudaMalloc(&s->d_names, nbytes + 1)) != cudaSuccess) return fail(e);
-  if ((e = cudaMalloc(&s->d_name_off, N * sizeof(uint64_t))) != cudaSuccess) return fail(e);
-  if ((e = cudaMalloc(&s->d_name_len, N * sizeof(int32_t))) != cudaSuccess) return fail(e);
+  // smallest pooled buffer that fits, else a new allocation
+  auto take = [&](void **p, size_t bytes, int k) -> cudaError_t {
+    bytes = std::max<size_t>(bytes, 256);
+    long best = -1;
+    for (size_t q = 0; q < ctx->set_pool.size(); q++)
+      if (ctx->set_pool[q].second >= bytes && (best < 0 || ctx->set_pool[q].second < ctx->set_pool[best].second))
+        best = (long)q;
+    if (best >= 0) {
+      *p = ctx->set_pool[best].first;
+      s->cap[k] = ctx->set_pool[best].second;
+      ctx->set_pool.erase(ctx->set_pool.begin() + best);
+      return cudaSuccess;
+    }
+    s->cap[k] = bytes;
+    return cudaMalloc(p, bytes);
+  };
+  if ((e = take((void **)&s->d_codes, (size_t)N * L, 0)) != cudaSuccess) return fail(e);
+  if ((e = take((void **)&s->d_counts, N * sizeof(long), 1)) != cudaSuccess) return fail(e);
+  if ((e = take((void **)&s->d_names, nbytes + 1, 2)) != cudaSuccess) return fail(e);
+  if ((e = take((void **)&s->d_name_off, N * sizeof(uint64_t), 3)) != cudaSuccess) return fail(e);
+  if ((e = take((void **)&s->d_name_len, N * sizeof(int32_t), 4)) != cudaSuccess) return fail(e);
   if ((e = cudaMemcpyAsync(s->d_codes, codes, (size_t)N * L, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
     return fail(e);
   if ((e = cudaMemcpyAsync(s->d_counts, copy_counts, N * sizeof(long), cudaMemcpyHostToDevice, ctx->stream)) !=
@@ -931,12 +1293,16 @@ int tn93g_upload(tn93g_ctx *ctx, tn93g_set **out, const uint8_t *codes, long N, 
 void tn93g_free_set(tn93g_ctx *ctx, tn93g_set *s)
 {
   if (!s) return;
-  if (ctx) cudaSetDevice(ctx->device);
-  cudaFree(s->d_codes);
-  cudaFree(s->d_counts);
-  cudaFree(s->d_names);
-  cudaFree(s->d_name_off);
-  cudaFree(s->d_name_len);
+  void *bufs[5] = {s->d_codes, s->d_counts, s->d_names, s->d_name_off, s->d_name_len};
+  if (ctx) {
+    // the buffers go back to the context's pool (the context's stream has no work left on them: every run and
+    // upload synchronises it before returning)
+    for (int k = 0; k < 5; k++)
+      if (bufs[k]) ctx->set_pool.push_back({bufs[k], s->cap[k]});
+  } else {
+    for (int k = 0; k < 5; k++)
+      if (bufs[k]) cudaFree(bufs[k]);
+  }
   delete s;
 }
 
@@ -1103,38 +1469,111 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   const long colbase = rc.cross ? n1 : 0;
   const long ncols = N - colbase;
   sum->pairwise = rc.cross ? (unsigned long)(N - n1) * (unsigned long)n1 : (unsigned long)(N - 1) * (unsigned long)N / 2;
-  // rows per band: about 64 M pair slots (512 MB of distances)
-  long band = std::max<long>(kWarps, std::min<long>(upper, (64l << 20) / std::max<long>(ncols, 1)));
-  band = std::min<long>((band + kWarps - 1) / kWarps * kWarps, 65535l * kWarps);
+  // Band schedule. When the text goes to the host, a band holds about 3 M pairs (at most 16 M pair slots), so
+  // that the copy of one band overlaps the kernels of the next; otherwise up to 64 M slots (512 MB of distances).
+  const bool stream_text = !(to_device || hyphy || !rc.emit);
+  static const long band_pairs = [] {
+    const char *e = getenv("TN93G_BAND_PAIRS");  // tuning knob: pairs per band when streaming text
+    return e && atol(e) > 0 ? atol(e) : (3l << 20);
+  }();
+  const long target_pairs = stream_text ? band_pairs : (1l << 62);
+  const long cap_slots = stream_text ? (16l << 20) : (64l << 20);
+  std::vector<std::pair<long, long>> bands;
+  long maxrows = 1;
+  for (long r0 = 0; r0 < upper;) {
+    long r = r0, pairs = 0;
+    while (r < upper && (r == r0 || ((r - r0 + 1) * ncols <= cap_slots && pairs < target_pairs &&
+                                     r - r0 < 65535l * kTile))) {
+      pairs += rc.cross ? ncols : (N - r - 1);
+      r++;
+    }
+    bands.push_back({r0, r});
+    maxrows = std::max(maxrows, r - r0);
+    r0 = r;
+  }
+  const long band = maxrows;
+  const long maxseg = std::max<long>(1, (ncols + kSeg - 1) / kSeg);
+  const long nseg = band * maxseg;  // per band parity
   if (hyphy) {
     TRY(ensure(ctx, ctx->hy, (size_t)N * N * sizeof(double)));
     fill_nan_kernel<<<1024, 256, 0, st>>>((double *)ctx->hy.p, (size_t)N * N);
     CU(cudaGetLastError());
     ctx->launches++;
   }
-  TRY(ensure(ctx, ctx->dist, (size_t)band * ncols * sizeof(double)));
-  TRY(ensure(ctx, ctx->rq, (size_t)band * ncols * sizeof(unsigned long long)));
+  // per band parity (double-buffered): distances, segment statistics, row sums; the replay queue is per band
+  const size_t dslots = (size_t)band * ncols;
+  TRY(ensure(ctx, ctx->dist, 2 * dslots * sizeof(double)));
+  TRY(ensure(ctx, ctx->rq, dslots * sizeof(unsigned long long)));
   TRY(ensure(ctx, ctx->rqn, sizeof(unsigned)));
   TRY(ensure(ctx, ctx->counters, 4 * sizeof(unsigned long long)));
-  TRY(ensure(ctx, ctx->rbytes, band * sizeof(unsigned long long)));
-  TRY(ensure(ctx, ctx->roff, band * sizeof(unsigned long long)));
-  TRY(ensure(ctx, ctx->rsum, band * 3 * sizeof(double)));
-  TRY(ensure(ctx, ctx->rw, band * 3 * sizeof(double)));
-  TRY(ensure(ctx, ctx->rmax, band * 3 * sizeof(double)));
-  TRY(ensure(ctx, ctx->rlinks, band * sizeof(long long)));
-  TRY(ensure(ctx, ctx->rskip, band * sizeof(long long)));
+  TRY(ensure(ctx, ctx->rbytes, 2 * nseg * sizeof(unsigned long long)));
+  TRY(ensure(ctx, ctx->roff, 2 * nseg * sizeof(unsigned long long)));
+  TRY(ensure(ctx, ctx->rsum, 2 * band * 3 * sizeof(double)));
+  TRY(ensure(ctx, ctx->rw, 2 * band * 3 * sizeof(double)));
+  TRY(ensure(ctx, ctx->rmax, 2 * nseg * 3 * sizeof(double)));
+  TRY(ensure(ctx, ctx->rlinks, 2 * nseg * sizeof(long long)));
+  TRY(ensure(ctx, ctx->rskip, 2 * nseg * sizeof(long long)));
   TRY(ensure(ctx, ctx->hist, 3 * kHistBins * sizeof(unsigned long long)));
+  TRY(ensure(ctx, ctx->total, 2 * sizeof(unsigned long long)));
+  // pinned staging of a band's statistics: row sums and weights (3 each), segment maxima (3 each), segment links
+  // and skips, total bytes
+  const size_t stat_stride = (size_t)band * 6 * sizeof(double) +
+                             (size_t)nseg * (3 * sizeof(double) + 2 * sizeof(long long)) + sizeof(unsigned long long);
+  TRY(ensure_pinned_at(ctx, ctx->pstats, ctx->pstats_n, 2 * stat_stride));
   CU(cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(unsigned long long), st));
   CU(cudaMemsetAsync(ctx->hist.p, 0, 3 * kHistBins * sizeof(unsigned long long), st));
-  std::vector<unsigned long long> rbytes(band), roff(band);
-  std::vector<double> rsum(band * 3), rw(band * 3), rmax(band * 3);
-  std::vector<long long> rlinks(band), rskip(band);
   double max_[3] = {0, 0, 0}, mean[3] = {0, 0, 0}, wc[3] = {0, 0, 0};
   long links = 0, skipped = 0;
   float ms = 0;
-  for (long r0 = 0; r0 < upper; r0 += band) {
-    const long r1 = std::min(upper, r0 + band), nr = r1 - r0;
-    CU(cudaEventRecord(E[2], st));
+  struct HostStats {
+    double *sum, *w, *max;
+    long long *links, *skip;
+    unsigned long long *total;
+  };
+  auto host_stats = [&](int par) {
+    char *base = (char *)ctx->pstats + par * stat_stride;
+    HostStats h;
+    h.sum = (double *)base;
+    h.w = h.sum + band * 3;
+    h.max = h.w + band * 3;
+    h.links = (long long *)(h.max + nseg * 3);
+    h.skip = h.links + nseg;
+    h.total = (unsigned long long *)(h.skip + nseg);
+    return h;
+  };
+  auto row_args = [&](int bi) {
+    const int par = bi & 1;
+    RowArgs RA;
+    RA.rc = rc;
+    RA.dist = (const double *)ctx->dist.p + par * dslots;
+    RA.r0 = bands[bi].first;
+    RA.r1 = bands[bi].second;
+    RA.ncols = ncols;
+    RA.colbase = colbase;
+    RA.counts = set->d_counts;
+    RA.name_len = set->d_name_len;
+    RA.name_off = set->d_name_off;
+    RA.names = set->d_names;
+    RA.maxseg = maxseg;
+    RA.seg_bytes = (unsigned long long *)ctx->rbytes.p + par * nseg;
+    RA.seg_links = (long long *)ctx->rlinks.p + par * nseg;
+    RA.seg_skip = (long long *)ctx->rskip.p + par * nseg;
+    RA.seg_max = (double *)ctx->rmax.p + par * nseg * 3;
+    RA.row_sum = (double *)ctx->rsum.p + par * band * 3;
+    RA.row_w = (double *)ctx->rw.p + par * band * 3;
+    RA.hist = (unsigned long long *)ctx->hist.p;
+    RA.seg_off = (const unsigned long long *)ctx->roff.p + par * nseg;
+    RA.out = nullptr;
+    RA.hy = (double *)ctx->hy.p;
+    RA.err = (unsigned long long *)ctx->counters.p + 3;
+    return RA;
+  };
+  // pair -> replay -> stats -> sums -> scan of band bi, then its statistics to the host (on the compute stream)
+  auto enqueue_compute = [&](int bi) -> int {
+    const int par = bi & 1;
+    const long r0 = bands[bi].first, r1 = bands[bi].second, nr = r1 - r0;
+    cudaEvent_t *K = ctx->evk[par];
+    CU(cudaEventRecord(K[0], st));
     CU(cudaMemsetAsync(ctx->rqn.p, 0, sizeof(unsigned), st));
     PairArgs A;
     A.rc = rc;
@@ -1148,10 +1587,10 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     A.r1 = r1;
     A.ncols = ncols;
     A.colbase = colbase;
-    A.dist = (double *)ctx->dist.p;
+    A.dist = (double *)ctx->dist.p + par * dslots;
     A.replay_q = (unsigned long long *)ctx->rq.p;
     A.replay_n = (unsigned *)ctx->rqn.p;
-    A.replay_cap = (unsigned long long)band * ncols;
+    A.replay_cap = (unsigned long long)dslots;
     A.counters = (unsigned long long *)ctx->counters.p;
     A.logt = ctx->d_logt;
     // columns: the smallest lower bound of the band's rows onwards
@@ -1160,119 +1599,140 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     const long cblks = (ncols + 31) / 32 - cblk0;
     if (cblks > 0) {
       A.cstart = colbase + cblk0 * 32;
-      dim3 g((unsigned)cblks, (unsigned)((nr + kWarps - 1) / kWarps));
-      if (rc.wplane) {
-        if (rc.gapmm)
-          pair_kernel<true, true><<<g, 256, 0, st>>>(A);
-        else
-          pair_kernel<true, false><<<g, 256, 0, st>>>(A);
-      } else
-        pair_kernel<false, false><<<g, 256, 0, st>>>(A);
-      CU(cudaGetLastError());
-    ctx->launches++;
+      CU(launch_pair(A, cblks, nr, st));
+      ctx->launches++;
     }
-    CU(cudaEventRecord(E[3], st));
-    unsigned nq = 0;
-    CU(cudaMemcpyAsync(&nq, ctx->rqn.p, sizeof nq, cudaMemcpyDeviceToHost, st));
-    CU(cudaStreamSynchronize(st));
-    if (nq) {
-      ReplayArgs R;
-      R.rc = rc;
-      R.cc = (const uint8_t *)ctx->cc.p;
-      R.site = (const SiteEntry *)ctx->site.p;
-      R.q = (const unsigned long long *)ctx->rq.p;
-      R.qn = (const unsigned *)ctx->rqn.p;
-      R.qcap = (unsigned long long)band * ncols;
-      nq = (unsigned)std::min<unsigned long long>(nq, R.qcap);
-      R.r0 = r0;
-      R.ncols = ncols;
-      R.colbase = colbase;
-      R.dist = (double *)ctx->dist.p;
-      R.counters = (unsigned long long *)ctx->counters.p;
-      R.logt = ctx->d_logt;
-      replay_kernel<<<(nq + 127) / 128, 128, 0, st>>>(R);
-      CU(cudaGetLastError());
-    ctx->launches++;
-      sum->pairs_replayed += nq;
-    }
-    CU(cudaEventRecord(E[4], st));
-    RowArgs RA;
-    RA.rc = rc;
-    RA.dist = (const double *)ctx->dist.p;
-    RA.r0 = r0;
-    RA.r1 = r1;
-    RA.ncols = ncols;
-    RA.colbase = colbase;
-    RA.counts = set->d_counts;
-    RA.name_len = set->d_name_len;
-    RA.name_off = set->d_name_off;
-    RA.names = set->d_names;
-    RA.row_bytes = (unsigned long long *)ctx->rbytes.p;
-    RA.row_sum = (double *)ctx->rsum.p;
-    RA.row_w = (double *)ctx->rw.p;
-    RA.row_max = (double *)ctx->rmax.p;
-    RA.row_links = (long long *)ctx->rlinks.p;
-    RA.row_skipped = (long long *)ctx->rskip.p;
-    RA.hist = (unsigned long long *)ctx->hist.p;
-    RA.row_off = (const unsigned long long *)ctx->roff.p;
-    RA.hy = (double *)ctx->hy.p;
-    const unsigned rblocks = (unsigned)((nr + kWarps - 1) / kWarps);
-    rows_kernel<<<rblocks, 256, 0, st>>>(RA);
+    CU(cudaEventRecord(K[1], st));
+    ReplayArgs R;
+    R.rc = rc;
+    R.cc = (const uint8_t *)ctx->cc.p;
+    R.planes = (const uint64_t *)ctx->planes.p;
+    R.site = (const SiteEntry *)ctx->site.p;
+    R.q = (const unsigned long long *)ctx->rq.p;
+    R.qn = (const unsigned *)ctx->rqn.p;
+    R.qcap = (unsigned long long)dslots;
+    R.r0 = r0;
+    R.ncols = ncols;
+    R.colbase = colbase;
+    R.dist = A.dist;
+    R.counters = (unsigned long long *)ctx->counters.p;
+    R.logt = ctx->d_logt;
+    replay_kernel<<<2 * 148, 256, 0, st>>>(R);
     CU(cudaGetLastError());
     ctx->launches++;
-    CU(cudaEventRecord(E[5], st));
-    CU(cudaMemcpyAsync(rbytes.data(), ctx->rbytes.p, nr * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(rsum.data(), ctx->rsum.p, nr * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(rw.data(), ctx->rw.p, nr * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(rmax.data(), ctx->rmax.p, nr * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(rlinks.data(), ctx->rlinks.p, nr * sizeof(long long), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(rskip.data(), ctx->rskip.p, nr * sizeof(long long), cudaMemcpyDeviceToHost, st));
-    CU(cudaStreamSynchronize(st));
-    CU(cudaEventElapsedTime(&ms, E[2], E[3]));
+    CU(cudaEventRecord(K[2], st));
+    RowArgs RA = row_args(bi);
+    stats_kernel<<<dim3((unsigned)((nr + kWarps - 1) / kWarps), (unsigned)maxseg), 256, 0, st>>>(RA);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    sum_kernel<<<(unsigned)((nr + kWarps - 1) / kWarps), 256, 0, st>>>(RA);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    unsigned long long *dtot = (unsigned long long *)ctx->total.p + par;
+    scan_kernel<<<1, 1024, 0, st>>>(RA.seg_bytes, (unsigned long long *)RA.seg_off, nr * maxseg, dtot);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    CU(cudaEventRecord(K[3], st));
+    const HostStats h = host_stats(par);
+    CU(cudaMemcpyAsync(h.sum, RA.row_sum, nr * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(h.w, RA.row_w, nr * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(h.max, RA.seg_max, nr * maxseg * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(h.links, RA.seg_links, nr * maxseg * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(h.skip, RA.seg_skip, nr * maxseg * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(h.total, dtot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CU(cudaEventRecord(K[4], st));
+    return TN93G_OK;
+  };
+  // bands whose text is on its way to the host: parities, oldest first
+  int pend_par[2], pend_n = 0;
+  size_t pend_bytes[2] = {0, 0};
+  bool par_used[2] = {false, false};
+  auto deliver_oldest = [&]() -> int {
+    const int q = pend_par[0];
+    CU(cudaEventSynchronize(ctx->evc1[q]));
+    CU(cudaEventElapsedTime(&ms, ctx->evw0[q], ctx->evw1[q]));
+    ctx->timings[4] += ms;
+    CU(cudaEventElapsedTime(&ms, ctx->evc0[q], ctx->evc1[q]));
+    ctx->timings[5] += ms;
+    pend_par[0] = pend_par[1];
+    pend_n--;
+    if (sink && sink(user, (const char *)ctx->pin2[q], pend_bytes[q])) return TN93G_ESINK;
+    return TN93G_OK;
+  };
+  // statistics of band bi in row order, then its text: written on the compute stream (behind the next band's
+  // kernels) and copied to the host on the copy stream
+  auto finish = [&](int bi) -> int {
+    const int par = bi & 1;
+    const long nr = bands[bi].second - bands[bi].first;
+    cudaEvent_t *K = ctx->evk[par];
+    CU(cudaEventSynchronize(K[4]));
+    CU(cudaEventElapsedTime(&ms, K[0], K[1]));
     ctx->timings[1] += ms;
-    CU(cudaEventElapsedTime(&ms, E[3], E[4]));
+    CU(cudaEventElapsedTime(&ms, K[1], K[2]));
     ctx->timings[2] += ms;
-    CU(cudaEventElapsedTime(&ms, E[4], E[5]));
+    CU(cudaEventElapsedTime(&ms, K[2], K[3]));
     ctx->timings[3] += ms;
+    const HostStats h = host_stats(par);
     // rows in order (swifttn93.cpp:2838-2848)
-    unsigned long long tot = 0;
     for (long r = 0; r < nr; r++) {
-      roff[r] = tot;
-      tot += rbytes[r];
-      links += rlinks[r];
-      skipped += rskip[r];
+      for (long g = r * maxseg; g < (r + 1) * maxseg; g++) {
+        links += h.links[g];
+        skipped += h.skip[g];
+        for (int q = 0; q < 3; q++)
+          if (h.max[g * 3 + q] > max_[q]) max_[q] = h.max[g * 3 + q];
+      }
       for (int q = 0; q < 3; q++) {
-        if (rmax[r * 3 + q] > max_[q]) max_[q] = rmax[r * 3 + q];
-        mean[q] += rsum[r * 3 + q];
-        wc[q] += rw[r * 3 + q];
+        mean[q] += h.sum[r * 3 + q];
+        wc[q] += h.w[r * 3 + q];
       }
     }
-    if (rc.emit && !hyphy && tot) {
-      if (to_device) {
-        TRY(ensure_keep(ctx, ctx->out, dev_off + tot, dev_off));
-      } else {
-        TRY(ensure(ctx, ctx->out, tot));
-        TRY(ensure_pinned(ctx, tot));
-      }
-      CU(cudaMemcpyAsync(ctx->roff.p, roff.data(), nr * sizeof(unsigned long long), cudaMemcpyHostToDevice, st));
-      RA.out = (char *)ctx->out.p + (to_device ? dev_off : 0);
-      CU(cudaEventRecord(E[6], st));
-      write_kernel<<<rblocks, 256, 0, st>>>(RA);
+    const unsigned long long tot = *h.total;
+    if (!(rc.emit && !hyphy && tot)) return TN93G_OK;
+    sum->output_bytes += tot;
+    RowArgs RA = row_args(bi);
+    const dim3 wgrid((unsigned)((nr + kWarps - 1) / kWarps), (unsigned)maxseg);
+    if (to_device) {
+      TRY(ensure_keep(ctx, ctx->out, dev_off + tot, dev_off));
+      RA.out = (char *)ctx->out.p + dev_off;
+      CU(cudaEventRecord(ctx->evw0[0], st));
+      write_kernel<<<wgrid, 256, 0, st>>>(RA);
       CU(cudaGetLastError());
-    ctx->launches++;
-      CU(cudaEventRecord(E[7], st));
-      if (!to_device) CU(cudaMemcpyAsync(ctx->pinned, ctx->out.p, tot, cudaMemcpyDeviceToHost, st));
-      CU(cudaEventRecord(E[8], st));
-      CU(cudaStreamSynchronize(st));
-      CU(cudaEventElapsedTime(&ms, E[6], E[7]));
+      ctx->launches++;
+      CU(cudaEventRecord(ctx->evw1[0], st));
+      CU(cudaEventSynchronize(ctx->evw1[0]));
+      CU(cudaEventElapsedTime(&ms, ctx->evw0[0], ctx->evw1[0]));
       ctx->timings[4] += ms;
-      CU(cudaEventElapsedTime(&ms, E[7], E[8]));
-      ctx->timings[5] += ms;
-      sum->output_bytes += tot;
       dev_off += tot;
-      if (!to_device && sink && sink(user, (const char *)ctx->pinned, tot)) return TN93G_ESINK;
+      return TN93G_OK;
+    }
+    // this parity's text buffers were last used by an older band, already delivered; wait for its copy
+    if (par_used[par]) CU(cudaEventSynchronize(ctx->evc1[par]));
+    TRY(ensure(ctx, ctx->out2[par], tot));
+    TRY(ensure_pinned_at(ctx, ctx->pin2[par], ctx->pin2_n[par], tot));
+    RA.out = (char *)ctx->out2[par].p;
+    CU(cudaEventRecord(ctx->evw0[par], st));
+    write_kernel<<<wgrid, 256, 0, st>>>(RA);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    CU(cudaEventRecord(ctx->evw1[par], st));
+    CU(cudaStreamWaitEvent(ctx->copy_stream, ctx->evw1[par], 0));
+    CU(cudaEventRecord(ctx->evc0[par], ctx->copy_stream));
+    CU(cudaMemcpyAsync(ctx->pin2[par], ctx->out2[par].p, tot, cudaMemcpyDeviceToHost, ctx->copy_stream));
+    CU(cudaEventRecord(ctx->evc1[par], ctx->copy_stream));
+    par_used[par] = true;
+    pend_bytes[par] = tot;
+    pend_par[pend_n++] = par;
+    return TN93G_OK;
+  };
+  const int nb = (int)bands.size();
+  for (int bi = 0; bi <= nb; bi++) {
+    if (bi < nb) TRY(enqueue_compute(bi));
+    if (bi >= 1) {
+      TRY(finish(bi - 1));
+      while (pend_n >= 2) TRY(deliver_oldest());
     }
   }
+  while (pend_n) TRY(deliver_oldest());
   if (hyphy) {
     TRY(ensure(ctx, ctx->rbytes, N * sizeof(unsigned long long)));
     TRY(ensure(ctx, ctx->roff, N * sizeof(unsigned long long)));
@@ -1330,7 +1790,12 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   sum->skipped = skipped;
   sum->logs_ambiguous = (long)counters[0];
   sum->undecided = (long)counters[1];
+  sum->pairs_replayed = (long)counters[2];
   ctx->dev_out_n = dev_off;
+  if (counters[3]) {
+    ctx->err = "internal error: a row's text did not match its counted length";
+    return TN93G_ECUDA;
+  }
   return TN93G_OK;
 }
 
@@ -1530,15 +1995,7 @@ int noalloc_run(const uint8_t *d_codes, long N, long L, const tn93g_opts *opts, 
   A.replay_cap = (unsigned long long)kNaMaxN * kNaMaxN;
   A.counters = counters;
   A.logt = (const LogTable *)(S + kNaLog);
-  dim3 g((unsigned)((N + 31) / 32), (unsigned)((N + kWarps - 1) / kWarps));
-  if (rc.wplane) {
-    if (rc.gapmm)
-      pair_kernel<true, true><<<g, 256, 0, st>>>(A);
-    else
-      pair_kernel<true, false><<<g, 256, 0, st>>>(A);
-  } else
-    pair_kernel<false, false><<<g, 256, 0, st>>>(A);
-  NA(cudaGetLastError());
+  NA(launch_pair(A, (N + 31) / 32, N, st));
   unsigned nq = 0;
   NA(cudaMemcpyAsync(&nq, rqn, sizeof nq, cudaMemcpyDeviceToHost, st));
   NA(cudaStreamSynchronize(st));
@@ -1546,6 +2003,7 @@ int noalloc_run(const uint8_t *d_codes, long N, long L, const tn93g_opts *opts, 
     ReplayArgs R;
     R.rc = rc;
     R.cc = pa.cc;
+    R.planes = pa.planes;
     R.site = (const SiteEntry *)(S + kNaSite);
     R.q = A.replay_q;
     R.qn = rqn;
@@ -1556,7 +2014,7 @@ int noalloc_run(const uint8_t *d_codes, long N, long L, const tn93g_opts *opts, 
     R.dist = d_dist;
     R.counters = counters;
     R.logt = A.logt;
-    replay_kernel<<<(nq + 127) / 128, 128, 0, st>>>(R);
+    replay_kernel<<<(unsigned)std::min<unsigned>(296, (nq + kWarps - 1) / kWarps), 256, 0, st>>>(R);
     NA(cudaGetLastError());
   }
   NA(cudaStreamSynchronize(st));

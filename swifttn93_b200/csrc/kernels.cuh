@@ -66,6 +66,7 @@ struct PairArgs {
 struct ReplayArgs {
   RunConsts rc;
   const uint8_t *cc;
+  const uint64_t *planes;
   const SiteEntry *site;  // [2][18*18]
   const unsigned long long *q;
   const unsigned int *qn;
@@ -84,14 +85,16 @@ struct RowArgs {
   const int32_t *name_len;
   const uint64_t *name_off;
   const char *names;
-  // per band row outputs
-  unsigned long long *row_bytes;
-  double *row_sum, *row_w, *row_max;  // [rows][3]
-  long long *row_links, *row_skipped;
-  unsigned long long *hist;  // [3][200] global
-  const unsigned long long *row_off;  // writer: byte offset of each row in the band's output
+  long maxseg;  // segments per row ([row][segment] arrays below)
+  unsigned long long *seg_bytes;
+  long long *seg_links, *seg_skip;
+  double *seg_max;                    // [row][segment][3]
+  double *row_sum, *row_w;            // [row][3]
+  unsigned long long *hist;           // [3][200] global
+  const unsigned long long *seg_off;  // writer: byte offset of each segment in the band's output
   char *out;
-  double *hy;  // hyphy: [N][N] reported distances (NaN = not reported)
+  double *hy;               // hyphy: [N][N] reported distances (NaN = not reported)
+  unsigned long long *err;  // set when a segment's text would exceed its counted length
 };
 
 }  // namespace tn93

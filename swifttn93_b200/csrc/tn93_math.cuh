@@ -535,6 +535,27 @@ TN_HD int fmt_g(double d, char *out)
   return n;
 }
 
+// length of printf("%g", d) without building the text (the same rules as fmt_g)
+TN_HD int fmt_g_len(double d)
+{
+  const uint64_t b = TBITS(d);
+  const int neg = (int)(b >> 63);
+  const uint64_t a = b & 0x7FFFFFFFFFFFFFFFull;
+  if (a >= 0x7FF0000000000000ull) return neg + 3;  // nan, inf
+  if (a == 0) return neg + 1;
+  const Dec D = decimal6(TDBL(a));
+  uint32_t q = D.q;
+  int nd = 6;
+  while (nd > 1 && q % 10u == 0) {
+    q /= 10u;
+    nd--;
+  }
+  const int X = D.X;
+  if (X < -4 || X >= 6) return neg + nd + (nd > 1 ? 1 : 0) + 2 + ((X <= -100 || X >= 100) ? 3 : 2);
+  if (X >= 0) return neg + (nd > X + 1 ? nd + 1 : X + 1);
+  return neg + 2 + (-X - 1) + nd;
+}
+
 // decimal digits of a non-negative integer below 10^18; returns the length
 TN_HD int fmt_long(long v, char *out)
 {

@@ -83,6 +83,10 @@ int main(int argc, char **argv)
       default: x = urand() * 1e-4; break;
     }
     int la = fmt_g(x, a);
+    if (fmt_g_len(x) != la) {
+      if (g_bad < 5) fprintf(stderr, "fmt_g_len mismatch %a: %d vs %d\n", x, fmt_g_len(x), la);
+      g_bad++;
+    }
     a[la] = 0;
     snprintf(b, sizeof b, "%g", x);
     g_n++;
