@@ -30,6 +30,7 @@ extern "C" {
 #define TN93G_ETIMEOUT (-6) /* a bounded device wait gave up (device error word set) */
 #define TN93G_ETOOBIG (-7)  /* alignment too long for the 32-bit x16 count lanes (L >= 2^25) */
 #define TN93G_ESCRATCH (-8) /* input beyond the fixed limits of tn93g_pair_distances_noalloc */
+#define TN93G_EFASTA (-9)   /* tn93g_read_fasta refused the file (tn93's message is returned with it) */
 
 /* Ambiguity modes, numbered as tn93's RESOLVE/AVERAGE/SKIP/GAPMM/SUBSET (solver/refkernel.h:14-18). */
 #define TN93G_RESOLVE 0
@@ -122,6 +123,55 @@ long tn93g_last_launches(tn93g_ctx *ctx);
  * [0] pack, [1] pair kernel, [2] site-order replay, [3] row reductions, [4] output formatting,
  * [5] device->host copies, [6] whole run. Returns the number of entries written (<= n). */
 int tn93g_last_timings(tn93g_ctx *ctx, double *ms, int n);
+
+/* ---- FASTA ----
+ * tn93's reader (swifttn93.cpp:259-406) on a file held in memory: out receives malloc'ed codes (0..17 in the order
+ * "ACGTURYSWKMBDHVN?-", row-major n x L), copy numbers (parsed after the last counts_sep), names and their offsets
+ * and lengths, in the layout tn93g_upload takes. expect_len > 0 requires that sequence length (a second file, as
+ * tn93 -s reads it after the first). On a refusal it returns TN93G_EFASTA with the message tn93 prints in msg.
+ * Replaces: read_fasta (swifttn93.cpp:292-406), which tn93 runs on a FILE*. */
+typedef struct tn93g_alignment {
+  uint8_t *codes;
+  long n, L;
+  long *copy_counts;
+  char *names;
+  size_t *name_off;
+  long *name_len;
+} tn93g_alignment;
+
+int tn93g_read_fasta(const char *bytes, size_t nbytes, long expect_len, char counts_sep, tn93g_alignment *out,
+                     char *msg, size_t msg_cap);
+void tn93g_alignment_free(tn93g_alignment *a);
+
+/* ---- the -s mode as a service: a resident reference and batches of queries ----
+ * A server keeps one reference alignment packed on the device and runs batches of query alignments against it.
+ * Each query's result is exactly the distance file body and summary of `tn93 -s QUERY.fa REF.fa` with the
+ * server's options: rows are the reference's sequences and columns the query's (swifttn93.cpp:2321-2322, 2392),
+ * and csvn indices are global (reference first, then the query). Replaces: nothing in the reference, which reads
+ * both files on every call (swifttn93.cpp:2243-2254); the per-query semantics are its -s mode. */
+typedef struct tn93g_server tn93g_server;
+
+/* Receives query q's whole distance file body (bytes valid only during the call); non-zero aborts. */
+typedef int (*tn93g_query_sink)(void *user, int query, const char *bytes, size_t n);
+
+/* Packs the reference (arguments as tn93g_upload) and allocates, within the context's HBM budget, every per-batch
+ * buffer for batches of up to max_batch_sequences query sequences in up to max_batch_queries queries (about
+ * 16 bytes per reference x query-sequence pair and 104 bytes per reference sequence x query); only the text
+ * buffer grows later. opts->format must be csv or csvn; the server's options apply to every batch. */
+int tn93g_server_create(tn93g_ctx *ctx, tn93g_server **out, const uint8_t *codes, long N, long L,
+                        const long *copy_counts, const char *names, const size_t *name_off, const long *name_len,
+                        const tn93g_opts *opts, long max_batch_sequences, int max_batch_queries);
+/* Runs nq query alignments (each of the reference's length L, as tn93g_read_fasta returns them; at most the
+ * server's capacity) in one batch; sums[q] receives query q's summary (its pairwise count is reference N x query
+ * n; engine counters are reported in sums[0]). */
+int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries, tn93g_query_sink sink, void *user,
+                       tn93g_summary *sums);
+void tn93g_server_destroy(tn93g_server *srv);
+
+/* The JSON summary tn93 prints for one run (swifttn93.cpp:2914-2958), byte for byte; n2 = 0 and second_file = 0
+ * for a single input file. Returns the length (the text is NUL-terminated when it fits in cap). */
+size_t tn93g_summary_json(const tn93g_summary *s, unsigned long n1, unsigned long n2, int second_file, int fst,
+                          char *buf, size_t cap);
 
 /* Allocation-free pair distances. This entry point has no counterpart in the reference; it exists for callers
  * that cannot allocate device memory -- code running while a CUDA graph is being captured, plugin hosts whose

@@ -542,6 +542,20 @@ int main(int argc, char **argv)
     if (read_fasta(A.in2, &S, &L, A.counts_sep)) return 1;
     n2 = (unsigned long)S.N - n1;
   }
+  /* test hook: TN93_ORACLE_DUMP=PATH writes the parsed alignment (name, copy number and codes of every sequence,
+     one line each) to PATH and stops, so a reader can be compared with this one */
+  const char *dump = getenv("TN93_ORACLE_DUMP");
+  if (dump) {
+    FILE *D = fopen(dump, "wb");
+    if (!D) return 1;
+    for (long i = 0; i < S.N; i++) {
+      fprintf(D, "%s\t%ld\t", S.names[i], S.counts[i]);
+      for (long k = 0; k < L; k++) fputc("ACGTURYSWKMBDHVN?-"[S.codes[(size_t)i * L + k]], D);
+      fputc('\n', D);
+    }
+    fclose(D);
+    return 0;
+  }
   const int fst = A.in2 && A.fst, cross = A.in2 && !fst;
   const int report_self = !A.in2 && A.self && !A.count;
   const long N = S.N;

@@ -28,7 +28,9 @@ FORMATS = {"csv": 0, "csvn": 1, "hyphy": 2}
 # symbols declared in include/tn93g.h
 EXPORTS = ("tn93g_create", "tn93g_destroy", "tn93g_strerror", "tn93g_last_cuda_error", "tn93g_upload",
            "tn93g_free_set", "tn93g_run", "tn93g_run_to_device", "tn93g_stream", "tn93g_last_launches",
-           "tn93g_last_timings", "tn93g_pair_distances_noalloc", "tn93g_noalloc_last_error")
+           "tn93g_last_timings", "tn93g_pair_distances_noalloc", "tn93g_noalloc_last_error", "tn93g_read_fasta",
+           "tn93g_alignment_free", "tn93g_server_create", "tn93g_server_batch", "tn93g_server_destroy",
+           "tn93g_summary_json")
 
 
 class _Opts(C.Structure):
@@ -45,7 +47,14 @@ class _Summary(C.Structure):
                 ("output_bytes", C.c_size_t)]
 
 
+class _Alignment(C.Structure):
+    _fields_ = [("codes", C.POINTER(C.c_uint8)), ("n", C.c_long), ("L", C.c_long),
+                ("copy_counts", C.POINTER(C.c_long)), ("names", C.POINTER(C.c_char)),
+                ("name_off", C.POINTER(C.c_size_t)), ("name_len", C.POINTER(C.c_long))]
+
+
 _SINK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_char), C.c_size_t)
+_QSINK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_char), C.c_size_t)
 
 _lib = None
 
@@ -77,6 +86,18 @@ def load_library(path: Path | str = LIB_PATH):
     lib.tn93g_stream.argtypes = [C.c_void_p]
     lib.tn93g_last_launches.restype = C.c_long
     lib.tn93g_last_launches.argtypes = [C.c_void_p]
+    lib.tn93g_read_fasta.argtypes = [C.c_char_p, C.c_size_t, C.c_long, C.c_char, C.POINTER(_Alignment), C.c_char_p,
+                                     C.c_size_t]
+    lib.tn93g_alignment_free.argtypes = [C.POINTER(_Alignment)]
+    lib.tn93g_server_create.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_void_p, C.c_long, C.c_long,
+                                        C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(_Opts), C.c_long,
+                                        C.c_int]
+    lib.tn93g_server_batch.argtypes = [C.c_void_p, C.c_int, C.POINTER(_Alignment), _QSINK, C.c_void_p,
+                                       C.POINTER(_Summary)]
+    lib.tn93g_server_destroy.argtypes = [C.c_void_p]
+    lib.tn93g_summary_json.restype = C.c_size_t
+    lib.tn93g_summary_json.argtypes = [C.POINTER(_Summary), C.c_ulong, C.c_ulong, C.c_int, C.c_int, C.c_char_p,
+                                       C.c_size_t]
     _lib = lib
     return lib
 
@@ -131,10 +152,60 @@ class Summary:
     undecided: int
     output_bytes: int
     timings_ms: dict = field(default_factory=dict)
+    raw: object = field(default=None, repr=False)
+
+    def json(self, n1: int, n2: int = 0, second_file: bool = False, fst: bool = False) -> bytes:
+        """tn93's JSON summary of this run, byte for byte (tn93g_summary_json)."""
+        lib = load_library()
+        n = lib.tn93g_summary_json(C.byref(self.raw), n1, n2, int(second_file), int(fst), None, 0)
+        buf = C.create_string_buffer(n + 1)
+        lib.tn93g_summary_json(C.byref(self.raw), n1, n2, int(second_file), int(fst), buf, n + 1)
+        return buf.raw[:n]
 
 
 class Tn93Error(RuntimeError):
     pass
+
+
+class FastaError(Tn93Error):
+    """The FASTA reader refused the input; str(e) is the message tn93 prints (it then exits with status 1)."""
+
+
+class Fasta:
+    """A FASTA file parsed by tn93's reader (tn93g_read_fasta): codes, names, copy numbers in host memory."""
+
+    def __init__(self, data: bytes, expect_len: int = 0, counts_sep: str = ":"):
+        lib = load_library()
+        self._a = _Alignment()
+        msg = C.create_string_buffer(512)
+        rc = lib.tn93g_read_fasta(data, len(data), int(expect_len), counts_sep.encode()[:1], C.byref(self._a), msg,
+                                  512)
+        if rc == -9:
+            raise FastaError(msg.value.decode(errors="replace"))
+        if rc != 0:
+            raise Tn93Error(f"tn93g error {rc}: {lib.tn93g_strerror(rc).decode()}")
+        self.n, self.L = self._a.n, self._a.L
+
+    @property
+    def codes(self) -> np.ndarray:
+        return np.ctypeslib.as_array(self._a.codes, shape=(self.n * self.L,)).reshape(self.n, self.L).copy()
+
+    @property
+    def counts(self) -> np.ndarray:
+        return np.ctypeslib.as_array(self._a.copy_counts, shape=(self.n,)).copy()
+
+    @property
+    def names(self) -> list:
+        off = np.ctypeslib.as_array(self._a.name_off, shape=(self.n,))
+        ln = np.ctypeslib.as_array(self._a.name_len, shape=(self.n,))
+        return [C.string_at(C.addressof(self._a.names.contents) + int(o), int(k)) for o, k in zip(off, ln)]
+
+    def __del__(self):
+        try:
+            if self._a.codes:
+                load_library().tn93g_alignment_free(C.byref(self._a))
+        except Exception:  # noqa: BLE001
+            pass
 
 
 @dataclass
@@ -230,13 +301,73 @@ class Engine:
                                                                  for q in range(3)], dtype=np.uint64),
                        pairs_replayed=S.pairs_replayed, logs_ambiguous=S.logs_ambiguous, undecided=S.undecided,
                        output_bytes=S.output_bytes,
-                       timings_ms={self.STAGES[q]: t[q] for q in range(k)})
+                       timings_ms={self.STAGES[q]: t[q] for q in range(k)}, raw=S)
         return summ
 
     def close(self):
         if self.ctx:
             self.lib.tn93g_destroy(self.ctx)
             self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+
+def _plain_summary(S) -> Summary:
+    return Summary(pairwise=S.pairwise, skipped=S.skipped, links=S.links, max=list(S.max), mean=list(S.mean),
+                   weighted=list(S.weighted), hist=np.array([[S.hist[q][k] for k in range(200)] for q in range(3)],
+                                                            dtype=np.uint64),
+                   pairs_replayed=S.pairs_replayed, logs_ambiguous=S.logs_ambiguous, undecided=S.undecided,
+                   output_bytes=S.output_bytes, raw=S)
+
+
+class ResidentReference:
+    """A reference alignment kept packed on the device, run against batches of query alignments
+    (tn93g_server_*). Each query's result is the distance file body and summary of
+    `tn93 -s QUERY.fa REF.fa` with this server's options (rows = reference, columns = the query)."""
+
+    def __init__(self, engine: Engine, ref: Fasta, opts: Options, max_batch_sequences: int = 4096,
+                 max_batch_queries: int = 256):
+        self.engine, self.lib, self.ref, self.opts = engine, engine.lib, ref, opts
+        self.max_batch_sequences, self.max_batch_queries = max_batch_sequences, max_batch_queries
+        self.srv = C.c_void_p()
+        a = ref._a
+        o = opts.to_c()
+        engine._check(self.lib.tn93g_server_create(
+            engine.ctx, C.byref(self.srv), C.cast(a.codes, C.c_void_p), a.n, a.L, C.cast(a.copy_counts, C.c_void_p),
+            C.cast(a.names, C.c_void_p), C.cast(a.name_off, C.c_void_p), C.cast(a.name_len, C.c_void_p),
+            C.byref(o), int(max_batch_sequences), int(max_batch_queries)))
+
+    def batch(self, queries: list) -> list:
+        """Runs the queries (Fasta objects of the reference's length) in one batch: [(body bytes, Summary)]."""
+        nq = len(queries)
+        arr = (_Alignment * nq)(*[q._a for q in queries])
+        sums = (_Summary * nq)()
+        bodies = [[] for _ in range(nq)]
+
+        def _sink(_user, q, ptr, n):
+            try:
+                bodies[q].append(C.string_at(ptr, n))
+                return 0
+            except Exception:  # noqa: BLE001 - an exception must not unwind through C
+                return 1
+
+        cb = _QSINK(_sink)
+        self.engine._check(self.lib.tn93g_server_batch(self.srv, nq, arr, cb, None, sums))
+        out = []
+        for q in range(nq):
+            S = _Summary()
+            C.memmove(C.byref(S), C.byref(sums[q]), C.sizeof(_Summary))
+            out.append((b"".join(bodies[q]), _plain_summary(S)))
+        return out
+
+    def close(self):
+        if self.srv:
+            self.lib.tn93g_server_destroy(self.srv)
+            self.srv = C.c_void_p()
 
     def __del__(self):
         try:

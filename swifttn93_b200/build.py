@@ -22,7 +22,7 @@ HOSTCXX = "g++"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 DEVICE_SOURCES = ["engine.cu"]
-HOST_SOURCES = ["tables.cpp", "logtable.cpp"]
+HOST_SOURCES = ["tables.cpp", "logtable.cpp", "summary_json.cpp", "fasta.cpp"]
 HEADERS = ["kernels.cuh", "tn93_math.cuh", "tables.h"]
 
 

@@ -1,7 +1,7 @@
 // cli.cpp -- the tn93 v1.1.0 command line on top of the B200 engine (libtn93g.so).
 //
 // Host side, as in the reference: option parsing with tn93's semantics and messages (argparse.cpp:20-446),
-// the FASTA reader's acceptance rules and error messages (swifttn93.cpp:259-406), the unsupported-option
+// the FASTA reader (tn93g_read_fasta, swifttn93.cpp:259-406), the unsupported-option
 // guard (swifttn93.cpp:2226-2233), the header line (swifttn93.cpp:2307-2316) and the JSON summary printed
 // with the same iostream statements as tn93 (swifttn93.cpp:2900-2963), so the bytes on stdout match. The
 // pair engine, its reductions and the distance-file text run on the GPU through include/tn93g.h.
@@ -11,6 +11,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <iomanip>
 #include <iostream>
 #include <string>
@@ -186,112 +187,37 @@ struct Alignment {
   long N = 0;
 };
 
-signed char g_code[256];  // code of toupper(byte), -1 for bytes the reader drops
-
-// The reader's rules (swifttn93.cpp:292-406): '>' or '#' opens a record whose name runs to the end of the
-// line; sequence bytes map through the alphabet case-insensitively, other bytes are dropped; every sequence
-// must have the first one's length. Returns false after printing tn93's message for a reader error; exits
-// with status 1 where tn93 exits.
+// Reads one FASTA with tn93's reader (tn93g_read_fasta) and appends it to A; every file after the first must
+// have the first one's sequence length. Returns false after printing tn93's message (tn93 then exits with 1).
 bool read_fasta(FILE *F, Alignment &A, long &first_len, char sep)
 {
-  std::vector<unsigned char> buf;
+  std::vector<char> buf;
   {
-    unsigned char tmp[1 << 16];
+    char tmp[1 << 16];
     size_t r;
     while ((r = fread(tmp, 1, sizeof tmp, F)) > 0) buf.insert(buf.end(), tmp, tmp + r);
   }
-  const unsigned char *p = buf.data(), *end = p + buf.size();
-  int state = 0;
-  size_t seq_begin = A.codes.size();
-  auto close_sequence = [&]() {
-    const long len = (long)(A.codes.size() - seq_begin);
-    if (A.N == 0) {
-      first_len = len;
-      if (first_len <= 0) {
-        std::cerr << "First sequence length must be positive." << std::endl;
-        exit(1);
-      }
-    } else if (len != first_len) {
-      std::cerr << "All sequences must have the same length (" << first_len << "), but sequence '"
-                << (A.names.data() + A.name_off.back()) << "' had length " << len;
-      exit(1);
-    }
-    A.N++;
-  };
-  while (p < end) {
-    if (state == 0) {
-      while (p < end && *p != '>' && *p != '#') p++;
-      if (p == end) break;
-      p++;
-      state = 1;
-      continue;
-    }
-    if (state == 1) {
-      const unsigned char *q = p;
-      while (q < end && *q != '\n' && *q != '\r') q++;
-      const size_t begin = A.names.size();
-      A.names.insert(A.names.end(), p, q);
-      if (q == end) {
-        p = q;
-        break;
-      }
-      p = q + 1;
-      const long len = (long)(A.names.size() - begin);
-      A.names.push_back('\0');
-      if (len <= 0) {
-        std::cerr << "Sequence names must be non-empty." << std::endl;
-        return false;
-      }
-      // copy number after the last separator that is neither the name's first nor its last character
-      unsigned long count = 1;
-      if (len >= 3) {
-        const char *nm = A.names.data() + begin;
-        long k = len - 2;
-        while (k >= 1 && nm[k] != sep) k--;
-        if (k >= 1) count = (unsigned long)(long)(int)strtol(nm + k + 1, nullptr, 10);
-        if (count < 1) count = 1;
-      }
-      A.counts.push_back((long)count);
-      A.name_off.push_back(begin);
-      A.name_len.push_back(len);
-      state = 2;
-      seq_begin = A.codes.size();
-      continue;
-    }
-    while (p < end) {
-      const signed char v = g_code[*p];
-      if (v >= 0) {
-        A.codes.push_back((uint8_t)v);
-        p++;
-        continue;
-      }
-      if (*p == '>' || *p == '#') break;
-      p++;
-    }
-    if (p == end) break;
-    p++;
-    close_sequence();
-    state = 1;
+  tn93g_alignment R;
+  char msg[512];
+  const int rc = tn93g_read_fasta(buf.data(), buf.size(), A.N ? first_len : 0, sep, &R, msg, sizeof msg);
+  if (rc != TN93G_OK) {
+    std::cerr << (rc == TN93G_EFASTA ? msg : tn93g_strerror(rc));
+    return false;
   }
-  if (state == 2) {
-    close_sequence();
-    return true;
+  if (!A.N) first_len = R.L;
+  const size_t base = A.names.size();
+  size_t nb = 0;
+  for (long k = 0; k < R.n; k++) nb = std::max(nb, R.name_off[k] + (size_t)R.name_len[k] + 1);
+  A.names.insert(A.names.end(), R.names, R.names + nb);
+  A.codes.insert(A.codes.end(), R.codes, R.codes + (size_t)R.n * R.L);
+  for (long k = 0; k < R.n; k++) {
+    A.name_off.push_back(base + R.name_off[k]);
+    A.name_len.push_back(R.name_len[k]);
+    A.counts.push_back(R.copy_counts[k]);
   }
-  std::cerr << "Unexpected end of file: state " << state << std::endl;
-  return false;
-}
-
-void dump_histogram(std::ostream *o, const char *tag, const unsigned long *hist)
-{
-  if (tag)
-    (*o) << "\t\"Histogram " << tag << "\" : [";
-  else
-    (*o) << "\t\"Histogram\" : [";
-  for (unsigned long k = 0; k < 200; k++) {
-    if (k) (*o) << ',';
-    (*o) << '[' << (k + 1.) / 200 << ',' << hist[k] << ']';
-  }
-  (*o) << "]" << std::endl;
+  A.N += R.n;
+  tn93g_alignment_free(&R);
+  return true;
 }
 
 int write_sink(void *user, const char *bytes, size_t n)
@@ -312,11 +238,6 @@ int main(int argc, char **argv)
   if (o.hamming) {
     std::cerr << "swifttn93: -H (Hamming early exit) is not supported" << std::endl;
     return 1;
-  }
-  for (int c = 0; c < 256; c++) g_code[c] = -1;
-  for (int c = 0; c < 256; c++) {
-    const char *f = strchr(kValid, toupper(c));
-    if (f && toupper(c)) g_code[c] = (signed char)(f - kValid);
   }
   unsigned char subset[18] = {0};
   for (unsigned char ch : o.subset) {
@@ -397,41 +318,14 @@ int main(int argc, char **argv)
               << " links found, " << std::setw(12) << std::setprecision(3) << (double)pairwise << " evals)";
   std::cerr << std::endl;
   std::ostream *os = o.out == stdout ? &std::cerr : &std::cout;
-  // tn93's summary statements (swifttn93.cpp:2914-2958)
-  (*os) << "{" << std::endl;
-  (*os) << '\t' << "\"Actual comparisons performed\" :" << pairwise - S.skipped << ',' << std::endl;
-  (*os) << "\t\"Comparisons accounting for copy numbers \" :" << (S.weighted[0] + S.weighted[1] + S.weighted[2]) << ','
-        << std::endl;
-  (*os) << "\t\"Total comparisons possible\" : " << pairwise << ',' << std::endl;
-  (*os) << "\t\"Links found\" : " << S.links << ',' << std::endl;
-  (*os) << "\t\"Maximum distance\" : " << S.max[0] << ',' << std::endl;
-  if (!o.in2) {
-    (*os) << "\t\"Sequences\" : " << N << ',' << std::endl;
-  } else {
-    (*os) << "\t\"Sequences in first file\" : " << n1 << ',' << std::endl;
-    (*os) << "\t\"Sequences in second file\" : " << n2 << ',' << std::endl;
+  // tn93's summary (swifttn93.cpp:2914-2958), printed by the library's formatter
+  {
+    const size_t len = tn93g_summary_json(&S, o.in2 ? n1 : N, n2, o.in2 != nullptr, fst, nullptr, 0);
+    std::string js(len + 1, '\0');
+    tn93g_summary_json(&S, o.in2 ? n1 : N, n2, o.in2 != nullptr, fst, &js[0], js.size());
+    os->write(js.data(), (std::streamsize)len);
+    os->flush();
   }
-  if (fst) {
-    const char *keys[4] = {"File 1", "File 2", "Between", "Combined"};
-    for (int k = 0; k < 3; k++)
-      (*os) << "\t\"Mean distance " << keys[k] << "\" : " << S.mean[k] / S.weighted[k] << ',' << std::endl;
-    const double meta = (S.mean[0] + S.mean[1] + S.mean[2]) / (S.weighted[0] + S.weighted[1] + S.weighted[2]),
-                 intra = (S.mean[0] + S.mean[1]) / (S.weighted[0] + S.weighted[1]),
-                 piD = S.mean[2] / S.weighted[2] - intra;
-    (*os) << "\t\"Mean distance [intra] " << "\" : " << intra << ',' << std::endl;
-    (*os) << "\t\"Mean distance [combined]" << "\" : " << meta << ',' << std::endl;
-    (*os) << "\t\"F_ST\" : " << piD / (intra + piD) << ',' << std::endl;
-    for (int k = 0; k < 3; k++) {
-      dump_histogram(os, keys[k], S.hist[k]);
-      (*os) << ',' << std::endl;
-    }
-    for (int k = 0; k < 200; k++) S.hist[0][k] += S.hist[1][k] + S.hist[2][k];
-    dump_histogram(os, keys[3], S.hist[0]);
-  } else {
-    (*os) << "\t\"Mean distance\" : " << S.mean[0] / S.weighted[0] << ',' << std::endl;
-    dump_histogram(os, nullptr, S.hist[0]);
-  }
-  (*os) << '}' << std::endl;
   if (o.count)
     fprintf(o.out, "Found %ld links among %ld pairwise comparisons\n", S.links, (long)(pairwise - S.skipped));
   if (o.out != stdout) fclose(o.out);

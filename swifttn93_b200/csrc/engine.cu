@@ -590,9 +590,20 @@ __global__ void __launch_bounds__(256) stats_kernel(RowArgs a)
   const long i = a.r0 + blockIdx.x * (long)kWarps + warp;
   const int sg = blockIdx.y;
   if (i < a.r1) {
-    const long r = i - a.r0, slot = r * a.maxseg + sg;
-    const long lb = rc.cross ? rc.n1 : i + 1;
-    const long c0 = lb + (long)sg * kSeg, c1 = min(rc.N, c0 + kSeg);
+    const long r = i - a.r0;
+    long slot, c0, c1;
+    if (a.seg_cols) {
+      slot = sg * a.nrows + r;
+      c0 = a.seg_cols[sg];
+      c1 = a.seg_cols[sg + 1];
+    } else {
+      slot = r * a.maxseg + sg;
+      const long lb = rc.cross ? rc.n1 : i + 1;
+      c0 = lb + (long)sg * kSeg;
+      c1 = min(rc.N, c0 + kSeg);
+    }
+    // csvn prints a query column's index in its own run (reference rows first, then the query's sequences)
+    const long jshift = a.seg_cols ? c0 - rc.n1 : 0;
     const long cnt_i = a.counts[i];
     const int nli = a.name_len[i];
     const int dli = rc.format == 1 ? digits_of(i) : 0;
@@ -623,7 +634,7 @@ __global__ void __launch_bounds__(256) stats_kernel(RowArgs a)
         if (rc.emit) {
           if (rc.format != 2) {
             const int gl = fmt_g_len(v.thisD);
-            bytes += rc.format == 0 ? nli + a.name_len[j] + gl + 3 : dli + digits_of(j) + gl + 3;
+            bytes += rc.format == 0 ? nli + a.name_len[j] + gl + 3 : dli + digits_of(j - jshift) + gl + 3;
           } else {
             a.hy[(size_t)i * rc.N + j] = v.thisD;
             a.hy[(size_t)j * rc.N + i] = v.thisD;
@@ -655,11 +666,12 @@ __global__ void __launch_bounds__(256) stats_kernel(RowArgs a)
     }
   }
   __syncthreads();
+  unsigned long long *hist = a.seg_cols ? a.hist + (size_t)sg * 3 * kHistBins : a.hist;
   for (int t = threadIdx.x; t < 3 * kHistBins; t += blockDim.x)
-    if (sh[t]) atomicAdd(&a.hist[t], sh[t]);
+    if (sh[t]) atomicAdd(&hist[t], sh[t]);
 }
 
-// one warp per row: tn93's row sums in column order (swifttn93.cpp:2594-2602); lane 0 adds each chunk's terms in
+// one warp per row (or per (row, query segment)): tn93's row sums in column order (swifttn93.cpp:2594-2602); lane 0 adds each chunk's terms in
 // order. The self-pair weights come first, as tn93 adds them when the row starts (swifttn93.cpp:2405-2415).
 __global__ void __launch_bounds__(256) sum_kernel(RowArgs a)
 {
@@ -671,6 +683,12 @@ __global__ void __launch_bounds__(256) sum_kernel(RowArgs a)
   if (i >= a.r1) return;
   const long cnt_i = a.counts[i];
   double s0 = 0., s1 = 0., s2 = 0., w0 = 0., w1 = 0., w2 = 0.;
+  long lb = rc.cross ? rc.n1 : i + 1, cend = rc.N, out_row = i - a.r0;
+  if (a.seg_cols) {
+    lb = a.seg_cols[blockIdx.y];
+    cend = a.seg_cols[blockIdx.y + 1];
+    out_row = (long)blockIdx.y * a.nrows + (i - a.r0);
+  }
   if (!rc.cross && cnt_i > 1) {
     const unsigned long long svs = (unsigned long long)(cnt_i * (cnt_i - 1l)) >> 1;
     if (i < rc.n1)
@@ -678,14 +696,13 @@ __global__ void __launch_bounds__(256) sum_kernel(RowArgs a)
     else
       w1 += (double)svs;
   }
-  const long lb = rc.cross ? rc.n1 : i + 1;
   const double *drow = a.dist + (size_t)(i - a.r0) * a.ncols - a.colbase;
-  for (long j0 = lb; j0 < rc.N; j0 += 32) {
+  for (long j0 = lb; j0 < cend; j0 += 32) {
     const long j = j0 + lane;
     bool inc = false;
     double term = 0., wl = 0.;
     int bin = 0;
-    if (j < rc.N) {
+    if (j < cend) {
       const double raw = drow[j];
       if ((uint64_t)__double_as_longlong(raw) != kSkipBits) {
         const double t = raw <= 0. ? 0. : raw;
@@ -701,7 +718,7 @@ __global__ void __launch_bounds__(256) sum_kernel(RowArgs a)
     sbin[warp][lane] = inc ? (unsigned char)bin : (unsigned char)255;
     __syncwarp();
     if (lane == 0) {
-      const int n = (int)min(32l, rc.N - j0);
+      const int n = (int)min(32l, cend - j0);
       if (!rc.fst) {
         for (int l = 0; l < n; l++)
           if (sbin[warp][l] == 0) {
@@ -727,7 +744,7 @@ __global__ void __launch_bounds__(256) sum_kernel(RowArgs a)
     __syncwarp();
   }
   if (lane == 0) {
-    const long r = i - a.r0;
+    const long r = out_row;
     a.row_sum[r * 3] = s0;
     a.row_sum[r * 3 + 1] = s1;
     a.row_sum[r * 3 + 2] = s2;
@@ -744,8 +761,8 @@ __device__ __forceinline__ char *put_bytes(char *o, const char *s, int n)
 }
 
 // the text of one reported pair at o (generic pointer: shared staging or global)
-__device__ __forceinline__ void put_line(char *o, const RowArgs &a, long i, long j, const char *ni, int nli,
-                                         const char *g, int gl)
+__device__ __forceinline__ void put_line(char *o, const RowArgs &a, long i, long j, long jshift, const char *ni,
+                                         int nli, const char *g, int gl)
 {
   const RunConsts &rc = a.rc;
   if (rc.format == 0) {
@@ -758,7 +775,7 @@ __device__ __forceinline__ void put_line(char *o, const RowArgs &a, long i, long
     int n = fmt_long(i, t);
     o = put_bytes(o, t, n);
     *o++ = rc.delim;
-    n = fmt_long(j, t);
+    n = fmt_long(j - jshift, t);
     o = put_bytes(o, t, n);
     *o++ = rc.delim;
   }
@@ -805,10 +822,19 @@ __global__ void __launch_bounds__(256) write_kernel(RowArgs a)
   const long i = a.r0 + blockIdx.x * (long)kWarps + warp;
   const int sg = blockIdx.y;
   if (i >= a.r1) return;
-  const long slot = (i - a.r0) * a.maxseg + sg;
+  long slot, c0, c1;
+  if (a.seg_cols) {
+    slot = sg * a.nrows + (i - a.r0);
+    c0 = a.seg_cols[sg];
+    c1 = a.seg_cols[sg + 1];
+  } else {
+    slot = (i - a.r0) * a.maxseg + sg;
+    const long lb = rc.cross ? rc.n1 : i + 1;
+    c0 = lb + (long)sg * kSeg;
+    c1 = min(rc.N, c0 + kSeg);
+  }
   if (a.seg_bytes[slot] == 0) return;
-  const long lb = rc.cross ? rc.n1 : i + 1;
-  const long c0 = lb + (long)sg * kSeg, c1 = min(rc.N, c0 + kSeg);
+  const long jshift = a.seg_cols ? c0 - rc.n1 : 0;
   const long cnt_i = a.counts[i];
   const int nli = a.name_len[i];
   const char *ni = a.names + a.name_off[i];
@@ -860,7 +886,7 @@ __global__ void __launch_bounds__(256) write_kernel(RowArgs a)
     int gl = 0, len = 0;
     if (put) {
       gl = fmt_g(v.thisD, g);
-      len = rc.format == 0 ? nli + a.name_len[j] + gl + 3 : dli + digits_of(j) + gl + 3;
+      len = rc.format == 0 ? nli + a.name_len[j] + gl + 3 : dli + digits_of(j - jshift) + gl + 3;
     }
     int pre = len;
     for (int o = 1; o < 32; o <<= 1) {
@@ -876,12 +902,12 @@ __global__ void __launch_bounds__(256) write_kernel(RowArgs a)
         S.over = true;
         break;
       }
-      if (put) put_line((char *)(S.gpos + pre - len), a, i, j, ni, nli, g, gl);
+      if (put) put_line((char *)(S.gpos + pre - len), a, i, j, jshift, ni, nli, g, gl);
       __syncwarp();
       S.gpos += total;
       S.head = (int)(S.gpos & 15);
     } else {
-      if (put) put_line(S.buf + S.head + S.fill + (pre - len), a, i, j, ni, nli, g, gl);
+      if (put) put_line(S.buf + S.head + S.fill + (pre - len), a, i, j, jshift, ni, nli, g, gl);
       __syncwarp();
       S.fill += total;
     }
@@ -1147,6 +1173,7 @@ const char *tn93g_strerror(int code)
     case TN93G_ETIMEOUT: return "device wait timed out";
     case TN93G_ETOOBIG: return "alignment too long (L >= 2^25)";
     case TN93G_ESCRATCH: return "alignment exceeds the allocation-free entry point's limits (N <= 512, L <= 4096)";
+    case TN93G_EFASTA: return "the FASTA reader refused the input";
     default: return "unknown error";
   }
 }
@@ -1563,6 +1590,8 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     RA.row_w = (double *)ctx->rw.p + par * band * 3;
     RA.hist = (unsigned long long *)ctx->hist.p;
     RA.seg_off = (const unsigned long long *)ctx->roff.p + par * nseg;
+    RA.seg_cols = nullptr;
+    RA.nrows = RA.r1 - RA.r0;
     RA.out = nullptr;
     RA.hy = (double *)ctx->hy.p;
     RA.err = (unsigned long long *)ctx->counters.p + 3;
@@ -2042,5 +2071,520 @@ int tn93g_pair_distances_noalloc(const uint8_t *d_codes, long N, long L, const t
 }
 
 const char *tn93g_noalloc_last_error(void) { return g_na_err; }
+
+}  // extern "C"
+
+//================================================================================================== resident-reference server
+// The -s mode as a service: a reference alignment stays packed on the device (bit planes, codes, sparse events,
+// with room after it for query sequences) and batches of query alignments are run against it. One batch is one
+// cross run (rows = reference, columns = the batch's queries, as tn93 -s QUERY REF orders them,
+// swifttn93.cpp:2321-2322, 2392) whose stats, sums and text are segmented by query, so every query gets the
+// distance file and summary of its own tn93 run. Columns are not folded (a fold must hold for every query that
+// will ever come), which changes no result.
+namespace {
+
+// per query: links, skips and maxima over its segments, and tn93's row-order mean and weights (lane 0 adds the
+// rows' sums in row order, as tn93's writer does, swifttn93.cpp:2838-2848); one warp per query
+__global__ void query_reduce_kernel(RowArgs a, int nq, double *qout /* [nq][9]: max, mean, weighted */,
+                                    long long *qlinks /* [nq][2] */)
+{
+  const int lane = threadIdx.x & 31;
+  const long q = blockIdx.x * (long)kWarps + (threadIdx.x >> 5);
+  if (q >= nq) return;
+  const long nr = a.nrows;
+  long long links = 0, skipped = 0;
+  double m0 = 0., m1 = 0., m2 = 0.;
+  double s[3] = {0., 0., 0.}, w[3] = {0., 0., 0.};
+  for (long r0 = 0; r0 < nr; r0 += 32) {
+    const long r = r0 + lane;
+    double rs[3] = {0., 0., 0.}, rw[3] = {0., 0., 0.};
+    if (r < nr) {
+      const long slot = q * nr + r;
+      links += a.seg_links[slot];
+      skipped += a.seg_skip[slot];
+      m0 = fmax(m0, a.seg_max[slot * 3]);
+      m1 = fmax(m1, a.seg_max[slot * 3 + 1]);
+      m2 = fmax(m2, a.seg_max[slot * 3 + 2]);
+      for (int k = 0; k < 3; k++) {
+        rs[k] = a.row_sum[slot * 3 + k];
+        rw[k] = a.row_w[slot * 3 + k];
+      }
+    }
+    const int n = (int)min(32l, nr - r0);
+    for (int l = 0; l < n; l++)
+      for (int k = 0; k < 3; k++) {
+        const double vs = __shfl_sync(0xffffffffu, rs[k], l), vw = __shfl_sync(0xffffffffu, rw[k], l);
+        s[k] = __dadd_rn(s[k], vs);
+        w[k] = __dadd_rn(w[k], vw);
+      }
+  }
+  for (int o = 16; o; o >>= 1) {
+    links += __shfl_xor_sync(0xffffffffu, links, o);
+    skipped += __shfl_xor_sync(0xffffffffu, skipped, o);
+    m0 = fmax(m0, __shfl_xor_sync(0xffffffffu, m0, o));
+    m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+    m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+  }
+  if (lane == 0) {
+    double *o = qout + q * 9;
+    o[0] = m0;
+    o[1] = m1;
+    o[2] = m2;
+    for (int k = 0; k < 3; k++) {
+      o[3 + k] = s[k];
+      o[6 + k] = w[k];
+    }
+    qlinks[q * 2] = links;
+    qlinks[q * 2 + 1] = skipped;
+  }
+}
+
+}  // namespace
+
+struct tn93g_server {
+  tn93g_ctx *ctx = nullptr;
+  RunConsts base;
+  long Nref = 0, L = 0, W = 0, Npad = 0, cap_q = 0;
+  int cap_nq = 0;
+  size_t ev_ref = 0, ev_cap = 0, names_ref = 0;
+  DevBuf planes, cc, ccT, evcount, evoff, ev, agg, site, varcol, qcodes, counts, names, name_off, name_len, dist, rq,
+      rqn, counters, segcols, sbytes, soff, slinks, sskip, smax, rsum, rw, hist, total, out, qout, qlinks;
+  void *pin = nullptr;
+  size_t pin_n = 0;
+};
+
+extern "C" {
+
+void tn93g_server_destroy(tn93g_server *srv)
+{
+  if (!srv) return;
+  tn93g_ctx *ctx = srv->ctx;
+  if (ctx) cudaSetDevice(ctx->device);
+  DevBuf *bufs[] = {&srv->planes, &srv->cc, &srv->ccT, &srv->evcount, &srv->evoff, &srv->ev, &srv->agg, &srv->site,
+                    &srv->varcol, &srv->qcodes, &srv->counts, &srv->names, &srv->name_off, &srv->name_len,
+                    &srv->dist, &srv->rq, &srv->rqn, &srv->counters, &srv->segcols, &srv->sbytes, &srv->soff,
+                    &srv->slinks, &srv->sskip, &srv->smax, &srv->rsum, &srv->rw, &srv->hist, &srv->total,
+                    &srv->out, &srv->qout, &srv->qlinks};
+  for (DevBuf *b : bufs)
+    if (b->p) {
+      cudaFree(b->p);
+      if (ctx) ctx->used -= b->n;
+    }
+  if (srv->pin) cudaFreeHost(srv->pin);
+  delete srv;
+}
+
+int tn93g_server_create(tn93g_ctx *ctx, tn93g_server **out, const uint8_t *codes, long N, long L,
+                        const long *copy_counts, const char *names, const size_t *name_off, const long *name_len,
+                        const tn93g_opts *opts, long max_batch_sequences, int max_batch_queries)
+{
+  if (!ctx || !out || !codes || N <= 0 || L <= 0 || !copy_counts || !names || !name_off || !name_len || !opts ||
+      max_batch_sequences <= 0 || max_batch_queries <= 0 || max_batch_queries > 65535)
+    return TN93G_EINVAL;
+  if (opts->mode < 0 || opts->mode > 4 || opts->format < 0 || opts->format > 1) return TN93G_EINVAL;
+  if (L >= (1l << 25) || N > 65535l * 32 || (unsigned long)(N + max_batch_sequences) * (unsigned long)L >= (1ul << 32))
+    return TN93G_ETOOBIG;
+  *out = nullptr;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  tn93g_server *srv = new tn93g_server();
+  srv->ctx = ctx;
+  int rc_ = TN93G_OK;
+#define SV(x)                   \
+  do {                          \
+    rc_ = (x);                  \
+    if (rc_ != TN93G_OK) {      \
+      tn93g_server_destroy(srv); \
+      return rc_;               \
+    }                           \
+  } while (0)
+#define SVC(call)                                                     \
+  do {                                                                \
+    cudaError_t e_ = (call);                                          \
+    if (e_ != cudaSuccess) {                                          \
+      ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);  \
+      tn93g_server_destroy(srv);                                      \
+      return TN93G_ECUDA;                                             \
+    }                                                                 \
+  } while (0)
+  RunConsts &rc = srv->base;
+  memset(&rc, 0, sizeof rc);
+  rc.mode = opts->mode;
+  rc.gapmm = opts->mode == TN93G_GAPMM;
+  rc.cross = true;
+  rc.fallback_avg = (opts->mode == TN93G_RESOLVE || opts->mode == TN93G_SUBSET) && opts->resolve_fraction < 1.;
+  rc.emit = !opts->count_only;
+  rc.format = opts->format;
+  rc.delim = opts->delimiter;
+  rc.threshold = opts->threshold;
+  rc.min_distance = opts->min_distance;
+  rc.resolve_fraction = opts->resolve_fraction;
+  rc.min_overlap = opts->min_overlap;
+  srv->Nref = N;
+  srv->L = L;
+  srv->W = (L + 63) / 64;
+  srv->cap_q = max_batch_sequences;
+  srv->cap_nq = max_batch_queries;
+  srv->Npad = (N + max_batch_sequences + 63) / 32 * 32;
+  const long cap_n = N + max_batch_sequences, Np = srv->Npad, W = srv->W;
+  rc.Lc = L;
+  rc.W = W;
+  rc.Npad = Np;
+  rc.NP = rc.gapmm ? 5 : 4;
+  // the reference's codes, its N count (the N plane is used when N is frequent, as in tn93g_run)
+  SV(ensure(ctx, srv->qcodes, std::max<size_t>((size_t)N, (size_t)max_batch_sequences) * L));
+  SVC(cudaMemcpyAsync(srv->qcodes.p, codes, (size_t)N * L, cudaMemcpyHostToDevice, st));
+  SV(ensure(ctx, ctx->seen, L * sizeof(uint32_t)));
+  SV(ensure(ctx, ctx->nN, sizeof(unsigned long long)));
+  SVC(cudaMemsetAsync(ctx->seen.p, 0, L * sizeof(uint32_t), st));
+  SVC(cudaMemsetAsync(ctx->nN.p, 0, sizeof(unsigned long long), st));
+  colscan_kernel<<<dim3((unsigned)((L + 255) / 256), (unsigned)((N + 63) / 64)), 256, 0, st>>>(
+      (const uint8_t *)srv->qcodes.p, N, L, (uint32_t *)ctx->seen.p, (unsigned long long *)ctx->nN.p);
+  SVC(cudaGetLastError());
+  unsigned long long nN = 0;
+  SVC(cudaMemcpyAsync(&nN, ctx->nN.p, sizeof nN, cudaMemcpyDeviceToHost, st));
+  SVC(cudaStreamSynchronize(st));
+  rc.wplane = rc.gapmm || nN > 16ull * (unsigned long long)N;
+  // resident arrays with room for max_batch_sequences query sequences after the reference
+  SV(ensure(ctx, srv->planes, (size_t)W * rc.NP * Np * sizeof(uint64_t)));
+  SV(ensure(ctx, srv->cc, (size_t)cap_n * L));
+  SV(ensure(ctx, srv->ccT, (size_t)L * Np));
+  SV(ensure(ctx, srv->evcount, cap_n * sizeof(uint32_t)));
+  SV(ensure(ctx, srv->evoff, (cap_n + 1) * sizeof(uint32_t)));
+  SV(ensure(ctx, srv->varcol, L * sizeof(int32_t)));
+  SVC(cudaMemsetAsync(srv->planes.p, 0, (size_t)W * rc.NP * Np * sizeof(uint64_t), st));
+  SVC(cudaMemsetAsync(srv->evcount.p, 0, cap_n * sizeof(uint32_t), st));
+  {
+    std::vector<int32_t> id(L);
+    for (long p = 0; p < L; p++) id[p] = (int32_t)p;
+    SVC(cudaMemcpy(srv->varcol.p, id.data(), L * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
+  PackArgs pa;
+  pa.codes = (const uint8_t *)srv->qcodes.p;
+  pa.N = N;
+  pa.L = L;
+  pa.Lc = L;
+  pa.W = W;
+  pa.Npad = Np;
+  pa.varcol = (const int32_t *)srv->varcol.p;
+  pa.NP = rc.NP;
+  pa.wplane = rc.wplane;
+  pa.gapmm = rc.gapmm;
+  pa.planes = (uint64_t *)srv->planes.p;
+  pa.cc = (uint8_t *)srv->cc.p;
+  pa.evcount = (uint32_t *)srv->evcount.p;
+  pack_kernel<<<dim3((unsigned)((N + kWarps - 1) / kWarps), (unsigned)std::min<long>(W, 65535)), 256, 0, st>>>(pa);
+  SVC(cudaGetLastError());
+  transpose_kernel<<<dim3((unsigned)((L + 31) / 32), (unsigned)((N + 31) / 32)), dim3(32, 8), 0, st>>>(
+      (const uint8_t *)srv->cc.p, (uint8_t *)srv->ccT.p, N, L, Np);
+  SVC(cudaGetLastError());
+  std::vector<uint32_t> evc(N), evo(N + 1);
+  SVC(cudaMemcpyAsync(evc.data(), srv->evcount.p, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  SVC(cudaStreamSynchronize(st));
+  evo[0] = 0;
+  for (long i = 0; i < N; i++) evo[i + 1] = evo[i] + evc[i];
+  srv->ev_ref = evo[N];
+  srv->ev_cap = srv->ev_ref + (size_t)max_batch_sequences * L;
+  SV(ensure(ctx, srv->ev, std::max<size_t>(srv->ev_cap, 1) * sizeof(uint32_t)));
+  SVC(cudaMemcpyAsync(srv->evoff.p, evo.data(), (N + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  pa.ev_off = (const uint32_t *)srv->evoff.p;
+  pa.ev = (uint32_t *)srv->ev.p;
+  if (srv->ev_ref) {
+    events_kernel<<<(unsigned)((N + kWarps - 1) / kWarps), 256, 0, st>>>(pa);
+    SVC(cudaGetLastError());
+  }
+  // tables of the server's mode
+  build_tables(ctx->h_tab, opts->mode, opts->subset);
+  const size_t agg_n = kSparseCodes * kCodes + 5;
+  SV(ensure(ctx, srv->agg, agg_n * sizeof(AggEntry)));
+  SV(ensure(ctx, srv->site, sizeof(ctx->h_tab->site)));
+  SVC(cudaMemcpyAsync(srv->agg.p, ctx->h_tab->ev, agg_n * sizeof(AggEntry), cudaMemcpyHostToDevice, st));
+  SVC(cudaMemcpyAsync(srv->site.p, ctx->h_tab->site, sizeof(ctx->h_tab->site), cudaMemcpyHostToDevice, st));
+  // names, name offsets and lengths, copy numbers of every sequence (the reference's now, the queries' per batch)
+  size_t nbytes = 0;
+  for (long i = 0; i < N; i++) nbytes = std::max(nbytes, name_off[i] + (size_t)name_len[i]);
+  srv->names_ref = nbytes;
+  SV(ensure(ctx, srv->names, nbytes + 1 + (size_t)max_batch_sequences * 64));
+  SV(ensure(ctx, srv->name_off, cap_n * sizeof(uint64_t)));
+  SV(ensure(ctx, srv->name_len, cap_n * sizeof(int32_t)));
+  SV(ensure(ctx, srv->counts, cap_n * sizeof(long)));
+  std::vector<uint64_t> off(name_off, name_off + N);
+  std::vector<int32_t> nl(N);
+  for (long i = 0; i < N; i++) nl[i] = (int32_t)name_len[i];
+  if (nbytes) SVC(cudaMemcpyAsync(srv->names.p, names, nbytes, cudaMemcpyHostToDevice, st));
+  SVC(cudaMemcpyAsync(srv->name_off.p, off.data(), N * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+  SVC(cudaMemcpyAsync(srv->name_len.p, nl.data(), N * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  SVC(cudaMemcpyAsync(srv->counts.p, copy_counts, N * sizeof(long), cudaMemcpyHostToDevice, st));
+  // per-batch buffers at capacity (a batch never reallocates them): distances and the replay queue of every
+  // pair, per (query, row) statistics, per-query histograms and results
+  {
+    const size_t dslots = (size_t)N * max_batch_sequences, nslot = (size_t)max_batch_queries * N;
+    const int nq = max_batch_queries;
+    SV(ensure(ctx, srv->dist, dslots * sizeof(double)));
+    SV(ensure(ctx, srv->rq, dslots * sizeof(unsigned long long)));
+    SV(ensure(ctx, srv->rqn, sizeof(unsigned)));
+    SV(ensure(ctx, srv->counters, 4 * sizeof(unsigned long long)));
+    SV(ensure(ctx, srv->sbytes, nslot * sizeof(unsigned long long)));
+    SV(ensure(ctx, srv->soff, nslot * sizeof(unsigned long long)));
+    SV(ensure(ctx, srv->slinks, nslot * sizeof(long long)));
+    SV(ensure(ctx, srv->sskip, nslot * sizeof(long long)));
+    SV(ensure(ctx, srv->smax, nslot * 3 * sizeof(double)));
+    SV(ensure(ctx, srv->rsum, nslot * 3 * sizeof(double)));
+    SV(ensure(ctx, srv->rw, nslot * 3 * sizeof(double)));
+    SV(ensure(ctx, srv->hist, (size_t)nq * 3 * kHistBins * sizeof(unsigned long long)));
+    SV(ensure(ctx, srv->total, sizeof(unsigned long long)));
+    SV(ensure(ctx, srv->segcols, (nq + 1) * sizeof(long)));
+    SV(ensure(ctx, srv->qout, (size_t)nq * 9 * sizeof(double)));
+    SV(ensure(ctx, srv->qlinks, (size_t)nq * 2 * sizeof(long long)));
+  }
+  SVC(cudaStreamSynchronize(st));
+#undef SV
+#undef SVC
+  *out = srv;
+  return TN93G_OK;
+}
+
+int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries, tn93g_query_sink sink, void *user,
+                       tn93g_summary *sums)
+{
+  if (!srv || nq <= 0 || !queries || !sums) return TN93G_EINVAL;
+  tn93g_ctx *ctx = srv->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  ctx->launches = 0;
+  const long Nref = srv->Nref, L = srv->L, Np = srv->Npad, W = srv->W;
+  if (nq > srv->cap_nq) {
+    ctx->err = "more queries than the server's batch capacity";
+    return TN93G_EINVAL;
+  }
+  std::vector<long> qstart(nq + 1);
+  qstart[0] = 0;
+  for (int q = 0; q < nq; q++) {
+    if (queries[q].n <= 0 || queries[q].L != srv->L || !queries[q].codes || !queries[q].copy_counts ||
+        !queries[q].names || !queries[q].name_off || !queries[q].name_len)
+      return TN93G_EINVAL;
+    qstart[q + 1] = qstart[q] + queries[q].n;
+  }
+  const long Q = qstart[nq];
+  if (Q > srv->cap_q) {
+    ctx->err = "batch larger than the server's query capacity";
+    return TN93G_EINVAL;
+  }
+  // query codes, names, offsets, lengths and copy numbers into the slots after the reference
+  std::vector<uint64_t> off(Q);
+  std::vector<int32_t> nl(Q);
+  std::vector<long> cnt(Q);
+  size_t nb = srv->names_ref;
+  std::vector<size_t> qname_base(nq);
+  for (int q = 0; q < nq; q++) {
+    size_t qn = 0;
+    for (long k = 0; k < queries[q].n; k++) qn = std::max(qn, queries[q].name_off[k] + (size_t)queries[q].name_len[k]);
+    qname_base[q] = nb;
+    for (long k = 0; k < queries[q].n; k++) {
+      off[qstart[q] + k] = nb + queries[q].name_off[k];
+      nl[qstart[q] + k] = (int32_t)queries[q].name_len[k];
+      cnt[qstart[q] + k] = queries[q].copy_counts[k];
+    }
+    nb += qn;
+  }
+  TRY(ensure_keep(ctx, srv->names, nb + 1, srv->names_ref));
+  for (int q = 0; q < nq; q++) {
+    CU(cudaMemcpyAsync((uint8_t *)srv->qcodes.p + (size_t)qstart[q] * L, queries[q].codes, (size_t)queries[q].n * L,
+                       cudaMemcpyHostToDevice, st));
+    size_t qn = 0;
+    for (long k = 0; k < queries[q].n; k++) qn = std::max(qn, queries[q].name_off[k] + (size_t)queries[q].name_len[k]);
+    if (qn) CU(cudaMemcpyAsync((char *)srv->names.p + qname_base[q], queries[q].names, qn, cudaMemcpyHostToDevice, st));
+  }
+  CU(cudaMemcpyAsync((uint64_t *)srv->name_off.p + Nref, off.data(), Q * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync((int32_t *)srv->name_len.p + Nref, nl.data(), Q * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync((long *)srv->counts.p + Nref, cnt.data(), Q * sizeof(long), cudaMemcpyHostToDevice, st));
+  // pack the queries into their slots
+  RunConsts rc = srv->base;
+  rc.N = Nref + Q;
+  rc.n1 = Nref;
+  PackArgs pa;
+  pa.codes = (const uint8_t *)srv->qcodes.p;
+  pa.N = Q;
+  pa.L = L;
+  pa.Lc = L;
+  pa.W = W;
+  pa.Npad = Np;
+  pa.varcol = (const int32_t *)srv->varcol.p;
+  pa.NP = rc.NP;
+  pa.wplane = rc.wplane;
+  pa.gapmm = rc.gapmm;
+  pa.planes = (uint64_t *)srv->planes.p + Nref;
+  pa.cc = (uint8_t *)srv->cc.p + (size_t)Nref * L;
+  pa.evcount = (uint32_t *)srv->evcount.p + Nref;
+  CU(cudaMemsetAsync(pa.evcount, 0, Q * sizeof(uint32_t), st));
+  pack_kernel<<<dim3((unsigned)((Q + kWarps - 1) / kWarps), (unsigned)std::min<long>(W, 65535)), 256, 0, st>>>(pa);
+  CU(cudaGetLastError());
+  ctx->launches++;
+  transpose_kernel<<<dim3((unsigned)((L + 31) / 32), (unsigned)((Q + 31) / 32)), dim3(32, 8), 0, st>>>(
+      pa.cc, (uint8_t *)srv->ccT.p + Nref, Q, L, Np);
+  CU(cudaGetLastError());
+  ctx->launches++;
+  std::vector<uint32_t> evc(Q), evo(Q + 1);
+  CU(cudaMemcpyAsync(evc.data(), pa.evcount, Q * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  evo[0] = (uint32_t)srv->ev_ref;
+  for (long k = 0; k < Q; k++) evo[k + 1] = evo[k] + evc[k];
+  CU(cudaMemcpyAsync((uint32_t *)srv->evoff.p + Nref, evo.data(), (Q + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                     st));
+  pa.ev_off = (const uint32_t *)srv->evoff.p + Nref;
+  pa.ev = (uint32_t *)srv->ev.p;
+  if (evo[Q] > evo[0]) {
+    events_kernel<<<(unsigned)((Q + kWarps - 1) / kWarps), 256, 0, st>>>(pa);
+    CU(cudaGetLastError());
+    ctx->launches++;
+  }
+  // the cross run: rows = reference, columns = the batch's queries
+  const size_t dslots = (size_t)Nref * Q;
+  const size_t nslot = (size_t)nq * Nref;
+  CU(cudaMemsetAsync(srv->rqn.p, 0, sizeof(unsigned), st));
+  CU(cudaMemsetAsync(srv->counters.p, 0, 4 * sizeof(unsigned long long), st));
+  CU(cudaMemsetAsync(srv->hist.p, 0, (size_t)nq * 3 * kHistBins * sizeof(unsigned long long), st));
+  std::vector<long> segc(nq + 1);
+  for (int q = 0; q <= nq; q++) segc[q] = Nref + qstart[q];
+  CU(cudaMemcpyAsync(srv->segcols.p, segc.data(), (nq + 1) * sizeof(long), cudaMemcpyHostToDevice, st));
+  PairArgs A;
+  A.rc = rc;
+  A.planes = (const uint64_t *)srv->planes.p;
+  A.cc = (const uint8_t *)srv->cc.p;
+  A.ccT = (const uint8_t *)srv->ccT.p;
+  A.ev_off = (const uint32_t *)srv->evoff.p;
+  A.ev = (const uint32_t *)srv->ev.p;
+  A.agg = (const AggEntry *)srv->agg.p;
+  A.r0 = 0;
+  A.r1 = Nref;
+  A.ncols = Q;
+  A.colbase = Nref;
+  A.cstart = Nref;
+  A.dist = (double *)srv->dist.p;
+  A.replay_q = (unsigned long long *)srv->rq.p;
+  A.replay_n = (unsigned *)srv->rqn.p;
+  A.replay_cap = dslots;
+  A.counters = (unsigned long long *)srv->counters.p;
+  A.logt = ctx->d_logt;
+  CU(launch_pair(A, (Q + 31) / 32, Nref, st));
+  ctx->launches++;
+  ReplayArgs R;
+  R.rc = rc;
+  R.cc = A.cc;
+  R.planes = A.planes;
+  R.site = (const SiteEntry *)srv->site.p;
+  R.q = A.replay_q;
+  R.qn = A.replay_n;
+  R.qcap = dslots;
+  R.r0 = 0;
+  R.ncols = Q;
+  R.colbase = Nref;
+  R.dist = A.dist;
+  R.counters = A.counters;
+  R.logt = ctx->d_logt;
+  replay_kernel<<<2 * 148, 256, 0, st>>>(R);
+  CU(cudaGetLastError());
+  ctx->launches++;
+  RowArgs RA;
+  RA.rc = rc;
+  RA.dist = A.dist;
+  RA.r0 = 0;
+  RA.r1 = Nref;
+  RA.ncols = Q;
+  RA.colbase = Nref;
+  RA.counts = (const long *)srv->counts.p;
+  RA.name_len = (const int32_t *)srv->name_len.p;
+  RA.name_off = (const uint64_t *)srv->name_off.p;
+  RA.names = (const char *)srv->names.p;
+  RA.maxseg = nq;
+  RA.seg_cols = (const long *)srv->segcols.p;
+  RA.nrows = Nref;
+  RA.seg_bytes = (unsigned long long *)srv->sbytes.p;
+  RA.seg_links = (long long *)srv->slinks.p;
+  RA.seg_skip = (long long *)srv->sskip.p;
+  RA.seg_max = (double *)srv->smax.p;
+  RA.row_sum = (double *)srv->rsum.p;
+  RA.row_w = (double *)srv->rw.p;
+  RA.hist = (unsigned long long *)srv->hist.p;
+  RA.seg_off = (const unsigned long long *)srv->soff.p;
+  RA.hy = nullptr;
+  RA.err = (unsigned long long *)srv->counters.p + 3;
+  RA.out = nullptr;
+  const dim3 g2((unsigned)((Nref + kWarps - 1) / kWarps), (unsigned)nq);
+  stats_kernel<<<g2, 256, 0, st>>>(RA);
+  CU(cudaGetLastError());
+  ctx->launches++;
+  sum_kernel<<<g2, 256, 0, st>>>(RA);
+  CU(cudaGetLastError());
+  ctx->launches++;
+  scan_kernel<<<1, 1024, 0, st>>>(RA.seg_bytes, (unsigned long long *)RA.seg_off, (long)nslot,
+                                  (unsigned long long *)srv->total.p);
+  CU(cudaGetLastError());
+  ctx->launches++;
+  query_reduce_kernel<<<(unsigned)((nq + kWarps - 1) / kWarps), 256, 0, st>>>(RA, nq, (double *)srv->qout.p,
+                                                                             (long long *)srv->qlinks.p);
+  CU(cudaGetLastError());
+  ctx->launches++;
+  unsigned long long total = 0;
+  std::vector<double> qo((size_t)nq * 9);
+  std::vector<long long> ql((size_t)nq * 2);
+  std::vector<unsigned long long> qoff(nq + 1);
+  CU(cudaMemcpyAsync(&total, srv->total.p, sizeof total, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(qo.data(), srv->qout.p, qo.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(ql.data(), srv->qlinks.p, ql.size() * sizeof(long long), cudaMemcpyDeviceToHost, st));
+  for (int q = 0; q < nq; q++)
+    CU(cudaMemcpyAsync(&qoff[q], (unsigned long long *)srv->soff.p + (size_t)q * Nref, sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, st));
+  std::vector<unsigned long long> hist((size_t)nq * 3 * kHistBins);
+  CU(cudaMemcpyAsync(hist.data(), srv->hist.p, hist.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  unsigned long long counters[4];
+  CU(cudaMemcpyAsync(counters, srv->counters.p, sizeof counters, cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  qoff[nq] = total;
+  if (rc.emit && total) {
+    if (srv->out.n < total) TRY(ensure(ctx, srv->out, total + total / 2));
+    if (srv->pin_n < total) {
+      if (srv->pin) cudaFreeHost(srv->pin);
+      srv->pin = nullptr;
+      srv->pin_n = 0;
+      CU(cudaHostAlloc(&srv->pin, total + total / 4, cudaHostAllocDefault));
+      srv->pin_n = total + total / 4;
+    }
+    RA.out = (char *)srv->out.p;
+    write_kernel<<<g2, 256, 0, st>>>(RA);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    CU(cudaMemcpyAsync(srv->pin, srv->out.p, total, cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(&counters[3], (unsigned long long *)srv->counters.p + 3, sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+  }
+  if (counters[3]) {
+    ctx->err = "internal error: a query's text did not match its counted length";
+    return TN93G_ECUDA;
+  }
+  for (int q = 0; q < nq; q++) {
+    tn93g_summary &S = sums[q];
+    memset(&S, 0, sizeof S);
+    S.pairwise = (unsigned long)Nref * (unsigned long)queries[q].n;
+    S.links = (long)ql[q * 2];
+    S.skipped = (long)ql[q * 2 + 1];
+    for (int k = 0; k < 3; k++) {
+      S.max[k] = qo[q * 9 + k];
+      S.mean[k] = qo[q * 9 + 3 + k];
+      S.weighted[k] = qo[q * 9 + 6 + k];
+      for (int b = 0; b < kHistBins; b++) S.hist[k][b] = hist[((size_t)q * 3 + k) * kHistBins + b];
+    }
+    S.output_bytes = qoff[q + 1] - qoff[q];
+    if (q == 0) {
+      S.pairs_replayed = (long)counters[2];
+      S.logs_ambiguous = (long)counters[0];
+      S.undecided = (long)counters[1];
+    }
+    if (rc.emit && sink && sink(user, q, (const char *)srv->pin + qoff[q], (size_t)(qoff[q + 1] - qoff[q])))
+      return TN93G_ESINK;
+  }
+  return TN93G_OK;
+}
 
 }  // extern "C"

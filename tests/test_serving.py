@@ -1,0 +1,123 @@
+"""The resident-reference server (tn93g_server_*) and the continuous-batching service on top of it.
+
+Every query's response must equal, byte for byte, what `tn93 -q FLAGS -s QUERY.fa -o OUT REF.fa` produces (exit
+status, distance file, JSON summary on stdout; the oracle is the checker), and must be the same whether the query
+runs alone or batched with others. The batching policy itself is host logic and is tested on the CPU."""
+from collections import deque
+from dataclasses import dataclass
+
+import numpy as np
+import pytest
+
+from tests.conftest import run_tn93
+
+SERVE_FLAGS = [
+    ("hivtrace_s", ["-t", "0.015", "-a", "resolve", "-l", "500"], dict(threshold=0.015, mode="resolve",
+                                                                      min_overlap=500)),
+    ("fallback_csvn", ["-t", "0.015", "-a", "resolve", "-g", "0.05", "-l", "500", "-f", "csvn"],
+     dict(threshold=0.015, mode="resolve", resolve_fraction=0.05, min_overlap=500, format="csvn")),
+    ("average_delim", ["-t", "0.03", "-a", "average", "-l", "100", "-D", ";"],
+     dict(threshold=0.03, mode="average", min_overlap=100, delimiter=";")),
+    ("gapmm", ["-t", "0.02", "-a", "gapmm", "-l", "200"], dict(threshold=0.02, mode="gapmm", min_overlap=200)),
+]
+
+
+@dataclass
+class _R:
+    n: int
+
+
+def test_take_batch_policy():
+    from swifttn93_b200.serve import take_batch
+
+    q = deque(_R(n) for n in (5, 7, 3, 20, 1, 1))
+    assert [r.n for r in take_batch(q, 10, 16)] == [5, 7, 3]
+    assert [r.n for r in q] == [20, 1, 1]
+    assert take_batch(q, 10, 16) == []          # the head does not fit: it waits, order is kept
+    q = deque(_R(1) for _ in range(9))
+    assert len(take_batch(q, 4, 100)) == 4 and len(q) == 5
+    assert take_batch(deque(), 4, 100) == []
+
+
+def _workload():
+    from swifttn93_b200 import synth
+
+    rng = np.random.default_rng(44)
+    rnames, rcodes = synth.serve_reference(seed=9, n=1500, L=1500)
+    ref = synth.to_fasta(rnames, rcodes)
+    queries = []
+    for k, q in enumerate((1, 2, 5, 17, 32, 64, 3, 130)):
+        names, codes = synth.serve_query(rng, rcodes, q, f"t{k}")
+        if k == 2:
+            names = [f"{n}:{1 + i % 4}" for i, n in enumerate(names)]  # copy numbers
+        fa = synth.to_fasta(names, codes, wrap=70 if k == 3 else 0)
+        if k == 4:
+            fa = fa.lower()
+        queries.append(fa)
+    return ref, queries
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("tag,flags,kw", SERVE_FLAGS, ids=[t for t, _, _ in SERVE_FLAGS])
+def test_served_queries_match_oracle_alone_and_batched(oracle_bin, tmp_path, tag, flags, kw):
+    from swifttn93_b200 import Engine, Fasta, Options, ResidentReference
+    from swifttn93_b200.serve import header_line
+
+    ref, queries = _workload()
+    refp = tmp_path / "ref.fa"
+    refp.write_bytes(ref)
+    opts = Options(**kw)
+    eng = Engine()
+    R = Fasta(ref)
+    res = ResidentReference(eng, R, opts, max_batch_sequences=512, max_batch_queries=16)
+    Q = [Fasta(q, expect_len=R.L) for q in queries]
+    batched = res.batch(Q)
+    assert len(batched) == len(Q)
+    for k, (qfa, qf) in enumerate(zip(queries, Q)):
+        alone = res.batch([qf])[0]
+        assert alone[0] == batched[k][0], (tag, k)
+        qp = tmp_path / f"q{k}.fa"
+        qp.write_bytes(qfa)
+        rc, fb, out, _ = run_tn93(oracle_bin, flags + ["-s", str(qp)], refp, tmp_path)
+        assert rc == 0
+        body, summ = batched[k]
+        assert header_line(opts) + body == fb, (tag, k, len(body), len(fb))
+        assert summ.json(R.n, qf.n, second_file=True) == out, (tag, k)
+        assert summ.pairwise == R.n * qf.n
+    res.close()
+    eng.close()
+
+
+@pytest.mark.gpu
+def test_service_continuous_batching_same_as_alone(oracle_bin, tmp_path):
+    """Requests arriving as a Poisson stream are batched by two workers; each response equals the oracle's run of
+    that query file, and a refused query (wrong sequence length) gets tn93's status and message alone."""
+    from swifttn93_b200 import Options
+    from swifttn93_b200.serve import Service, run_load
+
+    ref, queries = _workload()
+    bad = b">x\nACGT\n"
+    stream = queries * 3 + [bad]
+    refp = tmp_path / "ref.fa"
+    refp.write_bytes(ref)
+    flags = ["-t", "0.015", "-a", "resolve", "-l", "500"]
+    want = []
+    for k, qfa in enumerate(queries + [bad]):
+        qp = tmp_path / f"q{k}.fa"
+        qp.write_bytes(qfa)
+        rc, fb, out, err = run_tn93(oracle_bin, flags + ["-s", str(qp)], refp, tmp_path)
+        want.append((rc, fb if rc == 0 else None, out if rc == 0 else None, err))
+    with Service(ref, Options(threshold=0.015, mode="resolve", min_overlap=500), hbm_budget=4 << 30, workers=2,
+                 max_batch_queries=8, max_batch_sequences=300) as svc:
+        r = run_load(svc, stream, rate=400.0, seed=3)
+        stats = svc.stats
+    assert r["requests"] == len(stream) and r["ok"] == len(stream) - 1
+    for k, resp in enumerate(r["responses"]):
+        w = want[len(queries)] if k == len(stream) - 1 else want[k % len(queries)]
+        assert resp.rc == w[0], k
+        if w[0] == 0:
+            assert resp.file == w[1] and resp.stdout == w[2], k
+        else:
+            assert resp.stderr == w[3], (resp.stderr, w[3])
+    assert stats.batches < stats.done  # requests were batched together
+    assert max(stats.batch_sequences) <= 300
