@@ -364,6 +364,12 @@ class ResidentReference:
             out.append((b"".join(bodies[q]), _plain_summary(S)))
         return out
 
+    def last_timings(self) -> dict:
+        """Device milliseconds of the last batch per stage (pack, pair, replay, rows, write, d2h, total)."""
+        t = (C.c_double * 7)()
+        k = self.lib.tn93g_last_timings(self.engine.ctx, t, 7)
+        return {Engine.STAGES[q]: t[q] for q in range(k)}
+
     def close(self):
         if self.srv:
             self.lib.tn93g_server_destroy(self.srv)

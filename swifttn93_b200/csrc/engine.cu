@@ -525,6 +525,75 @@ __global__ void __launch_bounds__(1024) scan_kernel(const unsigned long long *in
   if (threadIdx.x == 1023) *total = part[1023];
 }
 
+// Large exclusive scans in three coalesced passes: tile sums, a scan of the tile sums (scan_kernel), then each
+// tile's scan from its offset. A tile is 256 threads x 16 consecutive elements.
+constexpr int kScanTile = 4096;
+
+__global__ void __launch_bounds__(256) tile_sum_kernel(const unsigned long long *in, long n,
+                                                       unsigned long long *tile_sum)
+{
+  __shared__ unsigned long long ws[8];
+  const long b = blockIdx.x * (long)kScanTile;
+  unsigned long long s = 0;
+  for (int k = threadIdx.x; k < kScanTile; k += 256) {
+    const long e = b + k;
+    if (e < n) s += in[e];
+  }
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int w = 0; w < 8; w++) t += ws[w];
+    tile_sum[blockIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(256) tile_scan_kernel(const unsigned long long *in, unsigned long long *out, long n,
+                                                        const unsigned long long *tile_off)
+{
+  __shared__ unsigned long long ws[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long b = blockIdx.x * (long)kScanTile + threadIdx.x * 16l;
+  unsigned long long v[16], s = 0;
+#pragma unroll
+  for (int k = 0; k < 16; k++) {
+    v[k] = b + k < n ? in[b + k] : 0;
+    s += v[k];
+  }
+  // exclusive scan of the per-thread sums over the block
+  unsigned long long inc = s;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) ws[warp] = inc;
+  __syncthreads();
+  unsigned long long base = tile_off[blockIdx.x];
+  for (int w = 0; w < warp; w++) base += ws[w];
+  unsigned long long run = base + inc - s;
+#pragma unroll
+  for (int k = 0; k < 16; k++) {
+    if (b + k < n) out[b + k] = run;
+    run += v[k];
+  }
+}
+
+// exclusive scan of n counters into out, the sum into *total; tmp holds 2 * ceil(n / kScanTile) + 1 counters
+cudaError_t launch_scan(const unsigned long long *in, unsigned long long *out, long n, unsigned long long *total,
+                        unsigned long long *tmp, cudaStream_t st)
+{
+  if (n <= 65536) {
+    scan_kernel<<<1, 1024, 0, st>>>(in, out, n, total);
+    return cudaGetLastError();
+  }
+  const long nt = (n + kScanTile - 1) / kScanTile;
+  tile_sum_kernel<<<(unsigned)nt, 256, 0, st>>>(in, n, tmp);
+  scan_kernel<<<1, 1024, 0, st>>>(tmp, tmp + nt, nt, total);
+  tile_scan_kernel<<<(unsigned)nt, 256, 0, st>>>(in, out, n, tmp + nt);
+  return cudaGetLastError();
+}
+
 //------------------------------------------------------------------------------------------------ rows
 __device__ __forceinline__ int digits_of(long v)
 {
@@ -591,19 +660,9 @@ __global__ void __launch_bounds__(256) stats_kernel(RowArgs a)
   const int sg = blockIdx.y;
   if (i < a.r1) {
     const long r = i - a.r0;
-    long slot, c0, c1;
-    if (a.seg_cols) {
-      slot = sg * a.nrows + r;
-      c0 = a.seg_cols[sg];
-      c1 = a.seg_cols[sg + 1];
-    } else {
-      slot = r * a.maxseg + sg;
-      const long lb = rc.cross ? rc.n1 : i + 1;
-      c0 = lb + (long)sg * kSeg;
-      c1 = min(rc.N, c0 + kSeg);
-    }
-    // csvn prints a query column's index in its own run (reference rows first, then the query's sequences)
-    const long jshift = a.seg_cols ? c0 - rc.n1 : 0;
+    const long slot = r * a.maxseg + sg;
+    const long lb = rc.cross ? rc.n1 : i + 1;
+    const long c0 = lb + (long)sg * kSeg, c1 = min(rc.N, c0 + kSeg);
     const long cnt_i = a.counts[i];
     const int nli = a.name_len[i];
     const int dli = rc.format == 1 ? digits_of(i) : 0;
@@ -634,7 +693,7 @@ __global__ void __launch_bounds__(256) stats_kernel(RowArgs a)
         if (rc.emit) {
           if (rc.format != 2) {
             const int gl = fmt_g_len(v.thisD);
-            bytes += rc.format == 0 ? nli + a.name_len[j] + gl + 3 : dli + digits_of(j - jshift) + gl + 3;
+            bytes += rc.format == 0 ? nli + a.name_len[j] + gl + 3 : dli + digits_of(j) + gl + 3;
           } else {
             a.hy[(size_t)i * rc.N + j] = v.thisD;
             a.hy[(size_t)j * rc.N + i] = v.thisD;
@@ -666,12 +725,11 @@ __global__ void __launch_bounds__(256) stats_kernel(RowArgs a)
     }
   }
   __syncthreads();
-  unsigned long long *hist = a.seg_cols ? a.hist + (size_t)sg * 3 * kHistBins : a.hist;
   for (int t = threadIdx.x; t < 3 * kHistBins; t += blockDim.x)
-    if (sh[t]) atomicAdd(&hist[t], sh[t]);
+    if (sh[t]) atomicAdd(&a.hist[t], sh[t]);
 }
 
-// one warp per row (or per (row, query segment)): tn93's row sums in column order (swifttn93.cpp:2594-2602); lane 0 adds each chunk's terms in
+// one warp per row: tn93's row sums in column order (swifttn93.cpp:2594-2602); lane 0 adds each chunk's terms in
 // order. The self-pair weights come first, as tn93 adds them when the row starts (swifttn93.cpp:2405-2415).
 __global__ void __launch_bounds__(256) sum_kernel(RowArgs a)
 {
@@ -683,12 +741,7 @@ __global__ void __launch_bounds__(256) sum_kernel(RowArgs a)
   if (i >= a.r1) return;
   const long cnt_i = a.counts[i];
   double s0 = 0., s1 = 0., s2 = 0., w0 = 0., w1 = 0., w2 = 0.;
-  long lb = rc.cross ? rc.n1 : i + 1, cend = rc.N, out_row = i - a.r0;
-  if (a.seg_cols) {
-    lb = a.seg_cols[blockIdx.y];
-    cend = a.seg_cols[blockIdx.y + 1];
-    out_row = (long)blockIdx.y * a.nrows + (i - a.r0);
-  }
+  const long lb = rc.cross ? rc.n1 : i + 1, cend = rc.N, out_row = i - a.r0;
   if (!rc.cross && cnt_i > 1) {
     const unsigned long long svs = (unsigned long long)(cnt_i * (cnt_i - 1l)) >> 1;
     if (i < rc.n1)
@@ -760,7 +813,7 @@ __device__ __forceinline__ char *put_bytes(char *o, const char *s, int n)
   return o + n;
 }
 
-// the text of one reported pair at o (generic pointer: shared staging or global)
+// the text of one reported pair at o (generic pointer: shared staging or global); csvn prints column j as j - jshift
 __device__ __forceinline__ void put_line(char *o, const RowArgs &a, long i, long j, long jshift, const char *ni,
                                          int nli, const char *g, int gl)
 {
@@ -822,19 +875,10 @@ __global__ void __launch_bounds__(256) write_kernel(RowArgs a)
   const long i = a.r0 + blockIdx.x * (long)kWarps + warp;
   const int sg = blockIdx.y;
   if (i >= a.r1) return;
-  long slot, c0, c1;
-  if (a.seg_cols) {
-    slot = sg * a.nrows + (i - a.r0);
-    c0 = a.seg_cols[sg];
-    c1 = a.seg_cols[sg + 1];
-  } else {
-    slot = (i - a.r0) * a.maxseg + sg;
-    const long lb = rc.cross ? rc.n1 : i + 1;
-    c0 = lb + (long)sg * kSeg;
-    c1 = min(rc.N, c0 + kSeg);
-  }
+  const long slot = (i - a.r0) * a.maxseg + sg;
+  const long lb = rc.cross ? rc.n1 : i + 1;
+  const long c0 = lb + (long)sg * kSeg, c1 = min(rc.N, c0 + kSeg);
   if (a.seg_bytes[slot] == 0) return;
-  const long jshift = a.seg_cols ? c0 - rc.n1 : 0;
   const long cnt_i = a.counts[i];
   const int nli = a.name_len[i];
   const char *ni = a.names + a.name_off[i];
@@ -886,7 +930,7 @@ __global__ void __launch_bounds__(256) write_kernel(RowArgs a)
     int gl = 0, len = 0;
     if (put) {
       gl = fmt_g(v.thisD, g);
-      len = rc.format == 0 ? nli + a.name_len[j] + gl + 3 : dli + digits_of(j - jshift) + gl + 3;
+      len = rc.format == 0 ? nli + a.name_len[j] + gl + 3 : dli + digits_of(j) + gl + 3;
     }
     int pre = len;
     for (int o = 1; o < 32; o <<= 1) {
@@ -902,12 +946,12 @@ __global__ void __launch_bounds__(256) write_kernel(RowArgs a)
         S.over = true;
         break;
       }
-      if (put) put_line((char *)(S.gpos + pre - len), a, i, j, jshift, ni, nli, g, gl);
+      if (put) put_line((char *)(S.gpos + pre - len), a, i, j, 0, ni, nli, g, gl);
       __syncwarp();
       S.gpos += total;
       S.head = (int)(S.gpos & 15);
     } else {
-      if (put) put_line(S.buf + S.head + S.fill + (pre - len), a, i, j, jshift, ni, nli, g, gl);
+      if (put) put_line(S.buf + S.head + S.fill + (pre - len), a, i, j, 0, ni, nli, g, gl);
       __syncwarp();
       S.fill += total;
     }
@@ -2083,57 +2127,168 @@ const char *tn93g_noalloc_last_error(void) { return g_na_err; }
 // will ever come), which changes no result.
 namespace {
 
-// per query: links, skips and maxima over its segments, and tn93's row-order mean and weights (lane 0 adds the
-// rows' sums in row order, as tn93's writer does, swifttn93.cpp:2838-2848); one warp per query
-__global__ void query_reduce_kernel(RowArgs a, int nq, double *qout /* [nq][9]: max, mean, weighted */,
-                                    long long *qlinks /* [nq][2] */)
+// Server rows: one thread per (reference row, query). The 256 threads of a block are 256 consecutive rows of one
+// query, so a warp walks the query's columns together (warp-uniform loop) while each thread adds its row's terms
+// in column order, the order tn93 adds a row's pairs in (swifttn93.cpp:2594-2602). Statistics and row sums are
+// fused; the histogram is aggregated per warp (lanes with the same bin add once) and per block in shared memory.
+__global__ void __launch_bounds__(256) qstats_kernel(RowArgs a)
 {
-  const int lane = threadIdx.x & 31;
-  const long q = blockIdx.x * (long)kWarps + (threadIdx.x >> 5);
-  if (q >= nq) return;
-  const long nr = a.nrows;
+  __shared__ unsigned long long sh[kHistBins];
+  for (int t = threadIdx.x; t < kHistBins; t += blockDim.x) sh[t] = 0;
+  __syncthreads();
+  const RunConsts &rc = a.rc;
+  const int q = blockIdx.y;
+  const long i = a.r0 + blockIdx.x * 256l + threadIdx.x;
+  const bool row = i < a.r1;
+  const long c0 = a.seg_cols[q], c1 = a.seg_cols[q + 1], jshift = c0 - rc.n1;
+  const long ii = row ? i : a.r0;
+  const long cnt_i = a.counts[ii];
+  const int nli = a.name_len[ii];
+  const int dli = rc.format == 1 ? digits_of(ii) : 0;
+  double mx = 0., s0 = 0., w0 = 0.;
   long long links = 0, skipped = 0;
-  double m0 = 0., m1 = 0., m2 = 0.;
-  double s[3] = {0., 0., 0.}, w[3] = {0., 0., 0.};
-  for (long r0 = 0; r0 < nr; r0 += 32) {
-    const long r = r0 + lane;
-    double rs[3] = {0., 0., 0.}, rw[3] = {0., 0., 0.};
-    if (r < nr) {
-      const long slot = q * nr + r;
-      links += a.seg_links[slot];
-      skipped += a.seg_skip[slot];
-      m0 = fmax(m0, a.seg_max[slot * 3]);
-      m1 = fmax(m1, a.seg_max[slot * 3 + 1]);
-      m2 = fmax(m2, a.seg_max[slot * 3 + 2]);
-      for (int k = 0; k < 3; k++) {
-        rs[k] = a.row_sum[slot * 3 + k];
-        rw[k] = a.row_w[slot * 3 + k];
+  unsigned long long bytes = 0;
+  for (long j = c0; j < c1; j++) {
+    PairView v = view_pair(a, ii, j, cnt_i);
+    if (!row) v.valid = v.computed = v.linked = false;
+    const int key = v.computed ? v.hb : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    if (__all_sync(0xffffffffu, !v.computed || v.w == 1)) {
+      if (v.computed && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&sh[key], (unsigned long long)__popc(peers));
+    } else if (v.computed) {
+      atomicAdd(&sh[key], (unsigned long long)v.w);
+    }
+    if (!v.valid) continue;
+    if (v.linked) {
+      links += v.w;
+      if (rc.emit) {
+        const int gl = fmt_g_len(v.thisD);
+        bytes += rc.format == 0 ? nli + a.name_len[j] + gl + 3 : dli + digits_of(j - jshift) + gl + 3;
       }
     }
-    const int n = (int)min(32l, nr - r0);
-    for (int l = 0; l < n; l++)
-      for (int k = 0; k < 3; k++) {
-        const double vs = __shfl_sync(0xffffffffu, rs[k], l), vw = __shfl_sync(0xffffffffu, rw[k], l);
-        s[k] = __dadd_rn(s[k], vs);
-        w[k] = __dadd_rn(w[k], vw);
+    if (!v.counted) {
+      skipped++;
+    } else {
+      mx = v.thisD > mx ? v.thisD : mx;
+      s0 = __dadd_rn(s0, __dmul_rn(v.thisD, (double)v.w));
+      w0 = __dadd_rn(w0, (double)v.w);
+    }
+  }
+  if (row) {
+    const size_t slot = (size_t)q * a.nrows + (i - a.r0);
+    a.seg_bytes[slot] = bytes;
+    a.seg_links[slot] = links;
+    a.seg_skip[slot] = skipped;
+    a.seg_max[slot * 3] = mx;
+    a.seg_max[slot * 3 + 1] = 0.;
+    a.seg_max[slot * 3 + 2] = 0.;
+    a.row_sum[slot * 3] = s0;
+    a.row_sum[slot * 3 + 1] = 0.;
+    a.row_sum[slot * 3 + 2] = 0.;
+    a.row_w[slot * 3] = w0;
+    a.row_w[slot * 3 + 1] = 0.;
+    a.row_w[slot * 3 + 2] = 0.;
+  }
+  __syncthreads();
+  unsigned long long *hist = a.hist + (size_t)q * 3 * kHistBins;
+  for (int t = threadIdx.x; t < kHistBins; t += blockDim.x)
+    if (sh[t]) atomicAdd(&hist[t], sh[t]);
+}
+
+// Server text: one thread per (reference row, query) writes that row's lines for the query's columns at its
+// scanned offset (the text is sparse at serving thresholds, so direct byte stores suffice).
+__global__ void __launch_bounds__(256) qwrite_kernel(RowArgs a)
+{
+  const RunConsts &rc = a.rc;
+  const int q = blockIdx.y;
+  const long i = a.r0 + blockIdx.x * 256l + threadIdx.x;
+  if (i >= a.r1) return;
+  const size_t slot = (size_t)q * a.nrows + (i - a.r0);
+  const unsigned long long nb = a.seg_bytes[slot];
+  if (nb == 0) return;
+  const long c0 = a.seg_cols[q], c1 = a.seg_cols[q + 1], jshift = c0 - rc.n1;
+  const long cnt_i = a.counts[i];
+  const int nli = a.name_len[i];
+  const char *ni = a.names + a.name_off[i];
+  const int dli = rc.format == 1 ? digits_of(i) : 0;
+  char *o = a.out + a.seg_off[slot], *const end = o + nb;
+  for (long j = c0; j < c1; j++) {
+    const PairView v = view_pair(a, i, j, cnt_i);
+    if (!(v.valid && v.linked)) continue;
+    char g[24];
+    const int gl = fmt_g(v.thisD, g);
+    const int len = rc.format == 0 ? nli + a.name_len[j] + gl + 3 : dli + digits_of(j - jshift) + gl + 3;
+    if (o + len > end) {
+      atomicAdd(a.err, 1ull);
+      return;
+    }
+    put_line(o, a, i, j, jshift, ni, nli, g, gl);
+    o += len;
+  }
+  if (o != end) atomicAdd(a.err, 1ull);
+}
+
+// Per query: links, skips and maxima over the reference rows, and tn93's mean numerator and weight: the rows' sums
+// added in row order, as tn93's writer adds them (swifttn93.cpp:2838-2848). One block per query: the block stages
+// chunks of row sums in shared memory with coalesced loads (and reduces the order-free counts and maxima), then
+// thread 0 adds the chunk in row order. Only bin 0 is used in a server batch (no -m).
+constexpr int kReduceChunk = 2048;
+
+__global__ void __launch_bounds__(256) query_reduce_kernel(RowArgs a, int nq, double *qout /* [nq][9] */,
+                                                           long long *qlinks /* [nq][2] */)
+{
+  __shared__ double ss[kReduceChunk], sw[kReduceChunk];
+  __shared__ long long rl[8], rs[8];
+  __shared__ double rm[8];
+  const int q = blockIdx.x;
+  const long nr = a.nrows;
+  const size_t base = (size_t)q * nr;
+  long long links = 0, skipped = 0;
+  double m = 0., s0 = 0., w0 = 0.;
+  for (long r0 = 0; r0 < nr; r0 += kReduceChunk) {
+    const int n = (int)min((long)kReduceChunk, nr - r0);
+    for (int k = threadIdx.x; k < n; k += 256) {
+      const size_t slot = base + r0 + k;
+      links += a.seg_links[slot];
+      skipped += a.seg_skip[slot];
+      m = fmax(m, a.seg_max[slot * 3]);
+      ss[k] = a.row_sum[slot * 3];
+      sw[k] = a.row_w[slot * 3];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll 8
+      for (int k = 0; k < n; k++) {
+        s0 = __dadd_rn(s0, ss[k]);
+        w0 = __dadd_rn(w0, sw[k]);
       }
+    }
+    __syncthreads();
   }
   for (int o = 16; o; o >>= 1) {
     links += __shfl_xor_sync(0xffffffffu, links, o);
     skipped += __shfl_xor_sync(0xffffffffu, skipped, o);
-    m0 = fmax(m0, __shfl_xor_sync(0xffffffffu, m0, o));
-    m1 = fmax(m1, __shfl_xor_sync(0xffffffffu, m1, o));
-    m2 = fmax(m2, __shfl_xor_sync(0xffffffffu, m2, o));
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
   }
-  if (lane == 0) {
-    double *o = qout + q * 9;
-    o[0] = m0;
-    o[1] = m1;
-    o[2] = m2;
-    for (int k = 0; k < 3; k++) {
-      o[3 + k] = s[k];
-      o[6 + k] = w[k];
+  if ((threadIdx.x & 31) == 0) {
+    rl[threadIdx.x >> 5] = links;
+    rs[threadIdx.x >> 5] = skipped;
+    rm[threadIdx.x >> 5] = m;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < 8; w++) {
+      links += rl[w];
+      skipped += rs[w];
+      m = fmax(m, rm[w]);
     }
+    double *o = qout + (size_t)q * 9;
+    o[0] = m;
+    o[1] = o[2] = 0.;
+    o[3] = s0;
+    o[4] = o[5] = 0.;
+    o[6] = w0;
+    o[7] = o[8] = 0.;
     qlinks[q * 2] = links;
     qlinks[q * 2 + 1] = skipped;
   }
@@ -2148,7 +2303,7 @@ struct tn93g_server {
   int cap_nq = 0;
   size_t ev_ref = 0, ev_cap = 0, names_ref = 0;
   DevBuf planes, cc, ccT, evcount, evoff, ev, agg, site, varcol, qcodes, counts, names, name_off, name_len, dist, rq,
-      rqn, counters, segcols, sbytes, soff, slinks, sskip, smax, rsum, rw, hist, total, out, qout, qlinks;
+      rqn, counters, segcols, sbytes, soff, slinks, sskip, smax, rsum, rw, hist, total, out, qout, qlinks, scantmp;
   void *pin = nullptr;
   size_t pin_n = 0;
 };
@@ -2164,7 +2319,7 @@ void tn93g_server_destroy(tn93g_server *srv)
                     &srv->varcol, &srv->qcodes, &srv->counts, &srv->names, &srv->name_off, &srv->name_len,
                     &srv->dist, &srv->rq, &srv->rqn, &srv->counters, &srv->segcols, &srv->sbytes, &srv->soff,
                     &srv->slinks, &srv->sskip, &srv->smax, &srv->rsum, &srv->rw, &srv->hist, &srv->total,
-                    &srv->out, &srv->qout, &srv->qlinks};
+                    &srv->out, &srv->qout, &srv->qlinks, &srv->scantmp};
   for (DevBuf *b : bufs)
     if (b->p) {
       cudaFree(b->p);
@@ -2336,6 +2491,12 @@ int tn93g_server_create(tn93g_ctx *ctx, tn93g_server **out, const uint8_t *codes
     SV(ensure(ctx, srv->segcols, (nq + 1) * sizeof(long)));
     SV(ensure(ctx, srv->qout, (size_t)nq * 9 * sizeof(double)));
     SV(ensure(ctx, srv->qlinks, (size_t)nq * 2 * sizeof(long long)));
+    SV(ensure(ctx, srv->scantmp, (2 * (nslot / kScanTile + 1) + 1) * sizeof(unsigned long long)));
+    // a first text buffer (device and pinned host), so that early batches do not stall on growth
+    const size_t text0 = 32u << 20;
+    SV(ensure(ctx, srv->out, text0));
+    SVC(cudaHostAlloc(&srv->pin, text0, cudaHostAllocDefault));
+    srv->pin_n = text0;
   }
   SVC(cudaStreamSynchronize(st));
 #undef SV
@@ -2352,6 +2513,8 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
   ctx->launches = 0;
+  for (double &t : ctx->timings) t = 0;
+  cudaEvent_t *E = ctx->evs;  // stage boundaries: start, packed, pair, replay, rows, written, copied
   const long Nref = srv->Nref, L = srv->L, Np = srv->Npad, W = srv->W;
   if (nq > srv->cap_nq) {
     ctx->err = "more queries than the server's batch capacity";
@@ -2388,6 +2551,7 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
     nb += qn;
   }
   TRY(ensure_keep(ctx, srv->names, nb + 1, srv->names_ref));
+  CU(cudaEventRecord(E[0], st));
   for (int q = 0; q < nq; q++) {
     CU(cudaMemcpyAsync((uint8_t *)srv->qcodes.p + (size_t)qstart[q] * L, queries[q].codes, (size_t)queries[q].n * L,
                        cudaMemcpyHostToDevice, st));
@@ -2438,6 +2602,7 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
     CU(cudaGetLastError());
     ctx->launches++;
   }
+  CU(cudaEventRecord(E[1], st));
   // the cross run: rows = reference, columns = the batch's queries
   const size_t dslots = (size_t)Nref * Q;
   const size_t nslot = (size_t)nq * Nref;
@@ -2468,6 +2633,7 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
   A.logt = ctx->d_logt;
   CU(launch_pair(A, (Q + 31) / 32, Nref, st));
   ctx->launches++;
+  CU(cudaEventRecord(E[2], st));
   ReplayArgs R;
   R.rc = rc;
   R.cc = A.cc;
@@ -2485,6 +2651,7 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
   replay_kernel<<<2 * 148, 256, 0, st>>>(R);
   CU(cudaGetLastError());
   ctx->launches++;
+  CU(cudaEventRecord(E[3], st));
   RowArgs RA;
   RA.rc = rc;
   RA.dist = A.dist;
@@ -2510,21 +2677,17 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
   RA.hy = nullptr;
   RA.err = (unsigned long long *)srv->counters.p + 3;
   RA.out = nullptr;
-  const dim3 g2((unsigned)((Nref + kWarps - 1) / kWarps), (unsigned)nq);
-  stats_kernel<<<g2, 256, 0, st>>>(RA);
+  const dim3 g2((unsigned)((Nref + 255) / 256), (unsigned)nq);
+  qstats_kernel<<<g2, 256, 0, st>>>(RA);
   CU(cudaGetLastError());
   ctx->launches++;
-  sum_kernel<<<g2, 256, 0, st>>>(RA);
+  CU(launch_scan(RA.seg_bytes, (unsigned long long *)RA.seg_off, (long)nslot, (unsigned long long *)srv->total.p,
+                 (unsigned long long *)srv->scantmp.p, st));
+  ctx->launches++;
+  query_reduce_kernel<<<(unsigned)nq, 256, 0, st>>>(RA, nq, (double *)srv->qout.p, (long long *)srv->qlinks.p);
   CU(cudaGetLastError());
   ctx->launches++;
-  scan_kernel<<<1, 1024, 0, st>>>(RA.seg_bytes, (unsigned long long *)RA.seg_off, (long)nslot,
-                                  (unsigned long long *)srv->total.p);
-  CU(cudaGetLastError());
-  ctx->launches++;
-  query_reduce_kernel<<<(unsigned)((nq + kWarps - 1) / kWarps), 256, 0, st>>>(RA, nq, (double *)srv->qout.p,
-                                                                             (long long *)srv->qlinks.p);
-  CU(cudaGetLastError());
-  ctx->launches++;
+  CU(cudaEventRecord(E[4], st));
   unsigned long long total = 0;
   std::vector<double> qo((size_t)nq * 9);
   std::vector<long long> ql((size_t)nq * 2);
@@ -2551,13 +2714,37 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
       srv->pin_n = total + total / 4;
     }
     RA.out = (char *)srv->out.p;
-    write_kernel<<<g2, 256, 0, st>>>(RA);
+    qwrite_kernel<<<g2, 256, 0, st>>>(RA);
     CU(cudaGetLastError());
     ctx->launches++;
+    CU(cudaEventRecord(E[5], st));
     CU(cudaMemcpyAsync(srv->pin, srv->out.p, total, cudaMemcpyDeviceToHost, st));
     CU(cudaMemcpyAsync(&counters[3], (unsigned long long *)srv->counters.p + 3, sizeof(unsigned long long),
                        cudaMemcpyDeviceToHost, st));
+    CU(cudaEventRecord(E[6], st));
     CU(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, E[4], E[5]));
+    ctx->timings[4] = ms;
+    CU(cudaEventElapsedTime(&ms, E[5], E[6]));
+    ctx->timings[5] = ms;
+    CU(cudaEventElapsedTime(&ms, E[0], E[6]));
+    ctx->timings[6] = ms;
+  } else {
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, E[0], E[4]));
+    ctx->timings[6] = ms;
+  }
+  {
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, E[0], E[1]));
+    ctx->timings[0] = ms;
+    CU(cudaEventElapsedTime(&ms, E[1], E[2]));
+    ctx->timings[1] = ms;
+    CU(cudaEventElapsedTime(&ms, E[2], E[3]));
+    ctx->timings[2] = ms;
+    CU(cudaEventElapsedTime(&ms, E[3], E[4]));
+    ctx->timings[3] = ms;
   }
   if (counters[3]) {
     ctx->err = "internal error: a query's text did not match its counted length";

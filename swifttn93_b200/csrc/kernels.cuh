@@ -86,10 +86,9 @@ struct RowArgs {
   const uint64_t *name_off;
   const char *names;
   long maxseg;  // segments per row ([row][segment] arrays below)
-  // Query-segmented runs (the resident-reference server): segment s of every row spans the columns
-  // [seg_cols[s], seg_cols[s+1]) (one query of a batch), per-segment arrays are indexed [segment][row] (query-major,
-  // so each query's text is contiguous), row sums are per (segment, row) and histograms per segment.
-  const long *seg_cols;  // nullptr: fixed segments of kSeg columns from each row's first column
+  // The resident-reference server's batches: query q spans the columns [seg_cols[q], seg_cols[q+1]); its
+  // arrays are indexed [query][row] (so each query's text is contiguous), with per-query histograms.
+  const long *seg_cols;  // nullptr outside the server
   long nrows;            // rows of the band (the query-major stride)
   unsigned long long *seg_bytes;
   long long *seg_links, *seg_skip;

@@ -109,15 +109,20 @@ def test_service_continuous_batching_same_as_alone(oracle_bin, tmp_path):
         want.append((rc, fb if rc == 0 else None, out if rc == 0 else None, err))
     with Service(ref, Options(threshold=0.015, mode="resolve", min_overlap=500), hbm_budget=4 << 30, workers=2,
                  max_batch_queries=8, max_batch_sequences=300) as svc:
-        r = run_load(svc, stream, rate=400.0, seed=3)
+        # a Poisson stream, then a burst (everything queued at once, so that batches fill up)
+        runs = [run_load(svc, stream, rate=400.0, seed=3)]
+        b0 = svc.stats.batches
+        runs.append(run_load(svc, stream, rate=1e7, seed=4))
+        burst_batches = svc.stats.batches - b0
         stats = svc.stats
-    assert r["requests"] == len(stream) and r["ok"] == len(stream) - 1
-    for k, resp in enumerate(r["responses"]):
-        w = want[len(queries)] if k == len(stream) - 1 else want[k % len(queries)]
-        assert resp.rc == w[0], k
-        if w[0] == 0:
-            assert resp.file == w[1] and resp.stdout == w[2], k
-        else:
-            assert resp.stderr == w[3], (resp.stderr, w[3])
-    assert stats.batches < stats.done  # requests were batched together
+    for r in runs:
+        assert r["requests"] == len(stream) and r["ok"] == len(stream) - 1
+        for k, resp in enumerate(r["responses"]):
+            w = want[len(queries)] if k == len(stream) - 1 else want[k % len(queries)]
+            assert resp.rc == w[0], k
+            if w[0] == 0:
+                assert resp.file == w[1] and resp.stdout == w[2], k
+            else:
+                assert resp.stderr == w[3], (resp.stderr, w[3])
+    assert burst_batches < len(stream) - 1  # the burst's requests were batched together
     assert max(stats.batch_sequences) <= 300
