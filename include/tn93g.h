@@ -124,6 +124,18 @@ long tn93g_last_launches(tn93g_ctx *ctx);
  * [5] device->host copies, [6] whole run. Returns the number of entries written (<= n). */
 int tn93g_last_timings(tn93g_ctx *ctx, double *ms, int n);
 
+/* ---- row bands (one alignment split over several GPUs) ----
+ * tn93g_run restricted to the rows [row_begin, row_end) of the pair triangle (pairs (i, j > i) with i in the
+ * range; under -s the rows of the first file): the sink receives those rows' lines in order, the summary covers
+ * those pairs only (its mean and weights are the rows' sums added in row order from 0), and row_sums, when not
+ * NULL, receives 6 doubles per row: the row's sums for bins 0-2, then its weights for bins 0-2. Concatenating the
+ * texts of consecutive bands and adding all bands' row sums in row order gives tn93g_run's bytes and summary
+ * exactly (integer counts and histograms add, maxima take the maximum). -f hyphy (one matrix over all pairs) is
+ * refused with TN93G_EINVAL. Replaces: the row range of swifttn93.cpp:2322, 2354, 2384 (one process runs every
+ * row there). */
+int tn93g_run_rows(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_opts *opts, long row_begin,
+                   long row_end, tn93g_sink sink, void *user, double *row_sums, tn93g_summary *summary);
+
 /* ---- FASTA ----
  * tn93's reader (swifttn93.cpp:259-406) on a file held in memory: out receives malloc'ed codes (0..17 in the order
  * "ACGTURYSWKMBDHVN?-", row-major n x L), copy numbers (parsed after the last counts_sep), names and their offsets

@@ -578,7 +578,24 @@ int main(int argc, char **argv)
     else
       fprintf(A.out, "Seq1%cSeq2%cDistance\n", A.delim, A.delim);
   }
-  const long upper = cross ? (long)n1 : N;
+  long upper = cross ? (long)n1 : N, row_b = 0;
+  /* test hook: TN93_ORACLE_ROWS=B:E runs only the rows [B, E) of the pair triangle (a row band, as one rank of a
+     sharded run computes it) and TN93_ORACLE_PARTIAL=PATH writes that band's counts, maxima, histograms and
+     per-row sums (hex floats) to PATH, so the merge of bands can be checked against a whole run */
+  const char *rows_env = getenv("TN93_ORACLE_ROWS");
+  FILE *partial = NULL;
+  if (rows_env) {
+    long b = 0, e = 0;
+    if (sscanf(rows_env, "%ld:%ld", &b, &e) != 2 || b < 0 || e < b || e > upper) return 1;
+    row_b = b;
+    upper = e;
+    const char *pp = getenv("TN93_ORACLE_PARTIAL");
+    if (pp) partial = fopen(pp, "wb");
+    if (cross)
+      pairwise = (unsigned long)(N - (long)n1) * (unsigned long)(e - b);
+    else
+      pairwise = (unsigned long)((e - b) * (2 * N - b - e - 1) / 2);
+  }
   const int emit = !A.count, hy = A.format == F_HYPHY;
   double maxv[3] = {0, 0, 0}, mean[3] = {0, 0, 0}, wc[3] = {0, 0, 0};
   long links = 0, skipped = 0;
@@ -595,7 +612,7 @@ int main(int argc, char **argv)
   }
   const long BLK = 256;
   Row *rows = (Row *)calloc(BLK, sizeof(Row));
-  for (long r0 = 0; r0 < upper; r0 += BLK) {
+  for (long r0 = row_b; r0 < upper; r0 += BLK) {
     const long r1 = r0 + BLK < upper ? r0 + BLK : upper;
 #pragma omp parallel for schedule(dynamic, 1)
     for (long i = r0; i < r1; i++) {
@@ -694,6 +711,9 @@ int main(int argc, char **argv)
         wc[q] += R->lw[q];
         for (int k = 0; k < HBINS; k++) hist[q][k] += R->hist[q][k];
       }
+      if (partial)
+        fprintf(partial, "row %ld %a %a %a %a %a %a\n", i, R->lsum[0], R->lsum[1], R->lsum[2], R->lw[0], R->lw[1],
+                R->lw[2]);
       for (long t = 0; t < R->hy_n; t++) {
         long js[2] = {i, R->hy_j[t]}, other[2] = {R->hy_j[t], i};
         for (int e = 0; e < 2; e++) {
@@ -730,6 +750,16 @@ int main(int argc, char **argv)
     fputs("\n}", A.out);
   }
   fflush(A.out);
+  if (partial) {
+    fprintf(partial, "pairwise %lu\nskipped %ld\nlinks %ld\nmax %a %a %a\n", pairwise, skipped, links, maxv[0], maxv[1],
+            maxv[2]);
+    for (int q = 0; q < 3; q++) {
+      fprintf(partial, "hist%d", q);
+      for (int k = 0; k < HBINS; k++) fprintf(partial, " %lu", hist[q][k]);
+      fputc('\n', partial);
+    }
+    fclose(partial);
+  }
   if (!A.quiet)
     fprintf(stderr, "\nProgress:%8g%% (%8ld links found, %12.3g evals)", 100., links, (double)pairwise);
   fprintf(stderr, "\n");

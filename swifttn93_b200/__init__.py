@@ -30,7 +30,7 @@ EXPORTS = ("tn93g_create", "tn93g_destroy", "tn93g_strerror", "tn93g_last_cuda_e
            "tn93g_free_set", "tn93g_run", "tn93g_run_to_device", "tn93g_stream", "tn93g_last_launches",
            "tn93g_last_timings", "tn93g_pair_distances_noalloc", "tn93g_noalloc_last_error", "tn93g_read_fasta",
            "tn93g_alignment_free", "tn93g_server_create", "tn93g_server_batch", "tn93g_server_destroy",
-           "tn93g_summary_json")
+           "tn93g_summary_json", "tn93g_run_rows")
 
 
 class _Opts(C.Structure):
@@ -95,6 +95,8 @@ def load_library(path: Path | str = LIB_PATH):
     lib.tn93g_server_batch.argtypes = [C.c_void_p, C.c_int, C.POINTER(_Alignment), _QSINK, C.c_void_p,
                                        C.POINTER(_Summary)]
     lib.tn93g_server_destroy.argtypes = [C.c_void_p]
+    lib.tn93g_run_rows.argtypes = [C.c_void_p, C.c_void_p, C.c_long, C.POINTER(_Opts), C.c_long, C.c_long, _SINK,
+                                   C.c_void_p, C.c_void_p, C.POINTER(_Summary)]
     lib.tn93g_summary_json.restype = C.c_size_t
     lib.tn93g_summary_json.argtypes = [C.POINTER(_Summary), C.c_ulong, C.c_ulong, C.c_int, C.c_int, C.c_char_p,
                                        C.c_size_t]
@@ -275,6 +277,26 @@ class Engine:
             n1 = s.N
         self._check(self.lib.tn93g_run(self.ctx, s.handle, int(n1), C.byref(o), cb, None, C.byref(S)))
         return b"".join(chunks), self._summary(S)
+
+    def run_rows(self, s: DeviceSet, opts: Options, row_begin: int, row_end: int, n1: int | None = None):
+        """tn93g_run_rows: the rows [row_begin, row_end) only. Returns (text bytes of those rows, Summary of their
+        pairs, per-row sums as a float64 array [rows, 6]: sums of bins 0-2, then weights of bins 0-2)."""
+        chunks = []
+
+        def _sink(_user, ptr, n):
+            try:
+                chunks.append(C.string_at(ptr, n))
+                return 0
+            except Exception:  # noqa: BLE001 - an exception must not unwind through C
+                return 1
+
+        cb = _SINK(_sink)
+        o = opts.to_c()
+        S = _Summary()
+        rows = np.zeros((max(0, row_end - row_begin), 6), dtype=np.float64)
+        self._check(self.lib.tn93g_run_rows(self.ctx, s.handle, int(s.N if n1 is None else n1), C.byref(o),
+                                            int(row_begin), int(row_end), cb, None, rows.ctypes.data, C.byref(S)))
+        return b"".join(chunks), self._summary(S), rows
 
     def run_to_device(self, s: DeviceSet, opts: Options, n1: int | None = None):
         """Runs all pairs with the distance file left in HBM; returns (device pointer, nbytes, Summary)."""

@@ -1390,12 +1390,20 @@ void *tn93g_stream(tn93g_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr;
 long tn93g_last_launches(tn93g_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
 static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_opts *opts, tn93g_sink sink, void *user,
-                    tn93g_summary *sum, bool to_device);
+                    tn93g_summary *sum, bool to_device, long row_begin = 0, long row_end = -1,
+                    double *row_sums = nullptr);
 
 int tn93g_run(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_opts *opts, tn93g_sink sink, void *user,
               tn93g_summary *sum)
 {
   return run_impl(ctx, set, n1, opts, sink, user, sum, false);
+}
+
+int tn93g_run_rows(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_opts *opts, long row_begin,
+                   long row_end, tn93g_sink sink, void *user, double *row_sums, tn93g_summary *sum)
+{
+  if (!opts || opts->format == TN93G_HYPHY || row_begin < 0 || row_end < row_begin) return TN93G_EINVAL;
+  return run_impl(ctx, set, n1, opts, sink, user, sum, false, row_begin, row_end, row_sums);
 }
 
 int tn93g_run_to_device(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_opts *opts, void **dev_out,
@@ -1409,7 +1417,7 @@ int tn93g_run_to_device(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn9
 }
 
 static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_opts *opts, tn93g_sink sink, void *user,
-                    tn93g_summary *sum, bool to_device)
+                    tn93g_summary *sum, bool to_device, long row_begin, long row_end, double *row_sums)
 {
   if (!ctx || !set || !opts || !sum || n1 <= 0 || n1 > set->N) return TN93G_EINVAL;
   if (opts->mode < 0 || opts->mode > 4 || opts->format < 0 || opts->format > 2) return TN93G_EINVAL;
@@ -1536,10 +1544,17 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   CU(cudaEventRecord(E[1], st));
 
   //------------------------------------------------------------------ bands
-  const long upper = rc.cross ? n1 : N;
+  // rows of the pair triangle (or of the first file under -s): all of them, or the caller's range
+  const long all_rows = rc.cross ? n1 : N;
+  if (row_end < 0) row_end = all_rows;
+  if (row_begin > all_rows || row_end > all_rows) return TN93G_EINVAL;
+  const long upper = row_end;
   const long colbase = rc.cross ? n1 : 0;
   const long ncols = N - colbase;
-  sum->pairwise = rc.cross ? (unsigned long)(N - n1) * (unsigned long)n1 : (unsigned long)(N - 1) * (unsigned long)N / 2;
+  if (rc.cross)
+    sum->pairwise = (unsigned long)(N - n1) * (unsigned long)(row_end - row_begin);
+  else  // pairs (i, j > i) of rows [row_begin, row_end)
+    sum->pairwise = (unsigned long)((row_end - row_begin) * (2 * N - row_begin - row_end - 1) / 2);
   // Band schedule. When the text goes to the host, a band holds about 3 M pairs (at most 16 M pair slots), so
   // that the copy of one band overlaps the kernels of the next; otherwise up to 64 M slots (512 MB of distances).
   const bool stream_text = !(to_device || hyphy || !rc.emit);
@@ -1551,7 +1566,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   const long cap_slots = stream_text ? (16l << 20) : (64l << 20);
   std::vector<std::pair<long, long>> bands;
   long maxrows = 1;
-  for (long r0 = 0; r0 < upper;) {
+  for (long r0 = row_begin; r0 < upper;) {
     long r = r0, pairs = 0;
     while (r < upper && (r == r0 || ((r - r0 + 1) * ncols <= cap_slots && pairs < target_pairs &&
                                      r - r0 < 65535l * kTile))) {
@@ -1757,6 +1772,13 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
       for (int q = 0; q < 3; q++) {
         mean[q] += h.sum[r * 3 + q];
         wc[q] += h.w[r * 3 + q];
+      }
+      if (row_sums) {
+        double *o = row_sums + (size_t)(bands[bi].first - row_begin + r) * 6;
+        for (int q = 0; q < 3; q++) {
+          o[q] = h.sum[r * 3 + q];
+          o[3 + q] = h.w[r * 3 + q];
+        }
       }
     }
     const unsigned long long tot = *h.total;
