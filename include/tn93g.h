@@ -136,12 +136,8 @@ int tn93g_last_timings(tn93g_ctx *ctx, double *ms, int n);
 int tn93g_run_rows(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_opts *opts, long row_begin,
                    long row_end, tn93g_sink sink, void *user, double *row_sums, tn93g_summary *summary);
 
-/* ---- FASTA ----
- * tn93's reader (swifttn93.cpp:259-406) on a file held in memory: out receives malloc'ed codes (0..17 in the order
- * "ACGTURYSWKMBDHVN?-", row-major n x L), copy numbers (parsed after the last counts_sep), names and their offsets
- * and lengths, in the layout tn93g_upload takes. expect_len > 0 requires that sequence length (a second file, as
- * tn93 -s reads it after the first). On a refusal it returns TN93G_EFASTA with the message tn93 prints in msg.
- * Replaces: read_fasta (swifttn93.cpp:292-406), which tn93 runs on a FILE*. */
+/* An alignment in host memory: n sequences of length L, codes 0..17 in the order "ACGTURYSWKMBDHVN?-" (row-major),
+ * copy numbers, and names (name k is names[name_off[k] .. name_off[k] + name_len[k])). */
 typedef struct tn93g_alignment {
   uint8_t *codes;
   long n, L;
@@ -151,6 +147,28 @@ typedef struct tn93g_alignment {
   long *name_len;
 } tn93g_alignment;
 
+/* Receives the whole distance file body of query (or batch alignment) number `query` (bytes valid only during the
+ * call); non-zero aborts the call with TN93G_ESINK. */
+typedef int (*tn93g_query_sink)(void *user, int query, const char *bytes, size_t n);
+
+/* ---- batches of independent alignments ----
+ * Runs K alignments (each with its own options; csv or csvn, no -m) in one pass: packing per alignment, one
+ * persistent pair launch per kernel class over a queue of every alignment's tiles (longest alignments first), then
+ * batched replay, statistics, sums, scan, per-alignment reduction and text. sink(user, k, bytes, n) receives
+ * alignment k's whole distance file body and sums[k] its summary, exactly as tn93g_run on that alignment alone
+ * would give them. rows_per_warp (NULL: 4) picks each alignment's pair-tile height (8 x 1, 2 or 4 rows by 32
+ * columns) and pair_blocks (0: 2) the resident blocks per SM of the pair kernel (2 or 3); neither changes a result.
+ * Replaces: one tn93 process per alignment (swifttn93.cpp:2222-2966 runs one file). */
+int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *alignments, const tn93g_opts *opts,
+                    const int *rows_per_warp, int pair_blocks, tn93g_query_sink sink, void *user,
+                    tn93g_summary *sums);
+
+/* ---- FASTA ----
+ * tn93's reader (swifttn93.cpp:259-406) on a file held in memory: out receives malloc'ed codes (0..17 in the order
+ * "ACGTURYSWKMBDHVN?-", row-major n x L), copy numbers (parsed after the last counts_sep), names and their offsets
+ * and lengths, in the layout tn93g_upload takes. expect_len > 0 requires that sequence length (a second file, as
+ * tn93 -s reads it after the first). On a refusal it returns TN93G_EFASTA with the message tn93 prints in msg.
+ * Replaces: read_fasta (swifttn93.cpp:292-406), which tn93 runs on a FILE*. */
 int tn93g_read_fasta(const char *bytes, size_t nbytes, long expect_len, char counts_sep, tn93g_alignment *out,
                      char *msg, size_t msg_cap);
 void tn93g_alignment_free(tn93g_alignment *a);
@@ -162,9 +180,6 @@ void tn93g_alignment_free(tn93g_alignment *a);
  * and csvn indices are global (reference first, then the query). Replaces: nothing in the reference, which reads
  * both files on every call (swifttn93.cpp:2243-2254); the per-query semantics are its -s mode. */
 typedef struct tn93g_server tn93g_server;
-
-/* Receives query q's whole distance file body (bytes valid only during the call); non-zero aborts. */
-typedef int (*tn93g_query_sink)(void *user, int query, const char *bytes, size_t n);
 
 /* Packs the reference (arguments as tn93g_upload) and allocates, within the context's HBM budget, every per-batch
  * buffer for batches of up to max_batch_sequences query sequences in up to max_batch_queries queries (about

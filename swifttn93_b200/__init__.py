@@ -30,7 +30,7 @@ EXPORTS = ("tn93g_create", "tn93g_destroy", "tn93g_strerror", "tn93g_last_cuda_e
            "tn93g_free_set", "tn93g_run", "tn93g_run_to_device", "tn93g_stream", "tn93g_last_launches",
            "tn93g_last_timings", "tn93g_pair_distances_noalloc", "tn93g_noalloc_last_error", "tn93g_read_fasta",
            "tn93g_alignment_free", "tn93g_server_create", "tn93g_server_batch", "tn93g_server_destroy",
-           "tn93g_summary_json", "tn93g_run_rows")
+           "tn93g_summary_json", "tn93g_run_rows", "tn93g_batch_run")
 
 
 class _Opts(C.Structure):
@@ -97,6 +97,8 @@ def load_library(path: Path | str = LIB_PATH):
     lib.tn93g_server_destroy.argtypes = [C.c_void_p]
     lib.tn93g_run_rows.argtypes = [C.c_void_p, C.c_void_p, C.c_long, C.POINTER(_Opts), C.c_long, C.c_long, _SINK,
                                    C.c_void_p, C.c_void_p, C.POINTER(_Summary)]
+    lib.tn93g_batch_run.argtypes = [C.c_void_p, C.c_int, C.POINTER(_Alignment), C.POINTER(_Opts),
+                                    C.POINTER(C.c_int), C.c_int, _QSINK, C.c_void_p, C.POINTER(_Summary)]
     lib.tn93g_summary_json.restype = C.c_size_t
     lib.tn93g_summary_json.argtypes = [C.POINTER(_Summary), C.c_ulong, C.c_ulong, C.c_int, C.c_int, C.c_char_p,
                                        C.c_size_t]
@@ -171,6 +173,31 @@ class Tn93Error(RuntimeError):
 
 class FastaError(Tn93Error):
     """The FASTA reader refused the input; str(e) is the message tn93 prints (it then exits with status 1)."""
+
+
+class HostAlignment:
+    """An alignment from arrays (codes uint8 [n, L] in 0..17, names, copy numbers), laid out as tn93g_alignment
+    for the batch and server calls (the arrays are kept alive by this object)."""
+
+    def __init__(self, codes: np.ndarray, names, counts=None):
+        self._codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        self.n, self.L = self._codes.shape
+        nb = [x.encode() if isinstance(x, str) else bytes(x) for x in names]
+        self._names = C.create_string_buffer(b"".join(nb) + b"\0")
+        self._off = np.zeros(self.n, dtype=np.uint64)
+        if self.n > 1:
+            self._off[1:] = np.cumsum([len(b) for b in nb[:-1]])
+        self._len = np.array([len(b) for b in nb], dtype=np.int64)
+        self._cnt = (np.ones(self.n, dtype=np.int64) if counts is None
+                     else np.ascontiguousarray(counts, dtype=np.int64))
+        a = _Alignment()
+        a.codes = self._codes.ctypes.data_as(C.POINTER(C.c_uint8))
+        a.n, a.L = self.n, self.L
+        a.copy_counts = self._cnt.ctypes.data_as(C.POINTER(C.c_long))
+        a.names = C.cast(self._names, C.POINTER(C.c_char))
+        a.name_off = self._off.ctypes.data_as(C.POINTER(C.c_size_t))
+        a.name_len = self._len.ctypes.data_as(C.POINTER(C.c_long))
+        self._a = a
 
 
 class Fasta:
@@ -306,6 +333,38 @@ class Engine:
         self._check(self.lib.tn93g_run_to_device(self.ctx, s.handle, int(s.N if n1 is None else n1), C.byref(o),
                                                  C.byref(ptr), C.byref(nb), C.byref(S)))
         return ptr.value, nb.value, self._summary(S)
+
+    def batch_run(self, alignments: list, opts: list, rows_per_warp=None, pair_blocks: int = 0) -> list:
+        """tn93g_batch_run: many alignments (HostAlignment or Fasta objects), each with its own Options, in one pass.
+        Returns [(body bytes, Summary)], each equal to run() on that alignment alone."""
+        K = len(alignments)
+        arr = (_Alignment * K)(*[a._a for a in alignments])
+        oc = (_Opts * K)(*[o.to_c() for o in opts])
+        rpw = None if rows_per_warp is None else (C.c_int * K)(*[int(x) for x in rows_per_warp])
+        sums = (_Summary * K)()
+        bodies = [[] for _ in range(K)]
+
+        def _sink(_user, k, ptr, n):
+            try:
+                bodies[k].append(C.string_at(ptr, n))
+                return 0
+            except Exception:  # noqa: BLE001 - an exception must not unwind through C
+                return 1
+
+        cb = _QSINK(_sink)
+        self._check(self.lib.tn93g_batch_run(self.ctx, K, arr, oc, rpw, int(pair_blocks), cb, None, sums))
+        out = []
+        for k in range(K):
+            S = _Summary()
+            C.memmove(C.byref(S), C.byref(sums[k]), C.sizeof(_Summary))
+            out.append((b"".join(bodies[k]), _plain_summary(S)))
+        return out
+
+    def last_timings(self) -> dict:
+        """Device milliseconds of the last call's stages (pack, pair, replay, rows, write, d2h, total)."""
+        t = (C.c_double * 7)()
+        k = self.lib.tn93g_last_timings(self.ctx, t, 7)
+        return {self.STAGES[q]: t[q] for q in range(k)}
 
     @property
     def stream(self) -> int:

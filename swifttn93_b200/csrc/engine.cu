@@ -280,24 +280,21 @@ __device__ __forceinline__ void pair_epilogue(const PairArgs &a, const AggEntry 
   }
 }
 
-template <bool WPLANE, bool GAPMM, int MINB>
-__global__ void __launch_bounds__(256, MINB) pair_kernel(PairArgs a)
+// One tile of pairs: rows [i0, i0 + 8 * rpw) (rpw = rows per warp, 1..4) x columns [j0, j0 + 32). The block's
+// agg table must be in sagg. All threads of the block call it with the same arguments.
+template <bool WPLANE, bool GAPMM>
+__device__ __forceinline__ void pair_tile(const PairArgs &a, const AggEntry *sagg, int *colacc, long i0, long j0,
+                                          int rpw)
 {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  AggEntry *sagg = reinterpret_cast<AggEntry *>(smem_raw);
-  int *colacc = reinterpret_cast<int *>(smem_raw + (size_t)kAggInts * 4);
   const RunConsts &rc = a.rc;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const long i0 = a.r0 + blockIdx.y * (long)kTile;
-  const long j0 = a.cstart + blockIdx.x * (long)kTile;
+  const int trows = kWarps * rpw;
   // block-uniform exits: no valid pair in the tile
   if (i0 >= a.r1 || j0 >= rc.N) return;
   if (!rc.cross && j0 + kTile - 1 <= i0) return;
-  for (int t = threadIdx.x; t < kAggInts; t += blockDim.x) ((int32_t *)sagg)[t] = ((const int32_t *)a.agg)[t];
-  __syncthreads();
   const long Np = rc.Npad;
   // ---- column-side sparse events: lane = tile row, warp-uniform column; skipped where the row is sparse too
-  {
+  if (lane < trows) {
     const long ib = min(i0 + lane, rc.N - 1);
     for (int cl = warp; cl < kTile; cl += kWarps) {
       const long j = j0 + cl;
@@ -323,7 +320,7 @@ __global__ void __launch_bounds__(256, MINB) pair_kernel(PairArgs a)
   const long jj = j < rc.N ? j : rc.N - 1;
   int namb = 0, nund = 0;
 #pragma unroll 1
-  for (int r = 0; r < kRowsPerWarp; r++) {
+  for (int r = 0; r < rpw; r++) {
     const long i = i0 + warp + kWarps * r;
     if (i >= a.r1) break;
     const long lb = rc.cross ? rc.n1 : i + 1;
@@ -371,6 +368,60 @@ __global__ void __launch_bounds__(256, MINB) pair_kernel(PairArgs a)
   count_flags(a.counters, namb, nund);
 }
 
+template <bool WPLANE, bool GAPMM, int MINB>
+__global__ void __launch_bounds__(256, MINB) pair_kernel(PairArgs a)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  AggEntry *sagg = reinterpret_cast<AggEntry *>(smem_raw);
+  int *colacc = reinterpret_cast<int *>(smem_raw + (size_t)kAggInts * 4);
+  const long i0 = a.r0 + blockIdx.y * (long)kTile;
+  const long j0 = a.cstart + blockIdx.x * (long)kTile;
+  if (i0 >= a.r1 || j0 >= a.rc.N || (!a.rc.cross && j0 + kTile - 1 <= i0)) return;
+  for (int t = threadIdx.x; t < kAggInts; t += blockDim.x) ((int32_t *)sagg)[t] = ((const int32_t *)a.agg)[t];
+  __syncthreads();
+  pair_tile<WPLANE, GAPMM>(a, sagg, colacc, i0, j0, kRowsPerWarp);
+}
+
+static_assert(sizeof(PairArgs) % 4 == 0, "PairArgs is copied as 32-bit words");
+
+// A tile of a batch: alignment k, first row i0, first column j0, rows per warp.
+struct BatchTile {
+  int k, rpw;
+  int i0, j0;
+};
+
+// Batched pair kernel over many alignments: a persistent grid takes tiles from a queue (one atomic per tile),
+// loads the tile's alignment descriptor and agg table into shared memory when the alignment changes, and runs
+// pair_tile. Tiles are ordered longest alignments first, so the tail is short.
+template <bool WPLANE, bool GAPMM, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+    pair_batch_kernel(const PairArgs *descs, const BatchTile *tiles, int ntiles, unsigned *next)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  AggEntry *sagg = reinterpret_cast<AggEntry *>(smem_raw);
+  int *colacc = reinterpret_cast<int *>(smem_raw + (size_t)kAggInts * 4);
+  __shared__ __align__(16) PairArgs sd;
+  __shared__ int s_t;
+  int cur = -1;
+  for (;;) {
+    if (threadIdx.x == 0) s_t = (int)atomicAdd(next, 1u);
+    __syncthreads();
+    const int t = s_t;
+    if (t >= ntiles) break;
+    const BatchTile T = tiles[t];
+    if (T.k != cur) {
+      for (int q = threadIdx.x; q < (int)(sizeof(PairArgs) / 4); q += blockDim.x)
+        reinterpret_cast<int32_t *>(&sd)[q] = reinterpret_cast<const int32_t *>(&descs[T.k])[q];
+      __syncthreads();
+      for (int q = threadIdx.x; q < kAggInts; q += blockDim.x) ((int32_t *)sagg)[q] = ((const int32_t *)sd.agg)[q];
+      cur = T.k;
+    }
+    __syncthreads();
+    pair_tile<WPLANE, GAPMM>(sd, sagg, colacc, T.i0, T.j0, T.rpw);
+    __syncthreads();
+  }
+}
+
 //------------------------------------------------------------------------------------------------ replay
 // position of the n-th set bit (0-based) of x; x has more than n set bits
 __device__ __forceinline__ int nth_bit32(unsigned x, int n)
@@ -394,7 +445,7 @@ __device__ __forceinline__ int nth_bit32(unsigned x, int n)
 //     order) and lane q adds the site's contribution to float cell q, so each cell is summed in site order as
 //     tn93 does; lanes 16..19 add the integer diagonal resolutions, lane 20 the ambiguity count;
 //   * lane 0: tn93's c1-major merge of float and integer cells, the -l / -g tests and the formula.
-__global__ void __launch_bounds__(256) replay_kernel(ReplayArgs a)
+__device__ __forceinline__ void replay_run(const ReplayArgs &a)
 {
   __shared__ unsigned char sc1[kWarps][64], sc2[kWarps][64];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -498,6 +549,15 @@ __global__ void __launch_bounds__(256) replay_kernel(ReplayArgs a)
       if (qund) atomicAdd(&a.counters[1], 1ull);
     }
   }
+}
+
+__global__ void __launch_bounds__(256) replay_kernel(ReplayArgs a) { replay_run(a); }
+
+// the replay queues of a batch's alignments, one after the other (each is usually empty or short)
+__global__ void __launch_bounds__(256) replay_batch_kernel(const ReplayArgs *descs, int K)
+{
+  for (int k = 0; k < K; k++)
+    if (*descs[k].qn) replay_run(descs[k]);
 }
 
 // exclusive scan of a band's segment byte counts (one block), and the band total
@@ -649,15 +709,14 @@ __device__ __forceinline__ int self_len(const RowArgs &a, long i)
 constexpr int kSeg = 1024;
 
 // one warp per (row, segment): histogram, links, skips, maxima and the byte count of the segment's text
-__global__ void __launch_bounds__(256) stats_kernel(RowArgs a)
+__device__ __forceinline__ void stats_rows(const RowArgs &a, long bx, int sg)
 {
   __shared__ unsigned long long sh[3 * kHistBins];
   for (int t = threadIdx.x; t < 3 * kHistBins; t += blockDim.x) sh[t] = 0;
   __syncthreads();
   const RunConsts &rc = a.rc;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const long i = a.r0 + blockIdx.x * (long)kWarps + warp;
-  const int sg = blockIdx.y;
+  const long i = a.r0 + bx * kWarps + warp;
   if (i < a.r1) {
     const long r = i - a.r0;
     const long slot = r * a.maxseg + sg;
@@ -729,15 +788,17 @@ __global__ void __launch_bounds__(256) stats_kernel(RowArgs a)
     if (sh[t]) atomicAdd(&a.hist[t], sh[t]);
 }
 
+__global__ void __launch_bounds__(256) stats_kernel(RowArgs a) { stats_rows(a, blockIdx.x, blockIdx.y); }
+
 // one warp per row: tn93's row sums in column order (swifttn93.cpp:2594-2602); lane 0 adds each chunk's terms in
 // order. The self-pair weights come first, as tn93 adds them when the row starts (swifttn93.cpp:2405-2415).
-__global__ void __launch_bounds__(256) sum_kernel(RowArgs a)
+__device__ __forceinline__ void sum_rows(const RowArgs &a, long bx)
 {
   __shared__ double sterm[kWarps][32], sw[kWarps][32];
   __shared__ unsigned char sbin[kWarps][32];
   const RunConsts &rc = a.rc;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const long i = a.r0 + blockIdx.x * (long)kWarps + warp;
+  const long i = a.r0 + bx * kWarps + warp;
   if (i >= a.r1) return;
   const long cnt_i = a.counts[i];
   double s0 = 0., s1 = 0., s2 = 0., w0 = 0., w1 = 0., w2 = 0.;
@@ -807,6 +868,8 @@ __global__ void __launch_bounds__(256) sum_kernel(RowArgs a)
   }
 }
 
+__global__ void __launch_bounds__(256) sum_kernel(RowArgs a) { sum_rows(a, blockIdx.x); }
+
 __device__ __forceinline__ char *put_bytes(char *o, const char *s, int n)
 {
   for (int k = 0; k < n; k++) o[k] = s[k];
@@ -867,13 +930,12 @@ struct Stager {
 };
 
 // one warp per (row, segment): the segment's text at its scanned offset (the row's self line in segment 0)
-__global__ void __launch_bounds__(256) write_kernel(RowArgs a)
+__device__ __forceinline__ void write_rows(const RowArgs &a, long bx, int sg)
 {
   __shared__ __align__(16) char stage[kWarps][kStage];
   const RunConsts &rc = a.rc;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const long i = a.r0 + blockIdx.x * (long)kWarps + warp;
-  const int sg = blockIdx.y;
+  const long i = a.r0 + bx * kWarps + warp;
   if (i >= a.r1) return;
   const long slot = (i - a.r0) * a.maxseg + sg;
   const long lb = rc.cross ? rc.n1 : i + 1;
@@ -958,6 +1020,89 @@ __global__ void __launch_bounds__(256) write_kernel(RowArgs a)
   }
   S.flush(lane);
   if (S.over && lane == 0) atomicAdd(a.err, 1ull);
+}
+
+__global__ void __launch_bounds__(256) write_kernel(RowArgs a) { write_rows(a, blockIdx.x, blockIdx.y); }
+
+// Batched row stage: block b of the batch is row block blocks[b].y of alignment blocks[b].x; blockIdx.y is the
+// segment (blocks past an alignment's segment count exit).
+__global__ void __launch_bounds__(256) stats_batch_kernel(const RowArgs *descs, const int2 *blocks)
+{
+  const int2 B = blocks[blockIdx.x];
+  const RowArgs &a = descs[B.x];
+  if ((long)blockIdx.y >= a.maxseg) return;
+  stats_rows(a, B.y, blockIdx.y);
+}
+
+__global__ void __launch_bounds__(256) sum_batch_kernel(const RowArgs *descs, const int2 *blocks)
+{
+  const int2 B = blocks[blockIdx.x];
+  sum_rows(descs[B.x], B.y);
+}
+
+__global__ void __launch_bounds__(256) write_batch_kernel(const RowArgs *descs, const int2 *blocks)
+{
+  const int2 B = blocks[blockIdx.x];
+  const RowArgs &a = descs[B.x];
+  if ((long)blockIdx.y >= a.maxseg) return;
+  write_rows(a, B.y, blockIdx.y);
+}
+
+// Per alignment of a batch (single-file runs, bin 0 only): links, skips and maximum over its (row, segment)
+// slots, and tn93's mean numerator and weight: the rows' sums added in row order from 0 (swifttn93.cpp:2838-2848).
+// One block per alignment; thread 0 adds a shared-memory stage of the row sums in order.
+__global__ void __launch_bounds__(256) aln_reduce_kernel(const RowArgs *descs, double *out /* [K][3] */,
+                                                         long long *cnt /* [K][2] */)
+{
+  __shared__ double ss[2048], sw[2048];
+  __shared__ long long rl[8], rs[8];
+  __shared__ double rm[8];
+  const RowArgs &a = descs[blockIdx.x];
+  const long nr = a.r1 - a.r0, ms = a.maxseg;
+  long long links = 0, skipped = 0;
+  double m = 0., s0 = 0., w0 = 0.;
+  for (long g = threadIdx.x; g < nr * ms; g += 256) {
+    links += a.seg_links[g];
+    skipped += a.seg_skip[g];
+    m = fmax(m, a.seg_max[g * 3]);
+  }
+  for (long r0 = 0; r0 < nr; r0 += 2048) {
+    const int n = (int)min(2048l, nr - r0);
+    for (int k = threadIdx.x; k < n; k += 256) {
+      ss[k] = a.row_sum[(r0 + k) * 3];
+      sw[k] = a.row_w[(r0 + k) * 3];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int k = 0; k < n; k++) {
+        s0 = __dadd_rn(s0, ss[k]);
+        w0 = __dadd_rn(w0, sw[k]);
+      }
+    __syncthreads();
+  }
+  for (int o = 16; o; o >>= 1) {
+    links += __shfl_xor_sync(0xffffffffu, links, o);
+    skipped += __shfl_xor_sync(0xffffffffu, skipped, o);
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    rl[threadIdx.x >> 5] = links;
+    rs[threadIdx.x >> 5] = skipped;
+    rm[threadIdx.x >> 5] = m;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < 8; w++) {
+      links += rl[w];
+      skipped += rs[w];
+      m = fmax(m, rm[w]);
+    }
+    out[blockIdx.x * 3] = m;
+    out[blockIdx.x * 3 + 1] = s0;
+    out[blockIdx.x * 3 + 2] = w0;
+    cnt[blockIdx.x * 2] = links;
+    cnt[blockIdx.x * 2 + 1] = skipped;
+  }
 }
 
 // -f hyphy: per matrix row the byte count, then the text: "\n{" d(r,0) "," ... "}" with 0 on the diagonal, the
@@ -1115,6 +1260,7 @@ struct tn93g_ctx {
   double timings[8] = {0};
   long launches = 0;
   size_t dev_out_n = 0;
+  DevBuf bb[48];  // buffers of tn93g_batch_run (indexed by BatchBuf)
 };
 
 namespace {
@@ -1278,6 +1424,8 @@ void tn93g_destroy(tn93g_ctx *ctx)
                     &ctx->roff, &ctx->out, &ctx->hy};
   for (DevBuf *b : bufs)
     if (b->p) cudaFree(b->p);
+  for (DevBuf &b : ctx->bb)
+    if (b.p) cudaFree(b.p);
   if (ctx->d_logt) cudaFree(ctx->d_logt);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   for (int q = 0; q < 2; q++) {
@@ -2797,3 +2945,498 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
 }
 
 }  // extern "C"
+
+//================================================================================================== batched runs
+// Many independent alignments in one pass (each with its own options): every stage runs over all of them at once.
+// Packing is per alignment on one stream; the pair stage is one persistent launch per kernel class over a queue of
+// all alignments' tiles (longest alignments first); the replay, statistics, sums, scan, reduction and text are
+// batched kernels over all alignments' rows. Each alignment's output equals its own tn93g_run byte for byte.
+namespace {
+
+enum BatchBuf {
+  BB_CODES, BB_SEEN, BB_NN, BB_VARCOL, BB_PLANES, BB_CC, BB_CCT, BB_EVCOUNT, BB_EVOFF, BB_EV, BB_AGG, BB_SITE,
+  BB_NAMES, BB_NAMEOFF, BB_NAMELEN, BB_COUNTS, BB_DIST, BB_RQ, BB_RQN, BB_COUNTERS, BB_PDESC, BB_RDESC, BB_ROWDESC,
+  BB_TILES, BB_NEXT, BB_BLOCKS, BB_SBYTES, BB_SOFF, BB_SLINKS, BB_SSKIP, BB_SMAX, BB_RSUM, BB_RW, BB_HIST, BB_TOTAL,
+  BB_SCANTMP, BB_RED, BB_REDC, BB_FIRST, BB_FIRSTIDX, BB_OUT, BB_COUNT
+};
+static_assert(BB_COUNT <= 48, "batch buffer table");
+
+__global__ void gather_u64_kernel(const unsigned long long *src, const long *idx, unsigned long long *dst, int n)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) dst[k] = src[idx[k]];
+}
+
+template <int MINB>
+cudaError_t launch_pair_batch_t(bool wplane, bool gapmm, const PairArgs *descs, const BatchTile *tiles, int ntiles,
+                                unsigned *next, cudaStream_t st)
+{
+  const dim3 g(148 * MINB);
+  if (gapmm) {
+    cudaFuncSetAttribute(pair_batch_kernel<true, true, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kPairSmem);
+    pair_batch_kernel<true, true, MINB><<<g, 256, kPairSmem, st>>>(descs, tiles, ntiles, next);
+  } else if (wplane) {
+    cudaFuncSetAttribute(pair_batch_kernel<true, false, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kPairSmem);
+    pair_batch_kernel<true, false, MINB><<<g, 256, kPairSmem, st>>>(descs, tiles, ntiles, next);
+  } else {
+    cudaFuncSetAttribute(pair_batch_kernel<false, false, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kPairSmem);
+    pair_batch_kernel<false, false, MINB><<<g, 256, kPairSmem, st>>>(descs, tiles, ntiles, next);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *alns, const tn93g_opts *opts,
+                               const int *rows_per_warp, int pair_blocks, tn93g_query_sink sink, void *user,
+                               tn93g_summary *sums)
+{
+  if (!ctx || K <= 0 || !alns || !opts || !sums) return TN93G_EINVAL;
+  for (int k = 0; k < K; k++) {
+    const tn93g_alignment &A = alns[k];
+    const tn93g_opts &o = opts[k];
+    if (A.n <= 0 || A.L <= 0 || !A.codes || !A.copy_counts || !A.names || !A.name_off || !A.name_len)
+      return TN93G_EINVAL;
+    if (o.mode < 0 || o.mode > 4 || (o.format != TN93G_CSV && o.format != TN93G_CSVN) || o.do_fst) return TN93G_EINVAL;
+    if (A.L >= (1l << 25) || A.n >= (1l << 31)) return TN93G_ETOOBIG;
+    if (rows_per_warp && rows_per_warp[k] != 1 && rows_per_warp[k] != 2 && rows_per_warp[k] != 4) return TN93G_EINVAL;
+  }
+  if (pair_blocks == 0) pair_blocks = 2;
+  if (pair_blocks != 2 && pair_blocks != 3) return TN93G_EINVAL;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  for (double &t : ctx->timings) t = 0;
+  ctx->launches = 0;
+  DevBuf *bb = ctx->bb;
+  cudaEvent_t *E = ctx->evs;
+  float ms = 0.f;
+  CU(cudaEventRecord(E[0], st));
+  //------------------------------------------------------------------ inputs
+  std::vector<size_t> code_off(K + 1), seen_off(K + 1), name_base(K + 1), row_base(K + 1);
+  code_off[0] = seen_off[0] = name_base[0] = row_base[0] = 0;
+  for (int k = 0; k < K; k++) {
+    size_t nb = 0;
+    for (long i = 0; i < alns[k].n; i++) nb = std::max(nb, alns[k].name_off[i] + (size_t)alns[k].name_len[i]);
+    code_off[k + 1] = code_off[k] + (size_t)alns[k].n * alns[k].L;
+    seen_off[k + 1] = seen_off[k] + alns[k].L;
+    name_base[k + 1] = name_base[k] + nb;
+    row_base[k + 1] = row_base[k] + alns[k].n;
+  }
+  const size_t NR = row_base[K];
+  TRY(ensure(ctx, bb[BB_CODES], code_off[K]));
+  TRY(ensure(ctx, bb[BB_NAMES], name_base[K] + 1));
+  TRY(ensure(ctx, bb[BB_NAMEOFF], NR * sizeof(uint64_t)));
+  TRY(ensure(ctx, bb[BB_NAMELEN], NR * sizeof(int32_t)));
+  TRY(ensure(ctx, bb[BB_COUNTS], NR * sizeof(long)));
+  std::vector<uint64_t> noff(NR);
+  std::vector<int32_t> nlen(NR);
+  std::vector<long> cnts(NR);
+  for (int k = 0; k < K; k++) {
+    CU(cudaMemcpyAsync((uint8_t *)bb[BB_CODES].p + code_off[k], alns[k].codes, code_off[k + 1] - code_off[k],
+                       cudaMemcpyHostToDevice, st));
+    if (name_base[k + 1] > name_base[k])
+      CU(cudaMemcpyAsync((char *)bb[BB_NAMES].p + name_base[k], alns[k].names, name_base[k + 1] - name_base[k],
+                         cudaMemcpyHostToDevice, st));
+    for (long i = 0; i < alns[k].n; i++) {
+      noff[row_base[k] + i] = name_base[k] + alns[k].name_off[i];
+      nlen[row_base[k] + i] = (int32_t)alns[k].name_len[i];
+      cnts[row_base[k] + i] = alns[k].copy_counts[i];
+    }
+  }
+  CU(cudaMemcpyAsync(bb[BB_NAMEOFF].p, noff.data(), NR * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(bb[BB_NAMELEN].p, nlen.data(), NR * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(bb[BB_COUNTS].p, cnts.data(), NR * sizeof(long), cudaMemcpyHostToDevice, st));
+  //------------------------------------------------------------------ column scan and folding
+  TRY(ensure(ctx, bb[BB_SEEN], seen_off[K] * sizeof(uint32_t)));
+  TRY(ensure(ctx, bb[BB_NN], K * sizeof(unsigned long long)));
+  CU(cudaMemsetAsync(bb[BB_SEEN].p, 0, seen_off[K] * sizeof(uint32_t), st));
+  CU(cudaMemsetAsync(bb[BB_NN].p, 0, K * sizeof(unsigned long long), st));
+  for (int k = 0; k < K; k++) {
+    const long N = alns[k].n, L = alns[k].L;
+    colscan_kernel<<<dim3((unsigned)((L + 255) / 256), (unsigned)((N + 63) / 64)), 256, 0, st>>>(
+        (const uint8_t *)bb[BB_CODES].p + code_off[k], N, L, (uint32_t *)bb[BB_SEEN].p + seen_off[k],
+        (unsigned long long *)bb[BB_NN].p + k);
+    CU(cudaGetLastError());
+    ctx->launches++;
+  }
+  std::vector<uint32_t> seen(seen_off[K]);
+  std::vector<unsigned long long> nN(K);
+  CU(cudaMemcpyAsync(seen.data(), bb[BB_SEEN].p, seen_off[K] * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(nN.data(), bb[BB_NN].p, K * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  std::vector<RunConsts> RC(K);
+  std::vector<int32_t> varcol;
+  std::vector<size_t> vc_off(K + 1), pl_off(K + 1), cc_off(K + 1), cct_off(K + 1), evo_off(K + 1);
+  vc_off[0] = pl_off[0] = cc_off[0] = cct_off[0] = evo_off[0] = 0;
+  for (int k = 0; k < K; k++) {
+    const long N = alns[k].n, L = alns[k].L;
+    const tn93g_opts *o = &opts[k];
+    RunConsts &rc = RC[k];
+    memset(&rc, 0, sizeof rc);
+    rc.N = N;
+    rc.n1 = N;
+    rc.mode = o->mode;
+    rc.gapmm = o->mode == TN93G_GAPMM;
+    rc.fallback_avg = (o->mode == TN93G_RESOLVE || o->mode == TN93G_SUBSET) && o->resolve_fraction < 1.;
+    rc.emit = !o->count_only;
+    rc.format = o->format;
+    rc.delim = o->delimiter;
+    rc.report_self = o->report_self && rc.emit;
+    rc.threshold = o->threshold;
+    rc.min_distance = o->min_distance;
+    rc.resolve_fraction = o->resolve_fraction;
+    rc.min_overlap = o->min_overlap;
+    for (long p = 0; p < L; p++) {
+      const uint32_t m = seen[seen_off[k] + p];
+      if (m && !(m & (m - 1)) && m < 16) {
+        const int b = __builtin_ctz(m);
+        rc.constT++;
+        rc.constNf[b] += 2;
+        rc.constCnt[b]++;
+      } else
+        varcol.push_back((int32_t)p);
+    }
+    vc_off[k + 1] = varcol.size();
+    rc.Lc = (long)(vc_off[k + 1] - vc_off[k]);
+    rc.W = (rc.Lc + 63) / 64;
+    rc.Npad = (N + 31) / 32 * 32;
+    rc.wplane = rc.gapmm || nN[k] > 16ull * (unsigned long long)N;
+    rc.NP = rc.gapmm ? 5 : 4;
+    pl_off[k + 1] = pl_off[k] + (size_t)std::max<long>(rc.W, 1) * rc.NP * rc.Npad;
+    cc_off[k + 1] = cc_off[k] + (size_t)N * std::max<long>(rc.Lc, 1);
+    cct_off[k + 1] = cct_off[k] + (size_t)std::max<long>(rc.Lc, 1) * rc.Npad;
+    evo_off[k + 1] = evo_off[k] + N + 1;
+  }
+  TRY(ensure(ctx, bb[BB_VARCOL], std::max<size_t>(varcol.size(), 1) * sizeof(int32_t)));
+  TRY(ensure(ctx, bb[BB_PLANES], pl_off[K] * sizeof(uint64_t)));
+  TRY(ensure(ctx, bb[BB_CC], cc_off[K]));
+  TRY(ensure(ctx, bb[BB_CCT], cct_off[K]));
+  TRY(ensure(ctx, bb[BB_EVCOUNT], NR * sizeof(uint32_t)));
+  TRY(ensure(ctx, bb[BB_EVOFF], evo_off[K] * sizeof(uint32_t)));
+  if (!varcol.empty())
+    CU(cudaMemcpyAsync(bb[BB_VARCOL].p, varcol.data(), varcol.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  CU(cudaMemsetAsync(bb[BB_PLANES].p, 0, pl_off[K] * sizeof(uint64_t), st));
+  CU(cudaMemsetAsync(bb[BB_EVCOUNT].p, 0, NR * sizeof(uint32_t), st));
+  std::vector<PackArgs> PA(K);
+  for (int k = 0; k < K; k++) {
+    const RunConsts &rc = RC[k];
+    PackArgs &pa = PA[k];
+    pa.codes = (const uint8_t *)bb[BB_CODES].p + code_off[k];
+    pa.N = rc.N;
+    pa.L = alns[k].L;
+    pa.Lc = rc.Lc;
+    pa.W = rc.W;
+    pa.Npad = rc.Npad;
+    pa.varcol = (const int32_t *)bb[BB_VARCOL].p + vc_off[k];
+    pa.NP = rc.NP;
+    pa.wplane = rc.wplane;
+    pa.gapmm = rc.gapmm;
+    pa.planes = (uint64_t *)bb[BB_PLANES].p + pl_off[k];
+    pa.cc = (uint8_t *)bb[BB_CC].p + cc_off[k];
+    pa.evcount = (uint32_t *)bb[BB_EVCOUNT].p + row_base[k];
+    pa.ev_off = (const uint32_t *)bb[BB_EVOFF].p + evo_off[k];
+    if (rc.W) {
+      pack_kernel<<<dim3((unsigned)((rc.N + kWarps - 1) / kWarps), (unsigned)std::min<long>(rc.W, 65535)), 256, 0,
+                    st>>>(pa);
+      CU(cudaGetLastError());
+      transpose_kernel<<<dim3((unsigned)((rc.Lc + 31) / 32), (unsigned)(rc.Npad / 32)), dim3(32, 8), 0, st>>>(
+          pa.cc, (uint8_t *)bb[BB_CCT].p + cct_off[k], rc.N, rc.Lc, rc.Npad);
+      CU(cudaGetLastError());
+      ctx->launches += 2;
+    }
+  }
+  std::vector<uint32_t> evc(NR), evo(evo_off[K]);
+  CU(cudaMemcpyAsync(evc.data(), bb[BB_EVCOUNT].p, NR * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  size_t nev = 0;
+  for (int k = 0; k < K; k++) {
+    for (long i = 0; i < alns[k].n; i++) {
+      evo[evo_off[k] + i] = (uint32_t)nev;
+      nev += evc[row_base[k] + i];
+    }
+    evo[evo_off[k] + alns[k].n] = (uint32_t)nev;
+  }
+  if (nev >= (1ull << 32)) return TN93G_ETOOBIG;
+  TRY(ensure(ctx, bb[BB_EV], std::max<size_t>(nev, 1) * sizeof(uint32_t)));
+  CU(cudaMemcpyAsync(bb[BB_EVOFF].p, evo.data(), evo_off[K] * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+  for (int k = 0; k < K; k++) {
+    PA[k].ev = (uint32_t *)bb[BB_EV].p;
+    if (RC[k].W && evo[evo_off[k] + alns[k].n] > evo[evo_off[k]]) {
+      events_kernel<<<(unsigned)((RC[k].N + kWarps - 1) / kWarps), 256, 0, st>>>(PA[k]);
+      CU(cudaGetLastError());
+      ctx->launches++;
+    }
+  }
+  // tables: one copy per distinct (mode, ambiguity subset)
+  const size_t agg_n = kSparseCodes * kCodes + 5;
+  std::vector<int> tab_of(K);
+  std::vector<std::pair<int, std::string>> keys;
+  std::vector<AggEntry> h_agg;
+  std::vector<SiteEntry> h_site;
+  for (int k = 0; k < K; k++) {
+    const std::string sub((const char *)opts[k].subset, sizeof opts[k].subset);
+    const std::pair<int, std::string> key(opts[k].mode, opts[k].mode == TN93G_SUBSET ? sub : std::string());
+    int t = -1;
+    for (size_t q = 0; q < keys.size(); q++)
+      if (keys[q] == key) t = (int)q;
+    if (t < 0) {
+      build_tables(ctx->h_tab, opts[k].mode, opts[k].subset);
+      h_agg.insert(h_agg.end(), ctx->h_tab->ev, ctx->h_tab->ev + agg_n);
+      const SiteEntry *se = &ctx->h_tab->site[0][0];
+      h_site.insert(h_site.end(), se, se + sizeof(ctx->h_tab->site) / sizeof(SiteEntry));
+      t = (int)keys.size();
+      keys.push_back(key);
+    }
+    tab_of[k] = t;
+  }
+  const size_t site_n = sizeof(ctx->h_tab->site) / sizeof(SiteEntry);
+  TRY(ensure(ctx, bb[BB_AGG], h_agg.size() * sizeof(AggEntry)));
+  TRY(ensure(ctx, bb[BB_SITE], h_site.size() * sizeof(SiteEntry)));
+  CU(cudaMemcpyAsync(bb[BB_AGG].p, h_agg.data(), h_agg.size() * sizeof(AggEntry), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(bb[BB_SITE].p, h_site.data(), h_site.size() * sizeof(SiteEntry), cudaMemcpyHostToDevice, st));
+  CU(cudaEventRecord(E[1], st));
+  //------------------------------------------------------------------ pair stage
+  std::vector<size_t> d_off(K + 1), q_off(K + 1), seg_base(K + 1);
+  d_off[0] = q_off[0] = seg_base[0] = 0;
+  std::vector<long> maxseg(K);
+  for (int k = 0; k < K; k++) {
+    const size_t N = alns[k].n;
+    d_off[k + 1] = d_off[k] + N * N;
+    q_off[k + 1] = q_off[k] + std::max<size_t>(N * (N - 1) / 2, 1);
+    maxseg[k] = std::max<long>(1, ((long)N + kSeg - 1) / kSeg);
+    seg_base[k + 1] = seg_base[k] + N * maxseg[k];
+  }
+  TRY(ensure(ctx, bb[BB_DIST], d_off[K] * sizeof(double)));
+  TRY(ensure(ctx, bb[BB_RQ], q_off[K] * sizeof(unsigned long long)));
+  TRY(ensure(ctx, bb[BB_RQN], K * sizeof(unsigned)));
+  TRY(ensure(ctx, bb[BB_COUNTERS], (size_t)K * 4 * sizeof(unsigned long long)));
+  CU(cudaMemsetAsync(bb[BB_RQN].p, 0, K * sizeof(unsigned), st));
+  CU(cudaMemsetAsync(bb[BB_COUNTERS].p, 0, (size_t)K * 4 * sizeof(unsigned long long), st));
+  std::vector<PairArgs> PD(K);
+  std::vector<ReplayArgs> RD(K);
+  for (int k = 0; k < K; k++) {
+    PairArgs &A = PD[k];
+    memset(&A, 0, sizeof A);
+    A.rc = RC[k];
+    A.planes = (const uint64_t *)bb[BB_PLANES].p + pl_off[k];
+    A.cc = (const uint8_t *)bb[BB_CC].p + cc_off[k];
+    A.ccT = (const uint8_t *)bb[BB_CCT].p + cct_off[k];
+    A.ev_off = (const uint32_t *)bb[BB_EVOFF].p + evo_off[k];
+    A.ev = (const uint32_t *)bb[BB_EV].p;
+    A.agg = (const AggEntry *)bb[BB_AGG].p + (size_t)tab_of[k] * agg_n;
+    A.r0 = 0;
+    A.r1 = alns[k].n;
+    A.ncols = alns[k].n;
+    A.colbase = 0;
+    A.cstart = 0;
+    A.dist = (double *)bb[BB_DIST].p + d_off[k];
+    A.replay_q = (unsigned long long *)bb[BB_RQ].p + q_off[k];
+    A.replay_n = (unsigned *)bb[BB_RQN].p + k;
+    A.replay_cap = q_off[k + 1] - q_off[k];
+    A.counters = (unsigned long long *)bb[BB_COUNTERS].p + 4 * k;
+    A.logt = ctx->d_logt;
+    ReplayArgs &R = RD[k];
+    memset(&R, 0, sizeof R);
+    R.rc = RC[k];
+    R.cc = A.cc;
+    R.planes = A.planes;
+    R.site = (const SiteEntry *)bb[BB_SITE].p + (size_t)tab_of[k] * site_n;
+    R.q = A.replay_q;
+    R.qn = A.replay_n;
+    R.qcap = A.replay_cap;
+    R.r0 = 0;
+    R.ncols = A.ncols;
+    R.colbase = 0;
+    R.dist = A.dist;
+    R.counters = A.counters;
+    R.logt = ctx->d_logt;
+  }
+  // the tile queue: per kernel class, longest alignments first
+  std::vector<BatchTile> tiles;
+  int cls_n[3] = {0, 0, 0};
+  std::vector<int> order(K);
+  for (int k = 0; k < K; k++) order[k] = k;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return RC[a].Lc > RC[b].Lc; });
+  for (int cls = 0; cls < 3; cls++)
+    for (int k : order) {
+      const int kc = RC[k].gapmm ? 2 : RC[k].wplane ? 1 : 0;
+      if (kc != cls || !RC[k].W) continue;
+      const int rpw = rows_per_warp ? rows_per_warp[k] : kRowsPerWarp, trows = kWarps * rpw;
+      const long N = alns[k].n;
+      for (long i0 = 0; i0 < N - 1; i0 += trows)
+        for (long j0 = (i0 + 1) / kTile * kTile; j0 < N; j0 += kTile) {
+          tiles.push_back(BatchTile{k, rpw, (int)i0, (int)j0});
+          cls_n[cls]++;
+        }
+    }
+  // alignments whose columns are all constant (Lc = 0) have no tiles: the epilogue runs on the constants alone
+  // in tn93g_run; here they take the single-alignment kernel
+  TRY(ensure(ctx, bb[BB_PDESC], K * sizeof(PairArgs)));
+  TRY(ensure(ctx, bb[BB_RDESC], K * sizeof(ReplayArgs)));
+  TRY(ensure(ctx, bb[BB_TILES], std::max<size_t>(tiles.size(), 1) * sizeof(BatchTile)));
+  TRY(ensure(ctx, bb[BB_NEXT], 3 * sizeof(unsigned)));
+  CU(cudaMemcpyAsync(bb[BB_PDESC].p, PD.data(), K * sizeof(PairArgs), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(bb[BB_RDESC].p, RD.data(), K * sizeof(ReplayArgs), cudaMemcpyHostToDevice, st));
+  if (!tiles.empty())
+    CU(cudaMemcpyAsync(bb[BB_TILES].p, tiles.data(), tiles.size() * sizeof(BatchTile), cudaMemcpyHostToDevice, st));
+  CU(cudaMemsetAsync(bb[BB_NEXT].p, 0, 3 * sizeof(unsigned), st));
+  int tbase = 0;
+  for (int cls = 0; cls < 3; cls++) {
+    if (!cls_n[cls]) continue;
+    const BatchTile *tp = (const BatchTile *)bb[BB_TILES].p + tbase;
+    unsigned *nx = (unsigned *)bb[BB_NEXT].p + cls;
+    const PairArgs *dp = (const PairArgs *)bb[BB_PDESC].p;
+    CU(pair_blocks == 3 ? launch_pair_batch_t<3>(cls >= 1, cls == 2, dp, tp, cls_n[cls], nx, st)
+                        : launch_pair_batch_t<2>(cls >= 1, cls == 2, dp, tp, cls_n[cls], nx, st));
+    ctx->launches++;
+    tbase += cls_n[cls];
+  }
+  for (int k = 0; k < K; k++)
+    if (!RC[k].W && alns[k].n > 1) {
+      CU(launch_pair(PD[k], (alns[k].n + kTile - 1) / kTile, alns[k].n, st));
+      ctx->launches++;
+    }
+  CU(cudaEventRecord(E[2], st));
+  replay_batch_kernel<<<2 * 148, 256, 0, st>>>((const ReplayArgs *)bb[BB_RDESC].p, K);
+  CU(cudaGetLastError());
+  ctx->launches++;
+  CU(cudaEventRecord(E[3], st));
+  //------------------------------------------------------------------ rows
+  const size_t NS = seg_base[K];
+  TRY(ensure(ctx, bb[BB_SBYTES], NS * sizeof(unsigned long long)));
+  TRY(ensure(ctx, bb[BB_SOFF], NS * sizeof(unsigned long long)));
+  TRY(ensure(ctx, bb[BB_SLINKS], NS * sizeof(long long)));
+  TRY(ensure(ctx, bb[BB_SSKIP], NS * sizeof(long long)));
+  TRY(ensure(ctx, bb[BB_SMAX], NS * 3 * sizeof(double)));
+  TRY(ensure(ctx, bb[BB_RSUM], NR * 3 * sizeof(double)));
+  TRY(ensure(ctx, bb[BB_RW], NR * 3 * sizeof(double)));
+  TRY(ensure(ctx, bb[BB_HIST], (size_t)K * 3 * kHistBins * sizeof(unsigned long long)));
+  TRY(ensure(ctx, bb[BB_TOTAL], sizeof(unsigned long long)));
+  TRY(ensure(ctx, bb[BB_SCANTMP], (2 * (NS / kScanTile + 1) + 1) * sizeof(unsigned long long)));
+  TRY(ensure(ctx, bb[BB_RED], (size_t)K * 3 * sizeof(double)));
+  TRY(ensure(ctx, bb[BB_REDC], (size_t)K * 2 * sizeof(long long)));
+  TRY(ensure(ctx, bb[BB_FIRST], (size_t)K * sizeof(unsigned long long)));
+  TRY(ensure(ctx, bb[BB_FIRSTIDX], (size_t)K * sizeof(long)));
+  TRY(ensure(ctx, bb[BB_ROWDESC], K * sizeof(RowArgs)));
+  CU(cudaMemsetAsync(bb[BB_HIST].p, 0, (size_t)K * 3 * kHistBins * sizeof(unsigned long long), st));
+  std::vector<RowArgs> RA(K);
+  std::vector<int2> blocks;
+  long segmax = 1;
+  std::vector<long> first_idx(K);
+  for (int k = 0; k < K; k++) {
+    RowArgs &a = RA[k];
+    memset(&a, 0, sizeof a);
+    a.rc = RC[k];
+    a.dist = PD[k].dist;
+    a.r0 = 0;
+    a.r1 = alns[k].n;
+    a.ncols = alns[k].n;
+    a.colbase = 0;
+    a.counts = (const long *)bb[BB_COUNTS].p + row_base[k];
+    a.name_len = (const int32_t *)bb[BB_NAMELEN].p + row_base[k];
+    a.name_off = (const uint64_t *)bb[BB_NAMEOFF].p + row_base[k];
+    a.names = (const char *)bb[BB_NAMES].p;
+    a.maxseg = maxseg[k];
+    a.seg_cols = nullptr;
+    a.nrows = alns[k].n;
+    a.seg_bytes = (unsigned long long *)bb[BB_SBYTES].p + seg_base[k];
+    a.seg_links = (long long *)bb[BB_SLINKS].p + seg_base[k];
+    a.seg_skip = (long long *)bb[BB_SSKIP].p + seg_base[k];
+    a.seg_max = (double *)bb[BB_SMAX].p + 3 * seg_base[k];
+    a.row_sum = (double *)bb[BB_RSUM].p + 3 * row_base[k];
+    a.row_w = (double *)bb[BB_RW].p + 3 * row_base[k];
+    a.hist = (unsigned long long *)bb[BB_HIST].p + (size_t)k * 3 * kHistBins;
+    a.seg_off = (const unsigned long long *)bb[BB_SOFF].p + seg_base[k];
+    a.out = nullptr;
+    a.hy = nullptr;
+    a.err = (unsigned long long *)bb[BB_COUNTERS].p + 4 * k + 3;
+    segmax = std::max(segmax, maxseg[k]);
+    for (long bx = 0; bx < (alns[k].n + kWarps - 1) / kWarps; bx++) blocks.push_back(make_int2(k, (int)bx));
+    first_idx[k] = (long)seg_base[k];
+  }
+  TRY(ensure(ctx, bb[BB_BLOCKS], blocks.size() * sizeof(int2)));
+  CU(cudaMemcpyAsync(bb[BB_ROWDESC].p, RA.data(), K * sizeof(RowArgs), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(bb[BB_BLOCKS].p, blocks.data(), blocks.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(bb[BB_FIRSTIDX].p, first_idx.data(), K * sizeof(long), cudaMemcpyHostToDevice, st));
+  const RowArgs *rd = (const RowArgs *)bb[BB_ROWDESC].p;
+  const int2 *bp = (const int2 *)bb[BB_BLOCKS].p;
+  stats_batch_kernel<<<dim3((unsigned)blocks.size(), (unsigned)segmax), 256, 0, st>>>(rd, bp);
+  CU(cudaGetLastError());
+  sum_batch_kernel<<<(unsigned)blocks.size(), 256, 0, st>>>(rd, bp);
+  CU(cudaGetLastError());
+  CU(launch_scan((const unsigned long long *)bb[BB_SBYTES].p, (unsigned long long *)bb[BB_SOFF].p, (long)NS,
+                 (unsigned long long *)bb[BB_TOTAL].p, (unsigned long long *)bb[BB_SCANTMP].p, st));
+  aln_reduce_kernel<<<K, 256, 0, st>>>(rd, (double *)bb[BB_RED].p, (long long *)bb[BB_REDC].p);
+  CU(cudaGetLastError());
+  gather_u64_kernel<<<(K + 255) / 256, 256, 0, st>>>((const unsigned long long *)bb[BB_SOFF].p,
+                                                     (const long *)bb[BB_FIRSTIDX].p,
+                                                     (unsigned long long *)bb[BB_FIRST].p, K);
+  CU(cudaGetLastError());
+  ctx->launches += 5;
+  CU(cudaEventRecord(E[4], st));
+  unsigned long long total = 0;
+  std::vector<double> red((size_t)K * 3);
+  std::vector<long long> redc((size_t)K * 2);
+  std::vector<unsigned long long> first(K + 1), hist((size_t)K * 3 * kHistBins), counters((size_t)K * 4);
+  CU(cudaMemcpyAsync(&total, bb[BB_TOTAL].p, sizeof total, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(red.data(), bb[BB_RED].p, red.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(redc.data(), bb[BB_REDC].p, redc.size() * sizeof(long long), cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(first.data(), bb[BB_FIRST].p, K * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(hist.data(), bb[BB_HIST].p, hist.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                     st));
+  CU(cudaStreamSynchronize(st));
+  first[K] = total;
+  bool any_emit = false;
+  for (int k = 0; k < K; k++) any_emit |= RC[k].emit;
+  if (any_emit && total) {
+    if (bb[BB_OUT].n < total) TRY(ensure(ctx, bb[BB_OUT], total + total / 4));
+    TRY(ensure_pinned(ctx, total));
+    for (int k = 0; k < K; k++) RA[k].out = (char *)bb[BB_OUT].p;
+    CU(cudaMemcpyAsync(bb[BB_ROWDESC].p, RA.data(), K * sizeof(RowArgs), cudaMemcpyHostToDevice, st));
+    write_batch_kernel<<<dim3((unsigned)blocks.size(), (unsigned)segmax), 256, 0, st>>>(rd, bp);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    CU(cudaEventRecord(E[5], st));
+    CU(cudaMemcpyAsync(ctx->pinned, bb[BB_OUT].p, total, cudaMemcpyDeviceToHost, st));
+  } else {
+    CU(cudaEventRecord(E[5], st));
+  }
+  CU(cudaMemcpyAsync(counters.data(), bb[BB_COUNTERS].p, counters.size() * sizeof(unsigned long long),
+                     cudaMemcpyDeviceToHost, st));
+  CU(cudaEventRecord(E[6], st));
+  CU(cudaStreamSynchronize(st));
+  const int pairs_e[7][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 4}, {4, 5}, {5, 6}, {0, 6}};
+  for (int q = 0; q < 7; q++) {
+    CU(cudaEventElapsedTime(&ms, E[pairs_e[q][0]], E[pairs_e[q][1]]));
+    ctx->timings[q] = ms;
+  }
+  for (int k = 0; k < K; k++) {
+    if (counters[4 * k + 3]) {
+      ctx->err = "internal error: a row's text did not match its counted length";
+      return TN93G_ECUDA;
+    }
+    tn93g_summary &S = sums[k];
+    memset(&S, 0, sizeof S);
+    const unsigned long N = (unsigned long)alns[k].n;
+    S.pairwise = N * (N - 1) / 2;
+    S.links = (long)redc[2 * k];
+    S.skipped = (long)redc[2 * k + 1];
+    S.max[0] = red[3 * k];
+    S.mean[0] = red[3 * k + 1];
+    S.weighted[0] = red[3 * k + 2];
+    for (int q = 0; q < 3; q++)
+      for (int b = 0; b < kHistBins; b++) S.hist[q][b] = hist[((size_t)k * 3 + q) * kHistBins + b];
+    S.logs_ambiguous = (long)counters[4 * k];
+    S.undecided = (long)counters[4 * k + 1];
+    S.pairs_replayed = (long)counters[4 * k + 2];
+    S.output_bytes = RC[k].emit ? first[k + 1] - first[k] : 0;
+  }
+  if (any_emit && sink)
+    for (int k = 0; k < K; k++)
+      if (RC[k].emit && sink(user, k, (const char *)ctx->pinned + first[k], (size_t)(first[k + 1] - first[k])))
+        return TN93G_ESINK;
+  return TN93G_OK;
+}
