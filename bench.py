@@ -17,7 +17,8 @@ e2e    : pairs/s through the C ABI from host buffers: every step uploads the cod
 Multi-GPU (torchrun): every rank runs its own replica of the workload (pairs are independent; no collective on
 the data path), value = pairs of all ranks / max over ranks of the device time.
 variant_hivtrace_t0.015: the same alignment at -t 0.015 (few pairs written). variant_served_s: the -s serving
-loop (serving_variant). Neither is the headline value.
+loop (serving_variant). variant_batched: 96 independent alignments in one batched call (batched_variant). None
+of them is the headline value.
 """
 from __future__ import annotations
 
@@ -211,6 +212,116 @@ def serving_variant(rates=(20.0, 200.0), seconds=4.0, saturate=1200, ref_sample=
     return out
 
 
+def _gen_batch_alignment(i):
+    from swifttn93_b200 import synth
+
+    return synth.batch_alignment(i)
+
+
+def batched_variant(eng, steps, warmup, n_aln=96, ref_sample=6):
+    """The batched form: 96 independent alignments (synth.batch_spec: sizes log-uniform 50-4,000, lengths
+    900-3,000, each with its own -t in 0.005-0.02 and -a mode; -g 0.05 -l 500 -f csv), all run by one
+    tn93g_batch_run call per step (inputs in pinned host memory, texts back on the host), against the plain path:
+    the same alignments one tn93g_upload + tn93g_run after another. Pair tiles are picked by the autotuner
+    (untimed). Every batched output is checked against the plain path's bytes."""
+    import concurrent.futures as cf
+    import hashlib
+    import multiprocessing as mp
+
+    import torch
+
+    from swifttn93_b200 import HostAlignment, Options, autotune
+
+    with cf.ProcessPoolExecutor(max_workers=min(16, os.cpu_count() or 1),
+                                mp_context=mp.get_context("spawn")) as ex:
+        gen = list(ex.map(_gen_batch_alignment, range(n_aln)))
+    specs = [g[0] for g in gen]
+    pinned = []
+    alns, opts = [], []
+    for sp, names, codes in gen:
+        t = torch.empty(codes.shape, dtype=torch.uint8).pin_memory()
+        t.numpy()[:] = codes
+        pinned.append(t)
+        alns.append(HostAlignment(t.numpy(), names))
+        opts.append(Options(threshold=sp["threshold"], mode=sp["mode"], resolve_fraction=0.05, min_overlap=500))
+    pairs = sum(a.n * (a.n - 1) // 2 for a in alns)
+    tuning = autotune.load_or_tune(eng, torch.cuda.get_device_name())
+    rpw = [autotune.rows_per_warp(tuning, a.L) for a in alns]
+    blocks = tuning["pair_blocks"]
+    out = eng.batch_run(alns, opts, rows_per_warp=rpw, pair_blocks=blocks)  # bytes for the parity check
+    text_bytes = sum(len(b) for b, _ in out)
+    bt, dev, stage = [], [], {}
+    for it in range(warmup + steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.batch_run(alns, opts, rows_per_warp=rpw, pair_blocks=blocks, sink="discard")
+        t1 = time.perf_counter()
+        if it >= warmup:
+            bt.append(t1 - t0)
+            tm = eng.last_timings()
+            dev.append(tm["total"])
+            for k, v in tm.items():
+                stage[k] = stage.get(k, 0.0) + v / steps
+            launches = eng.last_launches()
+    digest_b = hashlib.sha256(b"".join(hashlib.sha256(b).digest() for b, _ in out)).hexdigest()
+    # the plain path, alignment after alignment (the same host buffers; texts to the engine's pinned buffer)
+    names = [[bytes(a._names.raw[int(x):int(x) + int(n)]) for x, n in zip(a._off, a._len)] for a in alns]
+    plain = []
+    for a, o, nm in zip(alns, opts, names):
+        s = eng.upload(a._codes, nm)
+        plain.append(eng.run(s, o)[0])
+        eng.free(s)
+    digest_p = hashlib.sha256(b"".join(hashlib.sha256(b).digest() for b in plain)).hexdigest()
+    pt = []
+    for it in range(warmup + steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for a, o, nm in zip(alns, opts, names):
+            s = eng.upload(a._codes, nm)
+            eng.run(s, o, sink="discard")
+            eng.free(s)
+        if it >= warmup:
+            pt.append(time.perf_counter() - t0)
+    res = {"workload": f"{n_aln} alignments (batch_spec): n log-uniform 50-4000, L 900-3000, per-alignment -t "
+                       "0.005-0.02 and -a resolve/average/gapmm, -g 0.05 -l 500 -f csv",
+           "pairs_per_step": pairs, "unit": "pairs/s",
+           "value": pairs / float(np.mean(bt)), "device_value": pairs / (float(np.mean(dev)) / 1e3),
+           "plain_path_value": pairs / float(np.mean(pt)),
+           "note": "value = pairs / wall time of one tn93g_batch_run (inputs from pinned host memory, every text "
+                   "copied to the engine's pinned host buffer); device_value = pairs / device time of the call; "
+                   "plain_path_value = the same alignments one tn93g_upload + tn93g_run after another",
+           "outputs_identical_to_plain_path": digest_b == digest_p, "text_bytes_per_step": text_bytes,
+           "h2d_bytes_per_step": int(sum(a._codes.nbytes for a in alns)), "gpu_launches": launches,
+           "stage_ms": stage, "tuning": {k: tuning[k] for k in ("pair_blocks", "rows_per_warp", "bands")}}
+    binary = reference_binary()
+    if binary is not None and ref_sample:
+        from swifttn93_b200 import synth
+
+        tmpdir = Path("/dev/shm") if Path("/dev/shm").is_dir() else Path(tempfile.gettempdir())
+        td = Path(tempfile.mkdtemp(dir=tmpdir))
+        try:
+            env = {**os.environ, "OMP_NUM_THREADS": str(os.cpu_count())}
+            wall, rp = 0.0, 0
+            for k in range(0, n_aln, max(1, n_aln // ref_sample))[:ref_sample]:
+                sp, names, codes = gen[k]
+                (td / "a.fa").write_bytes(synth.to_fasta(names, codes))
+                t0 = time.perf_counter()
+                r = subprocess.run([str(binary), "-q", "-t", repr(sp["threshold"]), "-a", sp["mode"], "-g", "0.05",
+                                    "-l", "500", "-f", "csv", "-o", str(td / "o.csv"), str(td / "a.fa")],
+                                   stdout=subprocess.DEVNULL, env=env)
+                wall += time.perf_counter() - t0
+                if r.returncode != 0:
+                    wall = 0.0
+                    break
+                rp += sp["n"] * (sp["n"] - 1) // 2
+            if wall:
+                res["reference"] = {"binary": binary.name, "cores": os.cpu_count(), "pairs_per_s": rp / wall,
+                                    "sample": f"{ref_sample} of the {n_aln} alignments, one process each"}
+        finally:
+            shutil.rmtree(td, ignore_errors=True)
+    return res
+
+
 def dist_init():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws > 1:
@@ -231,6 +342,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--n", type=int, default=0, help="use the first N sequences only (profiling runs)")
     ap.add_argument("--no-serving", action="store_true", help="skip the served (-s) variant")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched variant")
     args = ap.parse_args()
     ws, rank, local = dist_init()
     names, codes = workload()
@@ -453,6 +565,8 @@ def main():
             if v15 is not None:
                 line["variant_hivtrace_t0.015"]["reference"] = v15
     eng.free(s)
+    if rank == 0 and ws == 1 and not args.no_batched and not args.n:
+        line["variant_batched"] = batched_variant(eng, args.steps, args.warmup)
     eng.close()
     if rank == 0 and ws == 1 and not args.no_serving and not args.n:
         line["variant_served_s"] = serving_variant()

@@ -334,9 +334,11 @@ class Engine:
                                                  C.byref(ptr), C.byref(nb), C.byref(S)))
         return ptr.value, nb.value, self._summary(S)
 
-    def batch_run(self, alignments: list, opts: list, rows_per_warp=None, pair_blocks: int = 0) -> list:
+    def batch_run(self, alignments: list, opts: list, rows_per_warp=None, pair_blocks: int = 0,
+                  sink=None) -> list:
         """tn93g_batch_run: many alignments (HostAlignment or Fasta objects), each with its own Options, in one pass.
-        Returns [(body bytes, Summary)], each equal to run() on that alignment alone."""
+        Returns [(body bytes, Summary)], each equal to run() on that alignment alone. sink="discard" leaves the
+        texts in the engine's pinned host buffer (bodies are returned empty)."""
         K = len(alignments)
         arr = (_Alignment * K)(*[a._a for a in alignments])
         oc = (_Opts * K)(*[o.to_c() for o in opts])
@@ -351,7 +353,7 @@ class Engine:
             except Exception:  # noqa: BLE001 - an exception must not unwind through C
                 return 1
 
-        cb = _QSINK(_sink)
+        cb = _QSINK() if (isinstance(sink, str) and sink == "discard") else _QSINK(_sink)
         self._check(self.lib.tn93g_batch_run(self.ctx, K, arr, oc, rpw, int(pair_blocks), cb, None, sums))
         out = []
         for k in range(K):
@@ -378,8 +380,7 @@ class Engine:
         t = (C.c_double * 7)()
         k = self.lib.tn93g_last_timings(self.ctx, t, 7)
         summ = Summary(pairwise=S.pairwise, skipped=S.skipped, links=S.links, max=list(S.max), mean=list(S.mean),
-                       weighted=list(S.weighted), hist=np.array([[S.hist[q][k2] for k2 in range(200)]
-                                                                 for q in range(3)], dtype=np.uint64),
+                       weighted=list(S.weighted), hist=_hist(S),
                        pairs_replayed=S.pairs_replayed, logs_ambiguous=S.logs_ambiguous, undecided=S.undecided,
                        output_bytes=S.output_bytes,
                        timings_ms={self.STAGES[q]: t[q] for q in range(k)}, raw=S)
@@ -397,10 +398,13 @@ class Engine:
             pass
 
 
+def _hist(S) -> np.ndarray:
+    return np.frombuffer(bytes(S.hist), dtype=np.uint64).reshape(3, 200).copy()
+
+
 def _plain_summary(S) -> Summary:
     return Summary(pairwise=S.pairwise, skipped=S.skipped, links=S.links, max=list(S.max), mean=list(S.mean),
-                   weighted=list(S.weighted), hist=np.array([[S.hist[q][k] for k in range(200)] for q in range(3)],
-                                                            dtype=np.uint64),
+                   weighted=list(S.weighted), hist=_hist(S),
                    pairs_replayed=S.pairs_replayed, logs_ambiguous=S.logs_ambiguous, undecided=S.undecided,
                    output_bytes=S.output_bytes, raw=S)
 
