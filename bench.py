@@ -218,7 +218,7 @@ def _gen_batch_alignment(i):
     return synth.batch_alignment(i)
 
 
-def batched_variant(eng, steps, warmup, n_aln=96, ref_sample=6):
+def batched_variant(eng, steps, warmup, n_aln=96, ref_sample=6, plain=True):
     """The batched form: 96 independent alignments (synth.batch_spec: sizes log-uniform 50-4,000, lengths
     900-3,000, each with its own -t in 0.005-0.02 and -a mode; -g 0.05 -l 500 -f csv), all run by one
     tn93g_batch_run call per step (inputs in pinned host memory, texts back on the host), against the plain path:
@@ -253,9 +253,11 @@ def batched_variant(eng, steps, warmup, n_aln=96, ref_sample=6):
     bt, dev, stage = [], [], {}
     for it in range(warmup + steps):
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("batch_step")  # profiling filter (ncu --nvtx-include batch_step/)
         t0 = time.perf_counter()
         eng.batch_run(alns, opts, rows_per_warp=rpw, pair_blocks=blocks, sink="discard")
         t1 = time.perf_counter()
+        torch.cuda.nvtx.range_pop()
         if it >= warmup:
             bt.append(t1 - t0)
             tm = eng.last_timings()
@@ -266,14 +268,14 @@ def batched_variant(eng, steps, warmup, n_aln=96, ref_sample=6):
     digest_b = hashlib.sha256(b"".join(hashlib.sha256(b).digest() for b, _ in out)).hexdigest()
     # the plain path, alignment after alignment (the same host buffers; texts to the engine's pinned buffer)
     names = [[bytes(a._names.raw[int(x):int(x) + int(n)]) for x, n in zip(a._off, a._len)] for a in alns]
-    plain = []
-    for a, o, nm in zip(alns, opts, names):
+    plain_out = []
+    for a, o, nm in (zip(alns, opts, names) if plain else ()):
         s = eng.upload(a._codes, nm)
-        plain.append(eng.run(s, o)[0])
+        plain_out.append(eng.run(s, o)[0])
         eng.free(s)
-    digest_p = hashlib.sha256(b"".join(hashlib.sha256(b).digest() for b in plain)).hexdigest()
+    digest_p = hashlib.sha256(b"".join(hashlib.sha256(b).digest() for b in plain_out)).hexdigest()
     pt = []
-    for it in range(warmup + steps):
+    for it in range(warmup + steps if plain else 0):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for a, o, nm in zip(alns, opts, names):
@@ -286,11 +288,12 @@ def batched_variant(eng, steps, warmup, n_aln=96, ref_sample=6):
                        "0.005-0.02 and -a resolve/average/gapmm, -g 0.05 -l 500 -f csv",
            "pairs_per_step": pairs, "unit": "pairs/s",
            "value": pairs / float(np.mean(bt)), "device_value": pairs / (float(np.mean(dev)) / 1e3),
-           "plain_path_value": pairs / float(np.mean(pt)),
+           "plain_path_value": pairs / float(np.mean(pt)) if pt else None,
            "note": "value = pairs / wall time of one tn93g_batch_run (inputs from pinned host memory, every text "
                    "copied to the engine's pinned host buffer); device_value = pairs / device time of the call; "
                    "plain_path_value = the same alignments one tn93g_upload + tn93g_run after another",
-           "outputs_identical_to_plain_path": digest_b == digest_p, "text_bytes_per_step": text_bytes,
+           "outputs_identical_to_plain_path": (digest_b == digest_p) if plain else None,
+           "text_bytes_per_step": text_bytes,
            "h2d_bytes_per_step": int(sum(a._codes.nbytes for a in alns)), "gpu_launches": launches,
            "stage_ms": stage, "tuning": {k: tuning[k] for k in ("pair_blocks", "rows_per_warp", "bands")}}
     binary = reference_binary()
@@ -343,6 +346,7 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="use the first N sequences only (profiling runs)")
     ap.add_argument("--no-serving", action="store_true", help="skip the served (-s) variant")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched variant")
+    ap.add_argument("--only", choices=["batched", "served"], help="run one variant alone (profiling runs)")
     args = ap.parse_args()
     ws, rank, local = dist_init()
     names, codes = workload()
@@ -377,6 +381,13 @@ def main():
 
     torch.cuda.set_device(local)
     eng = Engine(device=local)
+    if args.only:
+        if rank == 0:
+            v = (batched_variant(eng, args.steps, args.warmup, ref_sample=0, plain=False) if args.only == "batched"
+                 else serving_variant(ref_sample=0))
+            print(json.dumps({"variant": args.only, **v}))
+        eng.close()
+        return
     stream = torch.cuda.ExternalStream(eng.stream, device=local)
     flush = torch.empty(64 << 20, dtype=torch.float32, device=f"cuda:{local}")
     opts = [Options(mode=m, **FLAGS) for m in MODES]
