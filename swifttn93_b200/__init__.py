@@ -30,7 +30,7 @@ EXPORTS = ("tn93g_create", "tn93g_destroy", "tn93g_strerror", "tn93g_last_cuda_e
            "tn93g_free_set", "tn93g_run", "tn93g_run_to_device", "tn93g_stream", "tn93g_last_launches",
            "tn93g_last_timings", "tn93g_pair_distances_noalloc", "tn93g_noalloc_last_error", "tn93g_read_fasta",
            "tn93g_alignment_free", "tn93g_server_create", "tn93g_server_batch", "tn93g_server_destroy",
-           "tn93g_summary_json", "tn93g_run_rows", "tn93g_batch_run")
+           "tn93g_summary_json", "tn93g_run_rows", "tn93g_batch_run", "tn93g_set_count_path")
 
 
 class _Opts(C.Structure):
@@ -97,6 +97,7 @@ def load_library(path: Path | str = LIB_PATH):
     lib.tn93g_server_destroy.argtypes = [C.c_void_p]
     lib.tn93g_run_rows.argtypes = [C.c_void_p, C.c_void_p, C.c_long, C.POINTER(_Opts), C.c_long, C.c_long, _SINK,
                                    C.c_void_p, C.c_void_p, C.POINTER(_Summary)]
+    lib.tn93g_set_count_path.argtypes = [C.c_void_p, C.c_int]
     lib.tn93g_batch_run.argtypes = [C.c_void_p, C.c_int, C.POINTER(_Alignment), C.POINTER(_Opts),
                                     C.POINTER(C.c_int), C.c_int, _QSINK, C.c_void_p, C.POINTER(_Summary)]
     lib.tn93g_summary_json.restype = C.c_size_t
@@ -361,6 +362,10 @@ class Engine:
             C.memmove(C.byref(S), C.byref(sums[k]), C.sizeof(_Summary))
             out.append((b"".join(bodies[k]), _plain_summary(S)))
         return out
+
+    def set_count_path(self, path: str):
+        """"popc" (CUDA-core bit-plane counts) or "tc" (tcgen05 INT8 tensor-core counts); results are identical."""
+        self._check(self.lib.tn93g_set_count_path(self.ctx, {"popc": 0, "tc": 1}[path]))
 
     def last_timings(self) -> dict:
         """Device milliseconds of the last call's stages (pack, pair, replay, rows, write, d2h, total)."""

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "tc_count.cuh"
 #include "tn93g.h"
 
 namespace tn93 {
@@ -225,15 +226,15 @@ struct Counts {
 
 // the per-pair epilogue: exact x16 aggregates, tn93's -l / -g / order decisions, formula, certificate
 template <bool WPLANE>
-__device__ __forceinline__ void pair_epilogue(const PairArgs &a, const AggEntry *sagg, const Counts &c, const int acc[9],
-                                              long i, long j, int &namb, int &nund)
+// cl: the clean-site aggregates of the pair (jointly clean sites, matches, A<->G and C<->T transitions, A, C and G
+// base counts over both sequences), from the popcount loop or the tensor-core count kernel; c: N-plane counts
+__device__ __forceinline__ void pair_epilogue(const PairArgs &a, const AggEntry *sagg, const Counts &c, const int cl[7],
+                                              const int acc[9], long i, long j, int &namb, int &nund)
 {
   const RunConsts &rc = a.rc;
-  const int D = c.T - c.MM, nfT = c.T1 + c.T2, nfC = c.Y1 + c.Y2 - nfT, nfG = c.L1 + c.L2 - nfT;
-  const int nfA = 2 * c.T - nfC - nfG - nfT;
-  const int base[7] = {16 * (c.T + (int)rc.constT), 16 * (D + (int)rc.constT), 16 * (c.TS - c.CT), 16 * c.CT,
-                       16 * (nfA + (int)rc.constNf[0]), 16 * (nfC + (int)rc.constNf[1]),
-                       16 * (nfG + (int)rc.constNf[2])};
+  const int base[7] = {16 * (cl[0] + (int)rc.constT), 16 * (cl[1] + (int)rc.constT), 16 * cl[2], 16 * cl[3],
+                       16 * (cl[4] + (int)rc.constNf[0]), 16 * (cl[5] + (int)rc.constNf[1]),
+                       16 * (cl[6] + (int)rc.constNf[2])};
   int wb[4] = {0, 0, 0, 0}, nww = 0;
   if (WPLANE) {
     wb[3] = c.nWt;
@@ -327,22 +328,25 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const AggEntry *sag
     const bool valid = j >= lb && j < rc.N;
     if (!__any_sync(0xffffffffu, valid)) continue;
     Counts c = Counts{0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const bool tc = a.tcagg != nullptr;  // clean-site counts from the tensor-core kernel
     const uint64_t *P = a.planes;
-    for (long w = 0; w < rc.W; w++, P += (size_t)rc.NP * Np) {
+    for (long w = 0; w < ((tc && !WPLANE) ? 0 : rc.W); w++, P += (size_t)rc.NP * Np) {
       const uint64_t hj = __ldg(P + jj), lj = __ldg(P + Np + jj), cj = __ldg(P + 2 * Np + jj);
       const uint64_t hi = __ldg(P + i), lo = __ldg(P + Np + i), ci = __ldg(P + 2 * Np + i);
-      const uint64_t b = ci & cj, x = hi ^ hj, y = lo ^ lj;
-      const uint64_t ts = b & ~x & y;
-      c.T += popc(b);
-      c.MM += popc(b & (x | y));
-      c.TS += popc(ts);
-      c.CT += popc(ts & hi);
-      c.Y1 += popc(b & hi);
-      c.Y2 += popc(b & hj);
-      c.L1 += popc(b & lo);
-      c.L2 += popc(b & lj);
-      c.T1 += popc(b & hi & lo);
-      c.T2 += popc(b & hj & lj);
+      if (!tc) {
+        const uint64_t b = ci & cj, x = hi ^ hj, y = lo ^ lj;
+        const uint64_t ts = b & ~x & y;
+        c.T += popc(b);
+        c.MM += popc(b & (x | y));
+        c.TS += popc(ts);
+        c.CT += popc(ts & hi);
+        c.Y1 += popc(b & hi);
+        c.Y2 += popc(b & hj);
+        c.L1 += popc(b & lo);
+        c.L2 += popc(b & lj);
+        c.T1 += popc(b & hi & lo);
+        c.T2 += popc(b & hj & lj);
+      }
       if (WPLANE) {
         const uint64_t ni = __ldg(P + 3 * Np + i), nj = __ldg(P + 3 * Np + jj);
         c.nWc += popc(ni & cj) + popc(nj & ci);
@@ -363,7 +367,22 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const AggEntry *sag
       const int pc = a.ccT[(size_t)(v >> 5) * Np + jj];
       add_entry(acc, sagg[((v & 31) - 4) * kCodes + pc].v);
     }
-    if (valid) pair_epilogue<WPLANE>(a, sagg, c, acc, i, j, namb, nund);
+    int cl[7];
+    if (tc) {
+      const int32_t *g = a.tcagg + (size_t)(i - a.r0) * a.ncols + (jj - a.colbase);
+#pragma unroll
+      for (int q = 0; q < 7; q++) cl[q] = valid ? g[q * a.tcplane] : 0;
+    } else {
+      const int nfT = c.T1 + c.T2, nfC = c.Y1 + c.Y2 - nfT, nfG = c.L1 + c.L2 - nfT;
+      cl[0] = c.T;
+      cl[1] = c.T - c.MM;
+      cl[2] = c.TS - c.CT;
+      cl[3] = c.CT;
+      cl[4] = 2 * c.T - nfC - nfG - nfT;
+      cl[5] = nfC;
+      cl[6] = nfG;
+    }
+    if (valid) pair_epilogue<WPLANE>(a, sagg, c, cl, acc, i, j, namb, nund);
   }
   count_flags(a.counters, namb, nund);
 }
@@ -400,7 +419,8 @@ __global__ void __launch_bounds__(256, MINB)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   AggEntry *sagg = reinterpret_cast<AggEntry *>(smem_raw);
   int *colacc = reinterpret_cast<int *>(smem_raw + (size_t)kAggInts * 4);
-  __shared__ __align__(16) PairArgs sd;
+  __shared__ __align__(16) unsigned char sd_raw[sizeof(PairArgs)];
+  const PairArgs &sd = *reinterpret_cast<const PairArgs *>(sd_raw);
   __shared__ int s_t;
   int cur = -1;
   for (;;) {
@@ -411,7 +431,7 @@ __global__ void __launch_bounds__(256, MINB)
     const BatchTile T = tiles[t];
     if (T.k != cur) {
       for (int q = threadIdx.x; q < (int)(sizeof(PairArgs) / 4); q += blockDim.x)
-        reinterpret_cast<int32_t *>(&sd)[q] = reinterpret_cast<const int32_t *>(&descs[T.k])[q];
+        reinterpret_cast<int32_t *>(sd_raw)[q] = reinterpret_cast<const int32_t *>(&descs[T.k])[q];
       __syncthreads();
       for (int q = threadIdx.x; q < kAggInts; q += blockDim.x) ((int32_t *)sagg)[q] = ((const int32_t *)sd.agg)[q];
       cur = T.k;
@@ -1261,6 +1281,8 @@ struct tn93g_ctx {
   long launches = 0;
   size_t dev_out_n = 0;
   DevBuf bb[48];  // buffers of tn93g_batch_run (indexed by BatchBuf)
+  int count_path = 0;  // clean-site counts: 0 popcounts on the CUDA cores, 1 tensor cores (tcgen05)
+  DevBuf ohimg, tcagg, tcerr;
 };
 
 namespace {
@@ -1370,6 +1392,13 @@ const char *tn93g_strerror(int code)
 
 const char *tn93g_last_cuda_error(tn93g_ctx *ctx) { return ctx ? ctx->err.c_str() : ""; }
 
+int tn93g_set_count_path(tn93g_ctx *ctx, int path)
+{
+  if (!ctx || path < 0 || path > 1) return TN93G_EINVAL;
+  ctx->count_path = path;
+  return TN93G_OK;
+}
+
 int tn93g_create(tn93g_ctx **out, int device, size_t hbm_budget)
 {
   if (!out) return TN93G_EINVAL;
@@ -1399,6 +1428,7 @@ int tn93g_create(tn93g_ctx **out, int device, size_t hbm_budget)
         if (cudaEventCreate(&e) != cudaSuccess) rc = TN93G_ECUDA;
     }
     if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) rc = TN93G_ECUDA;
+    if (const char *e = getenv("TN93G_COUNT")) ctx->count_path = strcmp(e, "tc") == 0 ? 1 : 0;
     LogTable h;
     build_log_table(&h);
     if (cudaMalloc(&ctx->d_logt, sizeof(LogTable)) != cudaSuccess ||
@@ -1426,6 +1456,8 @@ void tn93g_destroy(tn93g_ctx *ctx)
     if (b->p) cudaFree(b->p);
   for (DevBuf &b : ctx->bb)
     if (b.p) cudaFree(b.p);
+  for (DevBuf *b : {&ctx->ohimg, &ctx->tcagg, &ctx->tcerr})
+    if (b->p) cudaFree(b->p);
   if (ctx->d_logt) cudaFree(ctx->d_logt);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   for (int q = 0; q < 2; q++) {
@@ -1689,6 +1721,25 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   TRY(ensure(ctx, ctx->site, sizeof(ctx->h_tab->site)));
   CU(cudaMemcpyAsync(ctx->agg.p, ctx->h_tab->ev, agg_n * sizeof(AggEntry), cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync(ctx->site.p, ctx->h_tab->site, sizeof(ctx->h_tab->site), cudaMemcpyHostToDevice, st));
+  // tensor-core count path: the one-hot operand image of every sequence (an extra 32-sequence block at the end,
+  // which the last 64-column tile reads)
+  const bool use_tc = ctx->count_path == 1 && Lc > 0;
+  const long tc_NB = (N + 31) / 32 + 1, tc_KS = (Lc + kTcStageK - 1) / kTcStageK;
+  if (use_tc) {
+    TRY(ensure(ctx, ctx->ohimg, (size_t)tc_KS * tc_NB * kTcBlockBytes));
+    TRY(ensure(ctx, ctx->tcerr, sizeof(unsigned long long)));
+    CU(cudaMemsetAsync(ctx->tcerr.p, 0, sizeof(unsigned long long), st));
+    const long nthr = tc_NB * 32 * tc_KS * (kTcStageK / 16);
+    onehot_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>((const uint8_t *)ctx->cc.p, N, Lc, tc_NB, tc_KS,
+                                                                  (uint8_t *)ctx->ohimg.p);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    static bool attr = false;
+    if (!attr) {
+      CU(cudaFuncSetAttribute(count_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+      attr = true;
+    }
+  }
   CU(cudaEventRecord(E[1], st));
 
   //------------------------------------------------------------------ bands
@@ -1737,6 +1788,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   // per band parity (double-buffered): distances, segment statistics, row sums; the replay queue is per band
   const size_t dslots = (size_t)band * ncols;
   TRY(ensure(ctx, ctx->dist, 2 * dslots * sizeof(double)));
+  if (use_tc) TRY(ensure(ctx, ctx->tcagg, 7 * dslots * sizeof(int32_t)));
   TRY(ensure(ctx, ctx->rq, dslots * sizeof(unsigned long long)));
   TRY(ensure(ctx, ctx->rqn, sizeof(unsigned)));
   TRY(ensure(ctx, ctx->counters, 4 * sizeof(unsigned long long)));
@@ -1833,6 +1885,30 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     const long cstart = rc.cross ? n1 : r0 + 1;
     const long cblk0 = (cstart - colbase) / 32;
     const long cblks = (ncols + 31) / 32 - cblk0;
+    if (use_tc && cblks > 0) {
+      // clean-site aggregates of the band's pairs on the tensor cores
+      TcArgs T;
+      T.onehot = (const uint8_t *)ctx->ohimg.p;
+      T.NB = tc_NB;
+      T.KS = tc_KS;
+      T.N = N;
+      T.n1 = n1;
+      T.cross = rc.cross;
+      T.r0 = r0;
+      T.r1 = r1;
+      T.ncols = ncols;
+      T.colbase = colbase;
+      T.cstart = cstart / kTcCols * kTcCols;
+      T.agg = (int32_t *)ctx->tcagg.p;
+      T.err = (unsigned long long *)ctx->tcerr.p;
+      const long rt0 = r0 / kTcRows * kTcRows;
+      const dim3 g((unsigned)((N - T.cstart + kTcCols - 1) / kTcCols), (unsigned)((r1 - rt0 + kTcRows - 1) / kTcRows));
+      count_tc_kernel<<<g, 128, kTcSmem, st>>>(T);
+      CU(cudaGetLastError());
+      ctx->launches++;
+      A.tcagg = (const int32_t *)ctx->tcagg.p;
+      A.tcplane = (size_t)nr * ncols;
+    }
     if (cblks > 0) {
       A.cstart = colbase + cblk0 * 32;
       CU(launch_pair(A, cblks, nr, st));
@@ -1880,7 +1956,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     return TN93G_OK;
   };
   // bands whose text is on its way to the host: parities, oldest first
-  int pend_par[2], pend_n = 0;
+  int pend_par[2] = {0, 0}, pend_n = 0;
   size_t pend_bytes[2] = {0, 0};
   bool par_used[2] = {false, false};
   auto deliver_oldest = [&]() -> int {
@@ -2035,6 +2111,14 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   sum->undecided = (long)counters[1];
   sum->pairs_replayed = (long)counters[2];
   ctx->dev_out_n = dev_off;
+  if (use_tc) {
+    unsigned long long tcerr = 0;
+    CU(cudaMemcpy(&tcerr, ctx->tcerr.p, sizeof tcerr, cudaMemcpyDeviceToHost));
+    if (tcerr) {
+      ctx->err = "the tensor-core count kernel timed out waiting for its pipeline";
+      return TN93G_ETIMEOUT;
+    }
+  }
   if (counters[3]) {
     ctx->err = "internal error: a row's text did not match its counted length";
     return TN93G_ECUDA;
@@ -3184,7 +3268,8 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
       if (keys[q] == key) t = (int)q;
     if (t < 0) {
       build_tables(ctx->h_tab, opts[k].mode, opts[k].subset);
-      h_agg.insert(h_agg.end(), ctx->h_tab->ev, ctx->h_tab->ev + agg_n);
+      const AggEntry *tab = reinterpret_cast<const AggEntry *>(ctx->h_tab);  // ev, ew, eww (contiguous)
+      h_agg.insert(h_agg.end(), tab, tab + agg_n);
       const SiteEntry *se = &ctx->h_tab->site[0][0];
       h_site.insert(h_site.end(), se, se + sizeof(ctx->h_tab->site) / sizeof(SiteEntry));
       t = (int)keys.size();

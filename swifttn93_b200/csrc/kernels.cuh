@@ -61,6 +61,8 @@ struct PairArgs {
   unsigned long long replay_cap;
   unsigned long long *counters;  // [0] pairs with an ambiguous log, [1] undecided pairs
   const LogTable *logt;
+  const int32_t *tcagg = nullptr;  // clean-site aggregates from the tensor-core kernel ([7][band rows][ncols])
+  size_t tcplane = 0;              // (band rows) x ncols
 };
 
 struct ReplayArgs {

@@ -1,6 +1,7 @@
 // tables.h -- per-site contribution tables of tn93's ambiguity semantics, built on the host once per run and
 // uploaded to the device.
 #pragma once
+#include <stddef.h>
 #include <stdint.h>
 
 namespace tn93 {
@@ -35,7 +36,12 @@ struct Tables {
   AggEntry ew[4];                      // N (or, under gapmm, a gap) facing clean base b
   AggEntry eww;                        // N facing N
   SiteEntry site[2][kCodes * kCodes];  // [0 main mode, 1 AVERAGE][c1 * 18 + c2]
+  // ev, ew and eww form one array of kSparseCodes * kCodes + 5 entries (copied to the device as one table)
+  const AggEntry *agg() const { return ev; }
 };
+static_assert(offsetof(Tables, ew) == sizeof(AggEntry) * kSparseCodes * kCodes &&
+                  offsetof(Tables, eww) == offsetof(Tables, ew) + 4 * sizeof(AggEntry),
+              "the event tables are contiguous");
 
 // mode: 0 resolve, 1 average, 2 skip, 3 gapmm, 4 subset; subset[c] = 1 for codes listed in -a LIST
 void build_tables(Tables *T, int mode, const unsigned char subset[kCodes]);

@@ -1,0 +1,306 @@
+// tc_count.cuh -- clean-site counts of every pair on the 5th-generation tensor cores (tcgen05, INT8).
+//
+// For a pair (i, j) the 4x4 table of clean-site base combinations is N_ab(i, j) = sum_k x_i[k][a] x_j[k][b], where
+// x_s[k][c] = 1 when sequence s has the clean base c (A, C, G, T = 0..3) at column k. Stacking the four class
+// indicator rows of 32 sequences gives A' (128 rows, K = columns); of 64 sequences, B' (256 rows). One
+// tcgen05.mma of kind::i8 (M = 128, N = 256, K = 32, u8 x u8 -> s32 in tensor memory) per 32 columns
+// accumulates D = A' B'^T, whose 4x4 blocks are the pairs' tables. The epilogue turns each table into the seven
+// clean-site aggregates the pair kernel needs (jointly clean sites, matches, A<->G and C<->T transitions, and the
+// A, C, G base counts over both sequences) and stores them as int32 [7][band rows][band columns].
+//
+// Operand image in HBM (built by onehot_kernel from the compressed codes): per 128-column stage s and 32-sequence
+// block b a 16 KB block at (s * NB + b) * 16 KB, in the canonical K-major layout without swizzle: row r =
+// 4 * sequence + class, row group g = r / 8 at g * 1024 B, 16-byte column chunk c at + c * 128 B, row r % 8 at
+// + (r % 8) * 16 B. Descriptor: leading (K) byte offset 128, stride (8-row group) byte offset 1024. A B' tile is
+// two consecutive blocks of the same stage (32 KB, row groups 16..31 continue at 16 KB).
+//
+// One CTA per tile of 32 rows x 64 columns, 128 threads: thread 0 issues the bulk copies (cp.async.bulk with
+// mbarrier transaction counts) into a 2-stage ring, thread 32 issues the MMAs and commits each stage back to its
+// producer barrier, then all four warps read the accumulator (warp w holds TMEM lanes 32w..32w+31). Every wait
+// is bounded; on a timeout the CTA records an error word, drains its copies and frees its tensor memory.
+#pragma once
+#include <stdint.h>
+
+namespace tn93 {
+
+constexpr int kTcRows = 32;                     // sequences per A' tile (128 rows of 4 classes)
+constexpr int kTcCols = 64;                     // sequences per B' tile (256 rows)
+constexpr int kTcStageK = 128;                  // columns (bytes) per pipeline stage
+constexpr int kTcBlockBytes = 32 * 4 * kTcStageK;  // one 32-sequence block of one stage: 16 KB
+constexpr int kTcStages = 2;
+constexpr int kTcStageBytes = 3 * kTcBlockBytes;   // A (one block) + B (two blocks)
+constexpr size_t kTcSmem = (size_t)kTcStages * kTcStageBytes + 1024;
+constexpr uint32_t kTcWaitLimit = 1u << 26;     // spin iterations before a wait gives up
+
+struct TcArgs {
+  const uint8_t *onehot;  // operand image
+  long NB;                // 32-sequence blocks in the image (the last B' tile reads one block past the data)
+  long KS;                // 128-column stages
+  long N, n1;             // sequences; first column sequence under -s
+  bool cross;
+  long r0, r1;            // band rows
+  long ncols, colbase;    // output row stride and first column it holds
+  long cstart;            // first column tile (a multiple of 64 past 0)
+  int32_t *agg;           // [7][r1 - r0][ncols]
+  unsigned long long *err;  // set when a wait gave up
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait: false when it gave up
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+  for (uint32_t it = 0; it < kTcWaitLimit; it++)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// K-major, no swizzle: start address, leading (K) byte offset, stride (8-row group) byte offset, version 1
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// kind::i8 instruction descriptor: s32 accumulator, u8 x u8, both K-major, N = 256, M = 128
+constexpr uint32_t kTcIdesc = (2u << 4) | ((uint32_t)(256 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
+{
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar)
+{
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16])
+{
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// one thread per (sequence, 16 columns): the four class rows' 16 bytes of the operand image
+__global__ void onehot_kernel(const uint8_t *__restrict__ cc, long N, long Lc, long NB, long KS, uint8_t *img)
+{
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long nchunk = KS * (kTcStageK / 16);
+  if (t >= NB * 32 * nchunk) return;
+  const long seq = t / nchunk, ch = t % nchunk;
+  const long s = ch / (kTcStageK / 16), c = ch % (kTcStageK / 16);
+  const long k0 = ch * 16;
+  uint8_t code[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) code[q] = (seq < N && k0 + q < Lc) ? cc[seq * Lc + k0 + q] : (uint8_t)17;
+  const long b = seq / 32, sl = seq % 32;
+  uint8_t *blk = img + ((size_t)s * NB + b) * kTcBlockBytes;
+#pragma unroll
+  for (int cls = 0; cls < 4; cls++) {
+    const int r = (int)sl * 4 + cls;
+    uint32_t w[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      w[q] = (uint32_t)(code[4 * q] == cls) | ((uint32_t)(code[4 * q + 1] == cls) << 8) |
+             ((uint32_t)(code[4 * q + 2] == cls) << 16) | ((uint32_t)(code[4 * q + 3] == cls) << 24);
+    *reinterpret_cast<uint4 *>(blk + (r / 8) * 1024 + c * 128 + (r % 8) * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+__global__ void __launch_bounds__(128) count_tc_kernel(TcArgs a)
+{
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  __shared__ __align__(8) uint64_t full[kTcStages], empty[kTcStages], done;
+  __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // A' tiles are whole 32-sequence blocks: the first one starts at the band's first row rounded down
+  const long i0 = (a.r0 / kTcRows) * kTcRows + blockIdx.y * (long)kTcRows;
+  const long j0 = a.cstart + blockIdx.x * (long)kTcCols;
+  // block-uniform exit: no valid pair in the tile
+  if (i0 >= a.r1 || j0 >= a.N) return;
+  if (!a.cross && j0 + kTcCols - 1 <= i0) return;
+  if (a.cross && j0 + kTcCols <= a.n1) return;
+  // 1 KB aligned stage ring
+  unsigned char *ring = (unsigned char *)(((uintptr_t)tsm + 1023) & ~(uintptr_t)1023);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kTcStages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(&done, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(256u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base;
+  const long KS = a.KS;
+  const long ab = (i0 / 32), bb = (j0 / 32);
+  int fills[kTcStages] = {0, 0};
+  if (threadIdx.x == 0) {
+    // producer: stage ring of A (16 KB) + B (32 KB)
+    for (long k = 0; k < KS; k++) {
+      const int s = (int)(k % kTcStages);
+      if (k >= kTcStages && !mbar_wait(&empty[s], (uint32_t)(((k / kTcStages) - 1) & 1))) {
+        atomicExch(&abort_flag, 1);
+        break;
+      }
+      if (*(volatile int *)&abort_flag) break;
+      unsigned char *dst = ring + (size_t)s * kTcStageBytes;
+      mbar_arrive_expect_tx(&full[s], (uint32_t)kTcStageBytes);
+      bulk_g2s(dst, a.onehot + ((size_t)k * a.NB + ab) * kTcBlockBytes, kTcBlockBytes, &full[s]);
+      bulk_g2s(dst + kTcBlockBytes, a.onehot + ((size_t)k * a.NB + bb) * kTcBlockBytes, 2 * kTcBlockBytes, &full[s]);
+      fills[s]++;
+    }
+  } else if (threadIdx.x == 32) {
+    // MMA issuer
+    long k = 0;
+    for (; k < KS; k++) {
+      const int s = (int)(k % kTcStages);
+      if (!mbar_wait(&full[s], (uint32_t)((k / kTcStages) & 1))) {
+        atomicExch(&abort_flag, 1);
+        break;
+      }
+      tc_fence_after();
+      const uint32_t sa = smem_u32(ring + (size_t)s * kTcStageBytes), sb = sa + kTcBlockBytes;
+#pragma unroll
+      for (int kk = 0; kk < kTcStageK / 32; kk++)
+        umma_i8(tmem, umma_desc(sa + kk * 256, 128, 1024), umma_desc(sb + kk * 256, 128, 1024),
+                (k > 0 || kk > 0) ? 1u : 0u);
+      umma_commit(&empty[s]);
+    }
+    umma_commit(&done);  // arrives when every MMA issued above has completed
+  }
+  // epilogue: all four warps (reconverged: tcgen05.ld is warp-collective)
+  __syncwarp();
+  const bool ok = __all_sync(0xffffffffu, mbar_wait(&done, 0));
+  tc_fence_after();
+  const bool go = __all_sync(0xffffffffu, ok && !*(volatile int *)&abort_flag);
+  if (go) {
+    const int il = warp * 8 + lane / 4, cls = lane & 3;
+    const long i = i0 + il;
+    const long rows = a.r1 - a.r0;
+    const size_t plane = (size_t)rows * a.ncols;
+    for (int c16 = 0; c16 < 256 / 16; c16++) {
+      uint32_t v[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c16 * 16), v);
+      // v[4 * jj + b] = N_{cls, b}(i, j = 4 * c16 + jj)
+      int T[4], dg[4], ag[4], ct[4], col[4][4], rowm[4];
+#pragma unroll
+      for (int jj = 0; jj < 4; jj++) {
+        const int n0 = (int)v[4 * jj], n1 = (int)v[4 * jj + 1], n2 = (int)v[4 * jj + 2], n3 = (int)v[4 * jj + 3];
+        rowm[jj] = n0 + n1 + n2 + n3;
+        T[jj] = rowm[jj];
+        dg[jj] = cls == 0 ? n0 : cls == 1 ? n1 : cls == 2 ? n2 : n3;
+        ag[jj] = cls == 0 ? n2 : cls == 2 ? n0 : 0;
+        ct[jj] = cls == 1 ? n3 : cls == 3 ? n1 : 0;
+        col[jj][0] = n0;
+        col[jj][1] = n1;
+        col[jj][2] = n2;
+        col[jj][3] = n3;
+      }
+      // totals over the four class rows of sequence i (lanes 4m..4m+3)
+#pragma unroll
+      for (int o = 1; o < 4; o <<= 1)
+#pragma unroll
+        for (int jj = 0; jj < 4; jj++) {
+          T[jj] += __shfl_xor_sync(0xffffffffu, T[jj], o);
+          dg[jj] += __shfl_xor_sync(0xffffffffu, dg[jj], o);
+          ag[jj] += __shfl_xor_sync(0xffffffffu, ag[jj], o);
+          ct[jj] += __shfl_xor_sync(0xffffffffu, ct[jj], o);
+#pragma unroll
+          for (int b = 0; b < 3; b++) col[jj][b] += __shfl_xor_sync(0xffffffffu, col[jj][b], o);
+        }
+      // this lane finishes column jj = cls: base counts of A, C, G over both sequences
+      const int base = lane & ~3;
+      int out[7] = {0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int jj = 0; jj < 4; jj++) {
+        const int rA = __shfl_sync(0xffffffffu, rowm[jj], base + 0);
+        const int rC = __shfl_sync(0xffffffffu, rowm[jj], base + 1);
+        const int rG = __shfl_sync(0xffffffffu, rowm[jj], base + 2);
+        if (jj == cls) {
+          out[0] = T[jj];
+          out[1] = dg[jj];
+          out[2] = ag[jj];
+          out[3] = ct[jj];
+          out[4] = rA + col[jj][0];
+          out[5] = rC + col[jj][1];
+          out[6] = rG + col[jj][2];
+        }
+      }
+      const long j = j0 + 4 * c16 + cls;
+      const long lb = a.cross ? a.n1 : i + 1;
+      if (i >= a.r0 && i < a.r1 && j >= lb && j < a.N) {
+        int32_t *dst = a.agg + (size_t)(i - a.r0) * a.ncols + (j - a.colbase);
+#pragma unroll
+        for (int q = 0; q < 7; q++) dst[q * plane] = out[q];
+      }
+    }
+  }
+  // on a timeout: report it, and let the last fill of each stage land before the ring is released (a stage is
+  // refilled only after its previous fill was consumed, so only the last fill can still be in flight)
+  if (!go && threadIdx.x == 0) {
+    atomicAdd(a.err, 1ull);
+    for (int s = 0; s < kTcStages; s++)
+      if (fills[s]) mbar_wait(&full[s], (uint32_t)((fills[s] - 1) & 1));
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u));
+}
+
+}  // namespace tn93

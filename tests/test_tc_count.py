@@ -1,0 +1,77 @@
+"""The tensor-core count path (tcgen05 INT8 one-hot products, tn93g_set_count_path(ctx, 1)) must give exactly the
+bytes and summaries of the CUDA-core popcount path, which the other parity tests pin to the oracle and the
+reference: tile and word edges in every ambiguity mode, the two-file modes, row bands starting off the 32-row
+grid, and a real alignment with non-dyadic pairs."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _both(eng, s, opts, n1=None, rows=None):
+    out = []
+    for path in ("popc", "tc"):
+        eng.set_count_path(path)
+        if rows is None:
+            body, summ = eng.run(s, opts, n1=n1)
+            out.append((body, summ.json(s.N if n1 is None else n1, 0 if n1 is None else s.N - n1, n1 is not None,
+                                        opts.do_fst), summ.links))
+        else:
+            body, summ, rs = eng.run_rows(s, opts, rows[0], rows[1], n1=n1)
+            out.append((body, rs.tobytes(), summ.links, summ.max))
+    eng.set_count_path("popc")
+    return out
+
+
+def test_tc_equals_popc_edges():
+    from swifttn93_b200 import Engine, Options, synth
+
+    names0, codes0 = synth.plain_small()
+    rng = np.random.default_rng(3)
+    eng = Engine()
+    for n, L in ((1, 70), (2, 1), (31, 63), (32, 64), (33, 65), (65, 129), (100, 300), (97, 1300)):
+        rows = rng.choice(len(names0), n, replace=False)
+        cols = np.sort(rng.choice(codes0.shape[1], L, replace=False))
+        s = eng.upload(codes0[rows][:, cols], [names0[r] for r in rows], 1 + np.arange(n) % 2)
+        for kw in (dict(threshold=1.0, mode="resolve", min_overlap=1),
+                   dict(threshold=0.1, mode="average", min_overlap=10, format="csvn"),
+                   dict(threshold=0.1, mode="gapmm", min_overlap=5, report_self=True),
+                   dict(threshold=0.2, mode="skip", min_overlap=1),
+                   dict(threshold=0.05, mode="RY", resolve_fraction=0.05, min_overlap=20)):
+            a, b = _both(eng, s, Options(**kw))
+            assert a == b, (n, L, kw)
+        eng.free(s)
+    eng.close()
+
+
+def test_tc_equals_popc_two_files_bands_and_real_data():
+    from swifttn93_b200 import Engine, Options, synth
+    from tests import cases
+
+    names, codes = synth.plain_small()
+    eng = Engine()
+    s = eng.upload(codes, names)
+    o = Options(threshold=0.03, mode="resolve", resolve_fraction=0.05, min_overlap=500)
+    for n1 in (300, 77):
+        a, b = _both(eng, s, o, n1=n1)
+        assert a == b, n1
+    a, b = _both(eng, s, Options(threshold=0.03, mode="average", do_fst=True), n1=300)
+    assert a == b
+    for r0, r1 in ((0, 500), (5, 37), (33, 250), (499, 500)):
+        a, b = _both(eng, s, o, rows=(r0, r1))
+        assert a == b, (r0, r1)
+    eng.free(s)
+    fa = cases.source_bytes("real:hiv_dev")[0].split(b">")[1:601]
+    nm = [r.split(b"\n", 1)[0].decode() for r in fa]
+    seqs = [r.split(b"\n", 1)[1].replace(b"\n", b"") for r in fa]
+    lut = np.full(256, 255, dtype=np.uint8)
+    for k, ch in enumerate(synth.ALPHABET):
+        lut[ch] = k
+        lut[ord(chr(ch).lower())] = k
+    c2 = np.stack([lut[np.frombuffer(x, dtype=np.uint8)] for x in seqs])
+    s2 = eng.upload(c2, nm)
+    for m in ("resolve", "average", "gapmm"):
+        a, b = _both(eng, s2, Options(threshold=0.05, mode=m, resolve_fraction=0.05, min_overlap=500))
+        assert a == b, m
+    eng.free(s2)
+    eng.close()
