@@ -124,10 +124,11 @@ long tn93g_last_launches(tn93g_ctx *ctx);
  * [5] device->host copies, [6] whole run. Returns the number of entries written (<= n). */
 int tn93g_last_timings(tn93g_ctx *ctx, double *ms, int n);
 
-/* Selects how the pair stage counts clean-site base combinations: 0 = AND/XOR + POPC over bit planes on the CUDA
- * cores (the default), 1 = one-hot INT8 matrix products on the tensor cores (tcgen05.mma kind::i8, counts in tensor
- * memory). Both give the same integers, so every output is identical; the environment variable TN93G_COUNT=tc
- * sets 1 when a context is created. Replaces: nothing (the reference has one CPU counting path). */
+/* Selects how the pair stage counts clean-site base combinations in tn93g_run / tn93g_run_rows: 0 = AND/XOR + POPC
+ * over bit planes on the CUDA cores, 1 = one-hot INT8 matrix products on the tensor cores (tcgen05.mma kind::i8,
+ * counts in tensor memory; the default, measured faster). Both give the same integers, so every output is
+ * identical; the environment variable TN93G_COUNT=popc selects 0 when a context is created. Replaces: nothing
+ * (the reference has one CPU counting path). */
 int tn93g_set_count_path(tn93g_ctx *ctx, int path);
 
 /* ---- row bands (one alignment split over several GPUs) ----

@@ -1281,7 +1281,7 @@ struct tn93g_ctx {
   long launches = 0;
   size_t dev_out_n = 0;
   DevBuf bb[48];  // buffers of tn93g_batch_run (indexed by BatchBuf)
-  int count_path = 0;  // clean-site counts: 0 popcounts on the CUDA cores, 1 tensor cores (tcgen05)
+  int count_path = 1;  // clean-site counts: 0 popcounts on the CUDA cores, 1 tensor cores (tcgen05)
   DevBuf ohimg, tcagg, tcerr;
 };
 
@@ -1428,7 +1428,7 @@ int tn93g_create(tn93g_ctx **out, int device, size_t hbm_budget)
         if (cudaEventCreate(&e) != cudaSuccess) rc = TN93G_ECUDA;
     }
     if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) rc = TN93G_ECUDA;
-    if (const char *e = getenv("TN93G_COUNT")) ctx->count_path = strcmp(e, "tc") == 0 ? 1 : 0;
+    if (const char *e = getenv("TN93G_COUNT")) ctx->count_path = strcmp(e, "popc") == 0 ? 0 : 1;
     LogTable h;
     build_log_table(&h);
     if (cudaMalloc(&ctx->d_logt, sizeof(LogTable)) != cudaSuccess ||
