@@ -3041,7 +3041,8 @@ enum BatchBuf {
   BB_CODES, BB_SEEN, BB_NN, BB_VARCOL, BB_PLANES, BB_CC, BB_CCT, BB_EVCOUNT, BB_EVOFF, BB_EV, BB_AGG, BB_SITE,
   BB_NAMES, BB_NAMEOFF, BB_NAMELEN, BB_COUNTS, BB_DIST, BB_RQ, BB_RQN, BB_COUNTERS, BB_PDESC, BB_RDESC, BB_ROWDESC,
   BB_TILES, BB_NEXT, BB_BLOCKS, BB_SBYTES, BB_SOFF, BB_SLINKS, BB_SSKIP, BB_SMAX, BB_RSUM, BB_RW, BB_HIST, BB_TOTAL,
-  BB_SCANTMP, BB_RED, BB_REDC, BB_FIRST, BB_FIRSTIDX, BB_OUT, BB_COUNT
+  BB_SCANTMP, BB_RED, BB_REDC, BB_FIRST, BB_FIRSTIDX, BB_OUT, BB_OH, BB_TCAGG, BB_TCDESC, BB_TCTILES, BB_TCERR,
+  BB_COUNT
 };
 static_assert(BB_COUNT <= 48, "batch buffer table");
 
@@ -3339,12 +3340,74 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
     R.counters = A.counters;
     R.logt = ctx->d_logt;
   }
-  // the tile queue: per kernel class, longest alignments first
-  std::vector<BatchTile> tiles;
-  int cls_n[3] = {0, 0, 0};
   std::vector<int> order(K);
   for (int k = 0; k < K; k++) order[k] = k;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return RC[a].Lc > RC[b].Lc; });
+  // tensor-core count path: per alignment a one-hot operand image and its clean-site aggregates ([7][n][n]),
+  // computed by one launch over every alignment's 32 x 64 tiles
+  const bool use_tc = ctx->count_path == 1;
+  if (use_tc) {
+    std::vector<size_t> oh_off(K + 1, 0), ag_off(K + 1, 0);
+    std::vector<TcArgs> TD(K);
+    std::vector<int4> tct;
+    for (int k = 0; k < K; k++) {
+      const long N = alns[k].n;
+      const bool on = RC[k].W > 0 && N > 1;
+      const long NB = (N + 31) / 32 + 1, KS = (RC[k].Lc + kTcStageK - 1) / kTcStageK;
+      oh_off[k + 1] = oh_off[k] + (on ? (size_t)KS * NB * kTcBlockBytes : 0);
+      ag_off[k + 1] = ag_off[k] + (on ? (size_t)7 * N * N : 0);
+      TcArgs &T = TD[k];
+      memset(&T, 0, sizeof T);
+      T.NB = NB;
+      T.KS = KS;
+      T.N = N;
+      T.n1 = N;
+      T.cross = false;
+      T.r0 = 0;
+      T.r1 = N;
+      T.ncols = N;
+      T.colbase = 0;
+      T.cstart = 0;
+    }
+    TRY(ensure(ctx, bb[BB_OH], std::max<size_t>(oh_off[K], 16)));
+    TRY(ensure(ctx, bb[BB_TCAGG], std::max<size_t>(ag_off[K], 1) * sizeof(int32_t)));
+    TRY(ensure(ctx, bb[BB_TCERR], sizeof(unsigned long long)));
+    CU(cudaMemsetAsync(bb[BB_TCERR].p, 0, sizeof(unsigned long long), st));
+    for (int k : order) {
+      if (oh_off[k + 1] == oh_off[k]) continue;
+      TcArgs &T = TD[k];
+      T.onehot = (const uint8_t *)bb[BB_OH].p + oh_off[k];
+      T.agg = (int32_t *)bb[BB_TCAGG].p + ag_off[k];
+      T.err = (unsigned long long *)bb[BB_TCERR].p;
+      const long nthr = T.NB * 32 * T.KS * (kTcStageK / 16);
+      onehot_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>(PA[k].cc, T.N, RC[k].Lc, T.NB, T.KS,
+                                                                    (uint8_t *)bb[BB_OH].p + oh_off[k]);
+      CU(cudaGetLastError());
+      ctx->launches++;
+      for (long i0 = 0; i0 < T.N - 1; i0 += kTcRows)
+        for (long j0 = (i0 + 1) / kTcCols * kTcCols; j0 < T.N; j0 += kTcCols) tct.push_back(make_int4(k, (int)i0, (int)j0, 0));
+      PD[k].tcagg = T.agg;
+      PD[k].tcplane = (size_t)T.N * T.N;
+    }
+    if (!tct.empty()) {
+      TRY(ensure(ctx, bb[BB_TCDESC], K * sizeof(TcArgs)));
+      TRY(ensure(ctx, bb[BB_TCTILES], tct.size() * sizeof(int4)));
+      CU(cudaMemcpyAsync(bb[BB_TCDESC].p, TD.data(), K * sizeof(TcArgs), cudaMemcpyHostToDevice, st));
+      CU(cudaMemcpyAsync(bb[BB_TCTILES].p, tct.data(), tct.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+      static bool attr = false;
+      if (!attr) {
+        CU(cudaFuncSetAttribute(count_tc_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+        attr = true;
+      }
+      count_tc_batch_kernel<<<(unsigned)tct.size(), 128, kTcSmem, st>>>((const TcArgs *)bb[BB_TCDESC].p,
+                                                                      (const int4 *)bb[BB_TCTILES].p);
+      CU(cudaGetLastError());
+      ctx->launches++;
+    }
+  }
+  // the tile queue: per kernel class, longest alignments first
+  std::vector<BatchTile> tiles;
+  int cls_n[3] = {0, 0, 0};
   for (int cls = 0; cls < 3; cls++)
     for (int k : order) {
       const int kc = RC[k].gapmm ? 2 : RC[k].wplane ? 1 : 0;
@@ -3497,6 +3560,14 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
   for (int q = 0; q < 7; q++) {
     CU(cudaEventElapsedTime(&ms, E[pairs_e[q][0]], E[pairs_e[q][1]]));
     ctx->timings[q] = ms;
+  }
+  if (use_tc) {
+    unsigned long long tcerr = 0;
+    CU(cudaMemcpy(&tcerr, bb[BB_TCERR].p, sizeof tcerr, cudaMemcpyDeviceToHost));
+    if (tcerr) {
+      ctx->err = "the tensor-core count kernel timed out waiting for its pipeline";
+      return TN93G_ETIMEOUT;
+    }
   }
   for (int k = 0; k < K; k++) {
     if (counters[4 * k + 3]) {

@@ -152,16 +152,15 @@ __global__ void onehot_kernel(const uint8_t *__restrict__ cc, long N, long Lc, l
   }
 }
 
-__global__ void __launch_bounds__(128) count_tc_kernel(TcArgs a)
+// One tile: A' = the 32 sequences from i0 (a multiple of 32), B' = the 64 from j0 (a multiple of 32). All 128
+// threads of the block call it with the same arguments.
+__device__ __forceinline__ void count_tc_tile(const TcArgs &a, long i0, long j0)
 {
   extern __shared__ __align__(1024) unsigned char tsm[];
   __shared__ __align__(8) uint64_t full[kTcStages], empty[kTcStages], done;
   __shared__ uint32_t tmem_base;
   __shared__ int abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // A' tiles are whole 32-sequence blocks: the first one starts at the band's first row rounded down
-  const long i0 = (a.r0 / kTcRows) * kTcRows + blockIdx.y * (long)kTcRows;
-  const long j0 = a.cstart + blockIdx.x * (long)kTcCols;
   // block-uniform exit: no valid pair in the tile
   if (i0 >= a.r1 || j0 >= a.N) return;
   if (!a.cross && j0 + kTcCols - 1 <= i0) return;
@@ -301,6 +300,19 @@ __global__ void __launch_bounds__(128) count_tc_kernel(TcArgs a)
   __syncthreads();
   tc_fence_after();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u));
+}
+
+// the tiles of one band: A' tiles start at the band's first row rounded down to a 32-sequence block
+__global__ void __launch_bounds__(128) count_tc_kernel(TcArgs a)
+{
+  count_tc_tile(a, (a.r0 / kTcRows) * kTcRows + blockIdx.y * (long)kTcRows, a.cstart + blockIdx.x * (long)kTcCols);
+}
+
+// a batch of alignments: block b is tile tiles[b] = (alignment, first row, first column)
+__global__ void __launch_bounds__(128) count_tc_batch_kernel(const TcArgs *descs, const int4 *tiles)
+{
+  const int4 t = tiles[blockIdx.x];
+  count_tc_tile(descs[t.x], t.y, t.z);
 }
 
 }  // namespace tn93

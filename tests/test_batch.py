@@ -61,12 +61,14 @@ def test_batch_equals_alone_for_every_tile_shape():
     eng = Engine()
     alone = [_alone(eng, a, o) for a, o in items]
     alns, opts = [a for a, _ in items], [o for _, o in items]
-    for rpw, blocks in ((None, 0), ([1] * len(items), 2), ([2] * len(items), 3), ([4, 1, 2] * 4, 2)):
+    for path, rpw, blocks in (("tc", None, 0), ("popc", None, 0), ("tc", [1] * len(items), 2),
+                              ("popc", [2] * len(items), 3), ("tc", [4, 1, 2] * 4, 3)):
+        eng.set_count_path(path)
         got = eng.batch_run(alns, opts, rows_per_warp=None if rpw is None else rpw[:len(items)], pair_blocks=blocks)
         for k, ((b, s), (wb, ws)) in enumerate(zip(got, alone)):
-            assert b == wb, (k, rpw, blocks, len(b), len(wb))
+            assert b == wb, (k, path, rpw, blocks, len(b), len(wb))
             n = alns[k].n
-            assert s.json(n) == ws.json(n), (k, rpw, blocks)
+            assert s.json(n) == ws.json(n), (k, path, rpw, blocks)
             assert s.links == ws.links and s.pairwise == ws.pairwise
     eng.close()
 
