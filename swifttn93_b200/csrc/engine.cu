@@ -1196,8 +1196,7 @@ __global__ void fill_nan_kernel(double *p, size_t n)
 }
 
 // pair kernel launch (dynamic shared memory above the 48 KB default needs the opt-in attribute once). Two
-// register budgets are built: 2 blocks per SM (128 registers, no spills) and 3 (80 registers, some spills);
-// TN93G_PAIR_BLOCKS=3 selects the second. They measured the same on the benchmark workload.
+// register budgets are built: 2 blocks per SM (128 registers, no spills) and 3 (80 registers, some spills).
 template <int MINB>
 cudaError_t launch_pair_t(const PairArgs &A, dim3 g, cudaStream_t st)
 {
@@ -1225,12 +1224,16 @@ cudaError_t launch_pair_t(const PairArgs &A, dim3 g, cudaStream_t st)
   return cudaGetLastError();
 }
 
+// Resident blocks per SM: 3 (80 registers a thread) when the clean-site counts come from the tensor cores, 2 (128)
+// with the popcount loop, which needs the registers (measured: 3 is 11% faster on the tensor-core path, and slower
+// with the popcount loop). TN93G_PAIR_BLOCKS=2|3 overrides.
 cudaError_t launch_pair(const PairArgs &A, long ncolblocks, long nrows, cudaStream_t st)
 {
-  static const int minb = [] {
+  static const int forced = [] {
     const char *e = getenv("TN93G_PAIR_BLOCKS");
-    return (e && atoi(e) == 3) ? 3 : 2;
+    return e ? (atoi(e) == 3 ? 3 : 2) : 0;
   }();
+  const int minb = forced ? forced : (A.tcagg ? 3 : 2);
   dim3 g((unsigned)ncolblocks, (unsigned)((nrows + kTile - 1) / kTile));
   return minb == 3 ? launch_pair_t<3>(A, g, st) : launch_pair_t<2>(A, g, st);
 }
