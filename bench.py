@@ -478,13 +478,13 @@ def main():
         work = pairs_run * classes * classes * Lc * 2  # INT8 one-hot MAC equivalents (x2 ops)
         achieved = work / (per_launch_ms / 1e3) / 1e12
         # DRAM bytes of the pair stage (count_tc_kernel + pair_kernel) from the ncu capture of the 4,000-sequence
-        # prefix (profiles/count_tc_kernel_hiv_bench_n4000.md: 215.5 + 281.4 MB for 7,998,000 pairs), scaled by
+        # prefix (profiles/count_tc_kernel_hiv_bench_n4000.md: 104.5 + 167.8 MB for 7,998,000 pairs), scaled by
         # pairs to this launch
-        traffic = 496.9e6 * pairs_run / 7998000
+        traffic = 272.3e6 * pairs_run / 7998000
         roof = {"kernel": "count_tc_kernel + pair_kernel", "bound": "tensor", "achieved": achieved,
                 "peak": 2 * P["bf16"], "unit": "TFLOP/s", "frac": achieved / (2 * P["bf16"]), "traffic": traffic,
                 "traffic_note": "bytes per pair stage, ncu on a 4,000-sequence prefix scaled by pairs; mostly the "
-                                "28-byte clean-site aggregates written by the tensor-core kernel and read back",
+                                "14-byte clean-site aggregates written by the tensor-core kernel and read back",
                 "tensor_pipe_active": 0.295,
                 "peak_note": f"dense INT8 = 2 x {P['src']} bf16 ({P['bf16']} TF/s)",
                 "work_note": f"{classes}x{classes}xLc INT8 MACs per pair, Lc={Lc}"}

@@ -369,9 +369,16 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const AggEntry *sag
     }
     int cl[7];
     if (tc) {
-      const int32_t *g = a.tcagg + (size_t)(i - a.r0) * a.ncols + (jj - a.colbase);
+      const size_t at = (size_t)(i - a.r0) * a.ncols + (jj - a.colbase);
+      if (a.tc16) {
+        const uint16_t *g = (const uint16_t *)a.tcagg + at;
 #pragma unroll
-      for (int q = 0; q < 7; q++) cl[q] = valid ? g[q * a.tcplane] : 0;
+        for (int q = 0; q < 7; q++) cl[q] = valid ? (int)g[q * a.tcplane] : 0;
+      } else {
+        const int32_t *g = (const int32_t *)a.tcagg + at;
+#pragma unroll
+        for (int q = 0; q < 7; q++) cl[q] = valid ? g[q * a.tcplane] : 0;
+      }
     } else {
       const int nfT = c.T1 + c.T2, nfC = c.Y1 + c.Y2 - nfT, nfG = c.L1 + c.L2 - nfT;
       cl[0] = c.T;
@@ -1791,7 +1798,8 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   // per band parity (double-buffered): distances, segment statistics, row sums; the replay queue is per band
   const size_t dslots = (size_t)band * ncols;
   TRY(ensure(ctx, ctx->dist, 2 * dslots * sizeof(double)));
-  if (use_tc) TRY(ensure(ctx, ctx->tcagg, 7 * dslots * sizeof(int32_t)));
+  const int tc16 = 2 * Lc < 65536;
+  if (use_tc) TRY(ensure(ctx, ctx->tcagg, 7 * dslots * (tc16 ? sizeof(uint16_t) : sizeof(int32_t))));
   TRY(ensure(ctx, ctx->rq, dslots * sizeof(unsigned long long)));
   TRY(ensure(ctx, ctx->rqn, sizeof(unsigned)));
   TRY(ensure(ctx, ctx->counters, 4 * sizeof(unsigned long long)));
@@ -1902,15 +1910,17 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
       T.ncols = ncols;
       T.colbase = colbase;
       T.cstart = cstart / kTcCols * kTcCols;
-      T.agg = (int32_t *)ctx->tcagg.p;
+      T.agg = ctx->tcagg.p;
+      T.agg16 = tc16;
       T.err = (unsigned long long *)ctx->tcerr.p;
       const long rt0 = r0 / kTcRows * kTcRows;
       const dim3 g((unsigned)((N - T.cstart + kTcCols - 1) / kTcCols), (unsigned)((r1 - rt0 + kTcRows - 1) / kTcRows));
       count_tc_kernel<<<g, 128, kTcSmem, st>>>(T);
       CU(cudaGetLastError());
       ctx->launches++;
-      A.tcagg = (const int32_t *)ctx->tcagg.p;
+      A.tcagg = ctx->tcagg.p;
       A.tcplane = (size_t)nr * ncols;
+      A.tc16 = tc16;
     }
     if (cblks > 0) {
       A.cstart = colbase + cblk0 * 32;
@@ -3358,7 +3368,9 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
       const bool on = RC[k].W > 0 && N > 1;
       const long NB = (N + 31) / 32 + 1, KS = (RC[k].Lc + kTcStageK - 1) / kTcStageK;
       oh_off[k + 1] = oh_off[k] + (on ? (size_t)KS * NB * kTcBlockBytes : 0);
-      ag_off[k + 1] = ag_off[k] + (on ? (size_t)7 * N * N : 0);
+      // byte offsets, each alignment's block 16-byte aligned
+      const size_t esz = 2 * RC[k].Lc < 65536 ? sizeof(uint16_t) : sizeof(int32_t);
+      ag_off[k + 1] = ag_off[k] + (on ? ((size_t)7 * N * N * esz + 15) / 16 * 16 : 0);
       TcArgs &T = TD[k];
       memset(&T, 0, sizeof T);
       T.NB = NB;
@@ -3373,14 +3385,15 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
       T.cstart = 0;
     }
     TRY(ensure(ctx, bb[BB_OH], std::max<size_t>(oh_off[K], 16)));
-    TRY(ensure(ctx, bb[BB_TCAGG], std::max<size_t>(ag_off[K], 1) * sizeof(int32_t)));
+    TRY(ensure(ctx, bb[BB_TCAGG], std::max<size_t>(ag_off[K], 16)));
     TRY(ensure(ctx, bb[BB_TCERR], sizeof(unsigned long long)));
     CU(cudaMemsetAsync(bb[BB_TCERR].p, 0, sizeof(unsigned long long), st));
     for (int k : order) {
       if (oh_off[k + 1] == oh_off[k]) continue;
       TcArgs &T = TD[k];
       T.onehot = (const uint8_t *)bb[BB_OH].p + oh_off[k];
-      T.agg = (int32_t *)bb[BB_TCAGG].p + ag_off[k];
+      T.agg = (char *)bb[BB_TCAGG].p + ag_off[k];
+      T.agg16 = 2 * RC[k].Lc < 65536;
       T.err = (unsigned long long *)bb[BB_TCERR].p;
       const long nthr = T.NB * 32 * T.KS * (kTcStageK / 16);
       onehot_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>(PA[k].cc, T.N, RC[k].Lc, T.NB, T.KS,
@@ -3391,6 +3404,7 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
         for (long j0 = (i0 + 1) / kTcCols * kTcCols; j0 < T.N; j0 += kTcCols) tct.push_back(make_int4(k, (int)i0, (int)j0, 0));
       PD[k].tcagg = T.agg;
       PD[k].tcplane = (size_t)T.N * T.N;
+      PD[k].tc16 = T.agg16;
     }
     if (!tct.empty()) {
       TRY(ensure(ctx, bb[BB_TCDESC], K * sizeof(TcArgs)));

@@ -61,8 +61,9 @@ struct PairArgs {
   unsigned long long replay_cap;
   unsigned long long *counters;  // [0] pairs with an ambiguous log, [1] undecided pairs
   const LogTable *logt;
-  const int32_t *tcagg = nullptr;  // clean-site aggregates from the tensor-core kernel ([7][band rows][ncols])
-  size_t tcplane = 0;              // (band rows) x ncols
+  const void *tcagg = nullptr;  // clean-site aggregates from the tensor-core kernel ([7][band rows][ncols])
+  size_t tcplane = 0;           // (band rows) x ncols
+  int tc16 = 0;                 // the aggregates are uint16 (every value fits: 2 Lc < 65536), else int32
 };
 
 struct ReplayArgs {

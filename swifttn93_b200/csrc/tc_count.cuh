@@ -6,7 +6,8 @@
 // tcgen05.mma of kind::i8 (M = 128, N = 256, K = 32, u8 x u8 -> s32 in tensor memory) per 32 columns
 // accumulates D = A' B'^T, whose 4x4 blocks are the pairs' tables. The epilogue turns each table into the seven
 // clean-site aggregates the pair kernel needs (jointly clean sites, matches, A<->G and C<->T transitions, and the
-// A, C, G base counts over both sequences) and stores them as int32 [7][band rows][band columns].
+// A, C, G base counts over both sequences) and stores them as [7][band rows][band columns], uint16 when twice the
+// column count fits in 16 bits (the largest aggregate is a base count over both sequences), else int32.
 //
 // Operand image in HBM (built by onehot_kernel from the compressed codes): per 128-column stage s and 32-sequence
 // block b a 16 KB block at (s * NB + b) * 16 KB, in the canonical K-major layout without swizzle: row r =
@@ -41,7 +42,8 @@ struct TcArgs {
   long r0, r1;            // band rows
   long ncols, colbase;    // output row stride and first column it holds
   long cstart;            // first column tile (a multiple of 64 past 0)
-  int32_t *agg;           // [7][r1 - r0][ncols]
+  void *agg;              // [7][r1 - r0][ncols], uint16 when agg16 (every aggregate < 65536) else int32
+  int agg16;
   unsigned long long *err;  // set when a wait gave up
 };
 
@@ -283,9 +285,16 @@ __device__ __forceinline__ void count_tc_tile(const TcArgs &a, long i0, long j0)
       const long j = j0 + 4 * c16 + cls;
       const long lb = a.cross ? a.n1 : i + 1;
       if (i >= a.r0 && i < a.r1 && j >= lb && j < a.N) {
-        int32_t *dst = a.agg + (size_t)(i - a.r0) * a.ncols + (j - a.colbase);
+        const size_t at = (size_t)(i - a.r0) * a.ncols + (j - a.colbase);
+        if (a.agg16) {
+          uint16_t *dst = (uint16_t *)a.agg + at;
 #pragma unroll
-        for (int q = 0; q < 7; q++) dst[q * plane] = out[q];
+          for (int q = 0; q < 7; q++) dst[q * plane] = (uint16_t)out[q];
+        } else {
+          int32_t *dst = (int32_t *)a.agg + at;
+#pragma unroll
+          for (int q = 0; q < 7; q++) dst[q * plane] = out[q];
+        }
       }
     }
   }
