@@ -838,6 +838,52 @@ __device__ __forceinline__ void sum_rows(const RowArgs &a, long bx)
       w1 += (double)svs;
   }
   const double *drow = a.dist + (size_t)(i - a.r0) * a.ncols - a.colbase;
+  if (!rc.fst) {
+    // Single bin: every lane adds the chunk's 32 terms in column order (the same chain in every lane, so no lane
+    // waits for another); skipped pairs and columns past the end add +0.0, which leaves a non-negative sum
+    // unchanged. The weights are integers: their double sum is exact, in any order, while the total stays below
+    // 2^53, so they are added as integers (and re-added one by one in the rare case the total is larger).
+    unsigned long long wsum = 0;
+    for (long j0 = lb; j0 < cend; j0 += 32) {
+      const long j = j0 + lane;
+      double term = 0.;
+      if (j < cend) {
+        const double raw = drow[j];
+        if ((uint64_t)__double_as_longlong(raw) != kSkipBits) {
+          const double t = raw <= 0. ? 0. : raw;
+          const long w = cnt_i * a.counts[j];
+          term = __dmul_rn(t, (double)w);
+          wsum += (unsigned long long)w;
+        }
+      }
+#pragma unroll
+      for (int l = 0; l < 32; l++) s0 = __dadd_rn(s0, __shfl_sync(0xffffffffu, term, l));
+    }
+    for (int o = 16; o; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+    const unsigned long long svs = (!rc.cross && cnt_i > 1) ? (unsigned long long)(cnt_i * (cnt_i - 1l)) >> 1 : 0;
+    if (wsum + svs < (1ull << 53)) {
+      w0 = (double)(wsum + svs);
+    } else {
+      w0 = (double)svs;
+      for (long j0 = lb; j0 < cend; j0 += 32) {
+        const long j = j0 + lane;
+        double wl = 0.;
+        if (j < cend && (uint64_t)__double_as_longlong(drow[j]) != kSkipBits) wl = (double)(cnt_i * a.counts[j]);
+#pragma unroll
+        for (int l = 0; l < 32; l++) w0 = __dadd_rn(w0, __shfl_sync(0xffffffffu, wl, l));
+      }
+    }
+    if (lane == 0) {
+      const long r = out_row;
+      a.row_sum[r * 3] = s0;
+      a.row_sum[r * 3 + 1] = 0.;
+      a.row_sum[r * 3 + 2] = 0.;
+      a.row_w[r * 3] = w0;
+      a.row_w[r * 3 + 1] = 0.;
+      a.row_w[r * 3 + 2] = 0.;
+    }
+    return;
+  }
   for (long j0 = lb; j0 < cend; j0 += 32) {
     const long j = j0 + lane;
     bool inc = false;
