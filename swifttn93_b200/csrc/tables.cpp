@@ -141,7 +141,7 @@ AggEntry make_agg(int c1, int c2, int mode, const unsigned char *subset)
   const bool da = aggregate(S, a);
   for (int k = 0; k < 7; k++) e.v[k] = m[k];
   e.v[7] = m[7];
-  e.v[8] = (dm ? 0 : 1) | (da ? 0 : 2);
+  e.v[8] = dm ? 0 : 1;  // counts entries whose main-mode contribution is not a multiple of 1/16
   for (int k = 0; k < 7; k++) e.v[9 + k] = a[k];
   return e;
 }

@@ -15,7 +15,8 @@ constexpr int kSparseCodes = 13;  // codes 4..16
 // Lanes of an aggregate entry (x16 integers, exact while every contribution is a multiple of 1/16):
 //   0 T (total), 1 D (diagonal), 2 AG (A<->G), 3 CT (C<->T), 4 nfA, 5 nfC, 6 nfG  -- the main mode
 //   7 ambiguity count (resolved events, for the -g test)
-//   8 flags: bit 0 = a main-mode contribution is not a multiple of 1/16, bit 1 = the same in AVERAGE mode
+//   8 1 when the main-mode contribution is not a multiple of 1/16 (a pair with any such site takes the
+//     site-order replay)
 //   9..15 lanes 0..6 in AVERAGE mode (the -g fallback)
 constexpr int kLanes = 16;
 struct AggEntry {

@@ -447,7 +447,17 @@ TN_HD Dec decimal6(double d)
     e2 = be - 1075;
   }
   const bool fast = d >= 1e-5 && d < 1e5;
-  int X = (int)floor(log10(d));
+  // decimal exponent estimate: a comparison chain in the fast window (an estimate off by one near a power of ten
+  // is corrected by the loop below, which checks that the scaled value has six digits), log10 elsewhere
+  int X;
+  if (fast) {
+    const double p10[9] = {1e-4, 1e-3, 1e-2, 1e-1, 1e0, 1e1, 1e2, 1e3, 1e4};
+    X = -5;
+#pragma unroll
+    for (int k = 0; k < 9; k++) X += d >= p10[k] ? 1 : 0;
+  } else {
+    X = (int)floor(log10(d));
+  }
   uint64_t q = 0;
   int cmp = 0;
   for (int guard = 0; guard < 4; guard++) {

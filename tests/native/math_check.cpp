@@ -95,6 +95,21 @@ int main(int argc, char **argv)
       g_bad++;
     }
   }
+  // powers of ten and their neighbours a few ulps away (the decade estimate's edges)
+  for (int e = -8; e <= 8; e++) {
+    double x = pow(10.0, (double)e);
+    for (int u = 0; u < 4; u++) x = nextafter(x, 0.0);
+    for (int u = 0; u < 9; u++, x = nextafter(x, 1e300)) {
+      const int la = fmt_g(x, a);
+      a[la] = 0;
+      snprintf(b, sizeof b, "%g", x);
+      g_n++;
+      if (strcmp(a, b) || fmt_g_len(x) != la) {
+        if (g_bad < 5) fprintf(stderr, "fmt mismatch at a power of ten %a: got '%s' want '%s'\n", x, a, b);
+        g_bad++;
+      }
+    }
+  }
   // 3. the full formula over plausible count tables (x16 integer aggregates / 16)
   for (long i = 0; i < n; i++) {
     long L = 50 + (long)(rnd() % 30000);
