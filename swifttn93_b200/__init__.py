@@ -263,7 +263,16 @@ class Engine:
                 msg += ": " + (self.lib.tn93g_last_cuda_error(self.ctx) or b"").decode()
             raise Tn93Error(f"tn93g error {rc}: {msg}")
 
-    def upload(self, codes: np.ndarray, names, counts=None):
+    def upload(self, codes, names=None, counts=None):
+        """tn93g_upload: an alignment from arrays (codes uint8 [N, L], names, copy numbers), or a prepared
+        HostAlignment / Fasta, whose encoded names and offsets are then used as they are (no per-call encoding)."""
+        if isinstance(codes, (HostAlignment, Fasta)):
+            a = codes._a
+            s = C.c_void_p()
+            self._check(self.lib.tn93g_upload(self.ctx, C.byref(s), C.cast(a.codes, C.c_void_p), a.n, a.L,
+                                              C.cast(a.copy_counts, C.c_void_p), C.cast(a.names, C.c_void_p),
+                                              C.cast(a.name_off, C.c_void_p), C.cast(a.name_len, C.c_void_p)))
+            return DeviceSet(s, a.n, a.L)
         codes = np.ascontiguousarray(codes, dtype=np.uint8)
         N, L = codes.shape
         nb = [n.encode() if isinstance(n, str) else bytes(n) for n in names]

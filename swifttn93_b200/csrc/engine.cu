@@ -369,7 +369,8 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const AggEntry *sag
     }
     int cl[7];
     if (tc) {
-      const size_t at = (size_t)(i - a.r0) * a.ncols + (jj - a.colbase);
+      const long tn = a.tcncols ? a.tcncols : a.ncols, tb = a.tcncols ? a.tccolbase : a.colbase;
+      const size_t at = (size_t)(i - a.r0) * tn + (jj - tb);
       if (a.tc16) {
         const uint16_t *g = (const uint16_t *)a.tcagg + at;
 #pragma unroll
@@ -1787,7 +1788,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     CU(cudaMemsetAsync(ctx->tcerr.p, 0, sizeof(unsigned long long), st));
     const long nthr = tc_NB * 32 * tc_KS * (kTcStageK / 16);
     onehot_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>((const uint8_t *)ctx->cc.p, N, Lc, tc_NB, tc_KS,
-                                                                  (uint8_t *)ctx->ohimg.p);
+                                                                  (uint8_t *)ctx->ohimg.p, 0, tc_NB * 32);
     CU(cudaGetLastError());
     ctx->launches++;
     static bool attr = false;
@@ -1956,6 +1957,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
       T.ncols = ncols;
       T.colbase = colbase;
       T.cstart = cstart / kTcCols * kTcCols;
+      T.cend = N;
       T.agg = ctx->tcagg.p;
       T.agg16 = tc16;
       T.err = (unsigned long long *)ctx->tcerr.p;
@@ -2619,7 +2621,24 @@ struct tn93g_server {
       rqn, counters, segcols, sbytes, soff, slinks, sskip, smax, rsum, rw, hist, total, out, qout, qlinks, scantmp;
   void *pin = nullptr;
   size_t pin_n = 0;
+  // tensor-core counts: the one-hot image of the reference and the batch's queries, and the aggregates of one
+  // chunk of query columns at a time
+  bool tc = false;
+  int tc16 = 0;
+  long tc_NB = 0, tc_KS = 0;
+  DevBuf ohimg, tcagg, tcerr;
 };
+
+namespace {
+constexpr long kServerTcChunk = 1024;  // query columns per tensor-core count launch (a multiple of 64)
+
+// opt-in to the count kernel's dynamic shared memory on the current device
+int tc_attr(tn93g_ctx *ctx)
+{
+  CU(cudaFuncSetAttribute(count_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+  return TN93G_OK;
+}
+}  // namespace
 
 extern "C" {
 
@@ -2632,7 +2651,7 @@ void tn93g_server_destroy(tn93g_server *srv)
                     &srv->varcol, &srv->qcodes, &srv->counts, &srv->names, &srv->name_off, &srv->name_len,
                     &srv->dist, &srv->rq, &srv->rqn, &srv->counters, &srv->segcols, &srv->sbytes, &srv->soff,
                     &srv->slinks, &srv->sskip, &srv->smax, &srv->rsum, &srv->rw, &srv->hist, &srv->total,
-                    &srv->out, &srv->qout, &srv->qlinks, &srv->scantmp};
+                    &srv->out, &srv->qout, &srv->qlinks, &srv->scantmp, &srv->ohimg, &srv->tcagg, &srv->tcerr};
   for (DevBuf *b : bufs)
     if (b->p) {
       cudaFree(b->p);
@@ -2811,6 +2830,37 @@ int tn93g_server_create(tn93g_ctx *ctx, tn93g_server **out, const uint8_t *codes
     SVC(cudaHostAlloc(&srv->pin, text0, cudaHostAllocDefault));
     srv->pin_n = text0;
   }
+  // tensor-core counts (the context's count path): the reference's blocks of the one-hot image now, the blocks
+  // holding queries per batch; when the budget cannot hold the image and one chunk of aggregates, the server
+  // counts with POPC instead (same results)
+  if (ctx->count_path == 1) {
+    srv->tc_NB = (N + max_batch_sequences + 31) / 32 + 1;
+    srv->tc_KS = (L + kTcStageK - 1) / kTcStageK;
+    srv->tc16 = 2 * L < 65536;
+    const size_t img = (size_t)srv->tc_KS * srv->tc_NB * kTcBlockBytes;
+    const size_t agg = (size_t)7 * N * kServerTcChunk * (srv->tc16 ? 2 : 4);
+    if (ensure(ctx, srv->ohimg, img) == TN93G_OK && ensure(ctx, srv->tcagg, agg) == TN93G_OK &&
+        ensure(ctx, srv->tcerr, sizeof(unsigned long long)) == TN93G_OK) {
+      srv->tc = true;
+      SV(tc_attr(ctx));
+      const long nfull = N / 32 * 32;  // whole reference blocks (the block shared with queries is built per batch)
+      if (nfull) {
+        const long nthr = nfull * srv->tc_KS * (kTcStageK / 16);
+        onehot_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>((const uint8_t *)srv->cc.p, N, L, srv->tc_NB,
+                                                                      srv->tc_KS, (uint8_t *)srv->ohimg.p, 0, nfull);
+        SVC(cudaGetLastError());
+      }
+    } else {
+      for (DevBuf *b : {&srv->ohimg, &srv->tcagg, &srv->tcerr})
+        if (b->p) {
+          cudaFree(b->p);
+          ctx->used -= b->n;
+          b->p = nullptr;
+          b->n = 0;
+        }
+      ctx->err.clear();
+    }
+  }
   SVC(cudaStreamSynchronize(st));
 #undef SV
 #undef SVC
@@ -2944,8 +2994,52 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
   A.replay_cap = dslots;
   A.counters = (unsigned long long *)srv->counters.p;
   A.logt = ctx->d_logt;
-  CU(launch_pair(A, (Q + 31) / 32, Nref, st));
-  ctx->launches++;
+  if (srv->tc) {
+    // the image blocks from the one shared by the reference's last rows and the first queries, through one zero
+    // block past the last query; then per chunk of query columns: counts on the tensor cores, then the pair kernel
+    const long b0 = Nref / 32, b1 = (Nref + Q + 31) / 32 + 1;
+    const long nthr = (b1 - b0) * 32 * srv->tc_KS * (kTcStageK / 16);
+    CU(cudaMemsetAsync(srv->tcerr.p, 0, sizeof(unsigned long long), st));
+    onehot_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>((const uint8_t *)srv->cc.p, Nref + Q, L, srv->tc_NB,
+                                                                  srv->tc_KS, (uint8_t *)srv->ohimg.p, b0 * 32,
+                                                                  (b1 - b0) * 32);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    for (long c0 = Nref; c0 < Nref + Q; c0 += kServerTcChunk) {
+      const long c1 = std::min(Nref + Q, c0 + kServerTcChunk);
+      TcArgs T;
+      T.onehot = (const uint8_t *)srv->ohimg.p;
+      T.NB = srv->tc_NB;
+      T.KS = srv->tc_KS;
+      T.N = Nref + Q;
+      T.n1 = Nref;
+      T.cross = true;
+      T.r0 = 0;
+      T.r1 = Nref;
+      T.ncols = kServerTcChunk;
+      T.colbase = c0;
+      T.cstart = c0 / kTcCols * kTcCols;
+      T.cend = c1;
+      T.agg = srv->tcagg.p;
+      T.agg16 = srv->tc16;
+      T.err = (unsigned long long *)srv->tcerr.p;
+      const dim3 g((unsigned)((c1 - T.cstart + kTcCols - 1) / kTcCols), (unsigned)((Nref + kTcRows - 1) / kTcRows));
+      count_tc_kernel<<<g, 128, kTcSmem, st>>>(T);
+      CU(cudaGetLastError());
+      PairArgs AC = A;
+      AC.tcagg = srv->tcagg.p;
+      AC.tcplane = (size_t)Nref * kServerTcChunk;
+      AC.tc16 = srv->tc16;
+      AC.tcncols = kServerTcChunk;
+      AC.tccolbase = c0;
+      AC.cstart = c0;
+      CU(launch_pair(AC, (c1 - c0 + 31) / 32, Nref, st));
+      ctx->launches += 2;
+    }
+  } else {
+    CU(launch_pair(A, (Q + 31) / 32, Nref, st));
+    ctx->launches++;
+  }
   CU(cudaEventRecord(E[2], st));
   ReplayArgs R;
   R.rc = rc;
@@ -3062,6 +3156,14 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
   if (counters[3]) {
     ctx->err = "internal error: a query's text did not match its counted length";
     return TN93G_ECUDA;
+  }
+  if (srv->tc) {
+    unsigned long long tcerr = 0;
+    CU(cudaMemcpy(&tcerr, srv->tcerr.p, sizeof tcerr, cudaMemcpyDeviceToHost));
+    if (tcerr) {
+      ctx->err = "the tensor-core count kernel timed out waiting for its pipeline";
+      return TN93G_ETIMEOUT;
+    }
   }
   for (int q = 0; q < nq; q++) {
     tn93g_summary &S = sums[q];
@@ -3429,6 +3531,7 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
       T.ncols = N;
       T.colbase = 0;
       T.cstart = 0;
+      T.cend = N;
     }
     TRY(ensure(ctx, bb[BB_OH], std::max<size_t>(oh_off[K], 16)));
     TRY(ensure(ctx, bb[BB_TCAGG], std::max<size_t>(ag_off[K], 16)));
@@ -3443,7 +3546,7 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
       T.err = (unsigned long long *)bb[BB_TCERR].p;
       const long nthr = T.NB * 32 * T.KS * (kTcStageK / 16);
       onehot_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>(PA[k].cc, T.N, RC[k].Lc, T.NB, T.KS,
-                                                                    (uint8_t *)bb[BB_OH].p + oh_off[k]);
+                                                                    (uint8_t *)bb[BB_OH].p + oh_off[k], 0, T.NB * 32);
       CU(cudaGetLastError());
       ctx->launches++;
       for (long i0 = 0; i0 < T.N - 1; i0 += kTcRows)

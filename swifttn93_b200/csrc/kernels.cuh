@@ -64,6 +64,8 @@ struct PairArgs {
   const void *tcagg = nullptr;  // clean-site aggregates from the tensor-core kernel ([7][band rows][ncols])
   size_t tcplane = 0;           // (band rows) x ncols
   int tc16 = 0;                 // the aggregates are uint16 (every value fits: 2 Lc < 65536), else int32
+  long tcncols = 0, tccolbase = 0;  // row stride and first column of the aggregates when they hold a chunk of the
+                                    // columns (0: the same as ncols and colbase)
 };
 
 struct ReplayArgs {

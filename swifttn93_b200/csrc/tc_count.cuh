@@ -42,6 +42,7 @@ struct TcArgs {
   long r0, r1;            // band rows
   long ncols, colbase;    // output row stride and first column it holds
   long cstart;            // first column tile (a multiple of 64 past 0)
+  long cend;              // columns at or past cend are not stored (a chunk of the columns; N for all of them)
   void *agg;              // [7][r1 - r0][ncols], uint16 when agg16 (every aggregate < 65536) else int32
   int agg16;
   unsigned long long *err;  // set when a wait gave up
@@ -128,13 +129,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16])
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// one thread per (sequence, 16 columns): the four class rows' 16 bytes of the operand image
-__global__ void onehot_kernel(const uint8_t *__restrict__ cc, long N, long Lc, long NB, long KS, uint8_t *img)
+// one thread per (sequence, 16 columns): the four class rows' 16 bytes of the operand image, for the sequences
+// [seq0, seq0 + nseq) (seq0 and nseq multiples of 32; sequences at or past N get zero rows)
+__global__ void onehot_kernel(const uint8_t *__restrict__ cc, long N, long Lc, long NB, long KS, uint8_t *img,
+                              long seq0, long nseq)
 {
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const long nchunk = KS * (kTcStageK / 16);
-  if (t >= NB * 32 * nchunk) return;
-  const long seq = t / nchunk, ch = t % nchunk;
+  if (t >= nseq * nchunk) return;
+  const long seq = seq0 + t / nchunk, ch = t % nchunk;
   const long s = ch / (kTcStageK / 16), c = ch % (kTcStageK / 16);
   const long k0 = ch * 16;
   uint8_t code[16];
@@ -164,7 +167,7 @@ __device__ __forceinline__ void count_tc_tile(const TcArgs &a, long i0, long j0)
   __shared__ int abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // block-uniform exit: no valid pair in the tile
-  if (i0 >= a.r1 || j0 >= a.N) return;
+  if (i0 >= a.r1 || j0 >= a.N || j0 >= a.cend) return;
   if (!a.cross && j0 + kTcCols - 1 <= i0) return;
   if (a.cross && j0 + kTcCols <= a.n1) return;
   // 1 KB aligned stage ring
@@ -284,7 +287,7 @@ __device__ __forceinline__ void count_tc_tile(const TcArgs &a, long i0, long j0)
       }
       const long j = j0 + 4 * c16 + cls;
       const long lb = a.cross ? a.n1 : i + 1;
-      if (i >= a.r0 && i < a.r1 && j >= lb && j < a.N) {
+      if (i >= a.r0 && i < a.r1 && j >= lb && j >= a.colbase && j < a.N && j < a.cend) {
         const size_t at = (size_t)(i - a.r0) * a.ncols + (j - a.colbase);
         if (a.agg16) {
           uint16_t *dst = (uint16_t *)a.agg + at;

@@ -51,6 +51,11 @@ def _alone(eng, aln, opts):
                    aln._cnt)
     body, summ = eng.run(s, opts)
     eng.free(s)
+    # the same alignment uploaded as a prepared HostAlignment gives the same run
+    s = eng.upload(aln)
+    body2, summ2 = eng.run(s, opts)
+    eng.free(s)
+    assert body2 == body and summ2.json(aln.n) == summ.json(aln.n)
     return body, summ
 
 

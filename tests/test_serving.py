@@ -126,3 +126,31 @@ def test_service_continuous_batching_same_as_alone(oracle_bin, tmp_path):
                 assert resp.stderr == w[3], (resp.stderr, w[3])
     assert burst_batches < len(stream) - 1  # the burst's requests were batched together
     assert max(stats.batch_sequences) <= 300
+
+
+@pytest.mark.gpu
+def test_server_tensor_core_chunks_equal_popcount():
+    """A batch wider than one 1,024-column chunk of the server's tensor-core count path (and a reference whose
+    size is not a multiple of 32, so one operand block mixes reference and query rows) gives the same bytes and
+    summaries as the popcount path."""
+    import numpy as np
+
+    from swifttn93_b200 import Engine, Fasta, Options, ResidentReference, synth
+
+    rng = np.random.default_rng(8)
+    rnames, rcodes = synth.serve_reference(seed=12, n=1499, L=1500)
+    R = Fasta(synth.to_fasta(rnames, rcodes))
+    Q = []
+    for k, q in enumerate((400, 1, 350, 33, 300, 64)):
+        names, codes = synth.serve_query(rng, rcodes, q, f"c{k}")
+        Q.append(Fasta(synth.to_fasta(names, codes), expect_len=R.L))
+    opts = Options(threshold=0.015, mode="resolve", resolve_fraction=0.05, min_overlap=500, format="csvn")
+    out = {}
+    for path in ("tc", "popc"):
+        eng = Engine()
+        eng.set_count_path(path)
+        res = ResidentReference(eng, R, opts, max_batch_sequences=1300, max_batch_queries=8)
+        out[path] = [(b, s.json(R.n, q.n, second_file=True)) for (b, s), q in zip(res.batch(Q), Q)]
+        res.close()
+        eng.close()
+    assert out["tc"] == out["popc"]
