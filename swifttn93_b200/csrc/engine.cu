@@ -20,6 +20,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -1249,13 +1250,23 @@ __global__ void fill_nan_kernel(double *p, size_t n)
     p[k] = __longlong_as_double(0x7FF8000000000000ll);
 }
 
-// pair kernel launch (dynamic shared memory above the 48 KB default needs the opt-in attribute once). Two
-// register budgets are built: 2 blocks per SM (128 registers, no spills) and 3 (80 registers, some spills).
+// True the first time it is called for the current device with this flag word. Kernel attributes (the opt-in to
+// more than 48 KB of dynamic shared memory) belong to each device's context, so they are set once per device.
+bool first_on_device(std::atomic<unsigned long long> &done)
+{
+  int d = 0;
+  cudaGetDevice(&d);
+  const unsigned long long bit = 1ull << (d & 63);
+  return !(done.fetch_or(bit) & bit);
+}
+
+// pair kernel launch (dynamic shared memory above the 48 KB default needs the opt-in attribute once per device).
+// Two register budgets are built: 2 blocks per SM (128 registers, no spills) and 3 (80 registers, some spills).
 template <int MINB>
 cudaError_t launch_pair_t(const PairArgs &A, dim3 g, cudaStream_t st)
 {
-  static bool attr_done = false;
-  if (!attr_done) {
+  static std::atomic<unsigned long long> attr_done{0};
+  if (first_on_device(attr_done)) {
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(pair_kernel<false, false, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kPairSmem)) != cudaSuccess)
@@ -1266,7 +1277,6 @@ cudaError_t launch_pair_t(const PairArgs &A, dim3 g, cudaStream_t st)
     if ((e = cudaFuncSetAttribute(pair_kernel<true, true, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kPairSmem)) != cudaSuccess)
       return e;
-    attr_done = true;
   }
   if (A.rc.wplane) {
     if (A.rc.gapmm)
@@ -1791,11 +1801,9 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
                                                                   (uint8_t *)ctx->ohimg.p, 0, tc_NB * 32);
     CU(cudaGetLastError());
     ctx->launches++;
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    if (first_on_device(attr))
       CU(cudaFuncSetAttribute(count_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
-      attr = true;
-    }
   }
   CU(cudaEventRecord(E[1], st));
 
@@ -3560,11 +3568,9 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
       TRY(ensure(ctx, bb[BB_TCTILES], tct.size() * sizeof(int4)));
       CU(cudaMemcpyAsync(bb[BB_TCDESC].p, TD.data(), K * sizeof(TcArgs), cudaMemcpyHostToDevice, st));
       CU(cudaMemcpyAsync(bb[BB_TCTILES].p, tct.data(), tct.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
-      static bool attr = false;
-      if (!attr) {
+      static std::atomic<unsigned long long> attr{0};
+      if (first_on_device(attr))
         CU(cudaFuncSetAttribute(count_tc_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
-        attr = true;
-      }
       count_tc_batch_kernel<<<(unsigned)tct.size(), 128, kTcSmem, st>>>((const TcArgs *)bb[BB_TCDESC].p,
                                                                       (const int4 *)bb[BB_TCTILES].p);
       CU(cudaGetLastError());
