@@ -1349,6 +1349,7 @@ struct tn93g_ctx {
   size_t dev_out_n = 0;
   DevBuf bb[48];  // buffers of tn93g_batch_run (indexed by BatchBuf)
   int count_path = 1;  // clean-site counts: 0 popcounts on the CUDA cores, 1 tensor cores (tcgen05)
+  int sms = 148;       // streaming multiprocessors of the device (persistent and grid-stride launches)
   DevBuf ohimg, tcagg, tcerr;
 };
 
@@ -1496,6 +1497,9 @@ int tn93g_create(tn93g_ctx **out, int device, size_t hbm_budget)
     }
     if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) rc = TN93G_ECUDA;
     if (const char *e = getenv("TN93G_COUNT")) ctx->count_path = strcmp(e, "popc") == 0 ? 0 : 1;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0)
+      ctx->sms = sms;
     LogTable h;
     build_log_table(&h);
     if (cudaMalloc(&ctx->d_logt, sizeof(LogTable)) != cudaSuccess ||
@@ -1998,7 +2002,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     R.dist = A.dist;
     R.counters = (unsigned long long *)ctx->counters.p;
     R.logt = ctx->d_logt;
-    replay_kernel<<<2 * 148, 256, 0, st>>>(R);
+    replay_kernel<<<2 * ctx->sms, 256, 0, st>>>(R);
     CU(cudaGetLastError());
     ctx->launches++;
     CU(cudaEventRecord(K[2], st));
@@ -3063,7 +3067,7 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
   R.dist = A.dist;
   R.counters = A.counters;
   R.logt = ctx->d_logt;
-  replay_kernel<<<2 * 148, 256, 0, st>>>(R);
+  replay_kernel<<<2 * ctx->sms, 256, 0, st>>>(R);
   CU(cudaGetLastError());
   ctx->launches++;
   CU(cudaEventRecord(E[3], st));
@@ -3222,10 +3226,10 @@ __global__ void gather_u64_kernel(const unsigned long long *src, const long *idx
 }
 
 template <int MINB>
-cudaError_t launch_pair_batch_t(bool wplane, bool gapmm, const PairArgs *descs, const BatchTile *tiles, int ntiles,
-                                unsigned *next, cudaStream_t st)
+cudaError_t launch_pair_batch_t(int sms, bool wplane, bool gapmm, const PairArgs *descs, const BatchTile *tiles,
+                                int ntiles, unsigned *next, cudaStream_t st)
 {
-  const dim3 g(148 * MINB);
+  const dim3 g((unsigned)(sms * MINB));
   if (gapmm) {
     cudaFuncSetAttribute(pair_batch_kernel<true, true, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)kPairSmem);
@@ -3609,8 +3613,8 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
     const BatchTile *tp = (const BatchTile *)bb[BB_TILES].p + tbase;
     unsigned *nx = (unsigned *)bb[BB_NEXT].p + cls;
     const PairArgs *dp = (const PairArgs *)bb[BB_PDESC].p;
-    CU(pair_blocks == 3 ? launch_pair_batch_t<3>(cls >= 1, cls == 2, dp, tp, cls_n[cls], nx, st)
-                        : launch_pair_batch_t<2>(cls >= 1, cls == 2, dp, tp, cls_n[cls], nx, st));
+    CU(pair_blocks == 3 ? launch_pair_batch_t<3>(ctx->sms, cls >= 1, cls == 2, dp, tp, cls_n[cls], nx, st)
+                        : launch_pair_batch_t<2>(ctx->sms, cls >= 1, cls == 2, dp, tp, cls_n[cls], nx, st));
     ctx->launches++;
     tbase += cls_n[cls];
   }
@@ -3620,7 +3624,7 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
       ctx->launches++;
     }
   CU(cudaEventRecord(E[2], st));
-  replay_batch_kernel<<<2 * 148, 256, 0, st>>>((const ReplayArgs *)bb[BB_RDESC].p, K);
+  replay_batch_kernel<<<2 * ctx->sms, 256, 0, st>>>((const ReplayArgs *)bb[BB_RDESC].p, K);
   CU(cudaGetLastError());
   ctx->launches++;
   CU(cudaEventRecord(E[3], st));
