@@ -111,6 +111,7 @@ class Service:
             t.start()
         self._ready.wait()
         if self._err:
+            self.close()  # the workers that did start exit once they see the stop flag
             raise self._err
 
     # ------------------------------------------------------------------ requests
@@ -146,10 +147,13 @@ class Service:
 
     # ------------------------------------------------------------------ workers
     def _worker(self, device, share):
+        eng = None
         try:
             eng = Engine(device, hbm_budget=share)
             res = ResidentReference(eng, self.ref, self.opts, self.cap_sequences, self.cap_queries)
         except BaseException as e:  # noqa: BLE001 - reported by the constructor
+            if eng is not None:
+                eng.close()
             self._err = e
             self._ready.wait()
             return
