@@ -154,3 +154,23 @@ def test_server_tensor_core_chunks_equal_popcount():
         res.close()
         eng.close()
     assert out["tc"] == out["popc"]
+
+
+def test_service_without_a_device_fails_cleanly():
+    """With no usable CUDA device the service's constructor raises the engine's error (no CPU fallback) and leaves
+    no worker thread behind."""
+    import threading
+
+    import torch
+
+    from swifttn93_b200 import Options, Tn93Error, build, synth
+    from swifttn93_b200.serve import Service
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    build.build_lib()
+    names, codes = synth.plain_small(n=40, L=300)
+    before = threading.active_count()
+    with pytest.raises(Tn93Error):
+        Service(synth.to_fasta(names, codes), Options(threshold=0.015), workers=2)
+    assert threading.active_count() == before
