@@ -9,7 +9,7 @@
 #   swifttn93_libm  -march=x86-64-v3: no AVX-512, so every logarithm is a plain libm log() call and the
 #                   formatting/tail paths are the portable scalar ones (the parity oracle; the reference
 #                   states both builds write identical bytes).
-# An explicit ISA instead of -march=native keeps the binaries runnable on the GPU box's host CPU.
+# An explicit ISA instead of -march=native keeps the binaries runnable on other x86-64 hosts (AVX-512 for the first).
 #
 # usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
 set -euo pipefail

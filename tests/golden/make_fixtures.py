@@ -1,6 +1,6 @@
 #!/usr/bin/env python3
 """Builds the committed parity fixtures under tests/golden/ from a reference checkout (default
-/root/reference). Run once in a container that has the reference; the GPU box only reads the outputs.
+/root/reference). Run once where the reference checkout exists; the parity tests only read the outputs.
 
 Outputs:
   real_hiv_pol_dev.fa.xz, real_hiv_pol_holdout.fa.xz, real_sars2_dev.fa.xz
@@ -14,7 +14,7 @@ Outputs:
   ref_outputs.json
       sha256 of the distance file and stdout of the reference binary (oracle/_ref/swifttn93_libm, built by
       oracle/build_ref.sh) on the seeded synthetic workloads and the real sets, for the flag sets that the
-      parity tests run. Generated here because the reference does not exist on the GPU box.
+      parity tests run. Generated here because the tests run where the reference checkout may not exist.
 """
 import hashlib
 import json
