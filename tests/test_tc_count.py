@@ -75,3 +75,34 @@ def test_tc_equals_popc_two_files_bands_and_real_data():
         assert a == b, m
     eng.free(s2)
     eng.close()
+
+
+def test_tc_equals_popc_wide_alignment_int32_aggregates():
+    """More than 32,767 variable columns: the aggregates no longer fit 16 bits and are stored as int32 (single run
+    and batch)."""
+    from swifttn93_b200 import Engine, HostAlignment, Options
+
+    rng = np.random.default_rng(21)
+    n, L = 40, 33000
+    base = rng.integers(0, 4, L).astype(np.uint8)
+    codes = np.tile(base, (n, 1))
+    mut = rng.random((n, L)) < 0.02
+    codes[mut] = rng.integers(0, 4, int(mut.sum())).astype(np.uint8)
+    amb = rng.random((n, L)) < 0.003
+    codes[amb] = rng.integers(5, 11, int(amb.sum())).astype(np.uint8)
+    # every column variable, so none is folded away
+    codes[0, :] = (base + 1) % 4
+    names = [f"w{i}" for i in range(n)]
+    eng = Engine()
+    s = eng.upload(codes, names)
+    o = Options(threshold=0.05, mode="resolve", resolve_fraction=0.05, min_overlap=500)
+    a, b = _both(eng, s, o)
+    assert a == b
+    eng.free(s)
+    aln = HostAlignment(codes, names)
+    got = {}
+    for path in ("tc", "popc"):
+        eng.set_count_path(path)
+        got[path] = [(body, summ.json(n)) for body, summ in eng.batch_run([aln], [o])]
+    assert got["tc"] == got["popc"]
+    eng.close()
