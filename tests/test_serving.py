@@ -129,6 +129,23 @@ def test_service_continuous_batching_same_as_alone(oracle_bin, tmp_path):
 
 
 @pytest.mark.gpu
+def test_service_refuses_a_query_larger_than_a_batch():
+    """A query with more sequences than one batch can hold within the HBM budget is refused with status 2 and a
+    message, and the service goes on answering the others."""
+    from swifttn93_b200 import Options
+    from swifttn93_b200.serve import Service
+
+    ref, queries = _workload()
+    big = queries[-1]  # 130 sequences
+    with Service(ref, Options(threshold=0.015, mode="resolve", min_overlap=500), hbm_budget=4 << 30, workers=1,
+                 max_batch_queries=4, max_batch_sequences=100) as svc:
+        r_big = svc.submit(big).result()
+        r_small = svc.submit(queries[0]).result()
+    assert r_big.rc == 2 and b"larger than a batch" in r_big.stderr and r_big.file == b""
+    assert r_small.rc == 0 and r_small.file.startswith(b"ID1,ID2,Distance\n")
+
+
+@pytest.mark.gpu
 def test_server_tensor_core_chunks_equal_popcount():
     """A batch wider than one 1,024-column chunk of the server's tensor-core count path (and a reference whose
     size is not a multiple of 32, so one operand block mixes reference and query rows) gives the same bytes and
