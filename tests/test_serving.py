@@ -191,3 +191,68 @@ def test_service_without_a_device_fails_cleanly():
     with pytest.raises(Tn93Error):
         Service(synth.to_fasta(names, codes), Options(threshold=0.015), workers=2)
     assert threading.active_count() == before
+
+
+class _FakeSummary:
+    def __init__(self, n):
+        self.pairwise, self.skipped, self.links = n, 0, 0
+
+    def json(self, n1, n2=0, second_file=False, fst=False):
+        return f"{n1} {n2}\n".encode()
+
+
+class _FakeEngine:
+    def __init__(self, device=0, hbm_budget=0):
+        self.closed = False
+
+    def close(self):
+        self.closed = True
+
+
+class _FakeReference:
+    batches = []
+
+    def __init__(self, eng, ref, opts, cap_sequences, cap_queries):
+        self.cap = (cap_sequences, cap_queries)
+
+    def batch(self, fastas):
+        _FakeReference.batches.append([f.n for f in fastas])
+        return [(f"body{f.n}\n".encode(), _FakeSummary(f.n)) for f in fastas]
+
+    def close(self):
+        pass
+
+
+def test_service_scheduling_with_a_stand_in_engine(monkeypatch):
+    """The service's host logic on the CPU, with the engine replaced by a stand-in: responses carry each query's
+    own body and summary, batches respect the capacity, a refused FASTA gets status 1 and tn93's message, an
+    oversized query status 2, and the others are still answered."""
+    from swifttn93_b200 import Options, build, synth
+    from swifttn93_b200 import serve
+
+    build.build_lib()
+    monkeypatch.setattr(serve, "Engine", _FakeEngine)
+    monkeypatch.setattr(serve, "ResidentReference", _FakeReference)
+    _FakeReference.batches = []
+    rng = __import__("numpy").random.default_rng(3)
+    rnames, rcodes = synth.serve_reference(seed=5, n=60, L=200)
+    ref = synth.to_fasta(rnames, rcodes)
+    qs = []
+    for k, q in enumerate((3, 1, 7, 2, 9, 4)):
+        names, codes = synth.serve_query(rng, rcodes, q, f"s{k}")
+        qs.append(synth.to_fasta(names, codes))
+    with serve.Service(ref, Options(threshold=0.015), workers=2, max_batch_queries=3,
+                       max_batch_sequences=8) as svc:
+        futs = [svc.submit(q) for q in qs] + [svc.submit(b">x\nACGT\n")]
+        res = [f.result(timeout=60) for f in futs]
+    sizes = (3, 1, 7, 2, 9, 4)
+    for r, n in zip(res[:6], sizes):
+        if n > 8:
+            assert r.rc == 2 and b"larger than a batch" in r.stderr
+        else:
+            assert r.rc == 0 and r.file == b"ID1,ID2,Distance\n" + f"body{n}\n".encode()
+            assert r.stdout == f"60 {n}\n".encode() and r.pairs == 60 * n
+    assert res[-1].rc == 1 and b"same length" in res[-1].stderr
+    done = sorted(n for b in _FakeReference.batches for n in b)
+    assert done == [1, 2, 3, 4, 7]
+    assert all(len(b) <= 3 and sum(b) <= 8 for b in _FakeReference.batches)
