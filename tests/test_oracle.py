@@ -28,7 +28,7 @@ def test_oracle_vs_reference_fuzz(oracle_bin, ref_bin):
     bad = []
     with tempfile.TemporaryDirectory() as td:
         td = Path(td)
-        for k in range(250):
+        for k in range(1000):
             files, flags = cases.fuzz_case(rng)
             paths = _write(files, td)
             fl = [str(paths["in2"]) if f == "{in2}" else f for f in flags]
