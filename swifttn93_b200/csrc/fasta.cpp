@@ -31,7 +31,9 @@ struct CodeMap {
 const CodeMap kMap;
 
 struct Reader {
-  std::vector<uint8_t> codes;
+  uint8_t *codes = nullptr;  // every input byte may be a code: sized to the input, written through a pointer
+  size_t ncodes = 0;
+  ~Reader() { free(codes); }
   std::vector<char> names;
   std::vector<size_t> name_off;
   std::vector<long> name_len, counts;
@@ -54,13 +56,15 @@ extern "C" int tn93g_read_fasta(const char *bytes, size_t nbytes, long expect_le
   memset(out, 0, sizeof *out);
   std::string err;
   Reader A;
+  A.codes = (uint8_t *)malloc(nbytes + 1);
+  if (!A.codes) return TN93G_ENOMEM;
   long N = 0, first_len = expect_len > 0 ? expect_len : 0;
   const bool have_len = expect_len > 0;
   const unsigned char *p = (const unsigned char *)bytes, *end = p + nbytes;
   int state = 0;
   size_t seq_begin = 0;
   auto close_sequence = [&]() -> bool {
-    const long len = (long)(A.codes.size() - seq_begin);
+    const long len = (long)(A.ncodes - seq_begin);
     if (N == 0 && !have_len) {
       first_len = len;
       if (first_len <= 0) {
@@ -113,19 +117,21 @@ extern "C" int tn93g_read_fasta(const char *bytes, size_t nbytes, long expect_le
       A.name_off.push_back(begin);
       A.name_len.push_back(len);
       state = 2;
-      seq_begin = A.codes.size();
+      seq_begin = A.ncodes;
       continue;
     }
+    uint8_t *dst = A.codes + A.ncodes;
     while (p < end) {
       const signed char v = kMap.v[*p];
       if (v >= 0) {
-        A.codes.push_back((uint8_t)v);
+        *dst++ = (uint8_t)v;
         p++;
         continue;
       }
       if (*p == '>' || *p == '#') break;
       p++;
     }
+    A.ncodes = (size_t)(dst - A.codes);
     if (p == end) break;
     p++;
     if (!close_sequence()) {
@@ -154,7 +160,8 @@ extern "C" int tn93g_read_fasta(const char *bytes, size_t nbytes, long expect_le
   if (A.names.empty()) A.names.push_back('\0');
   out->n = N;
   out->L = first_len;
-  out->codes = dup(A.codes);
+  out->codes = A.codes;  // the input-sized buffer (its first n x L bytes are the codes)
+  A.codes = nullptr;
   out->copy_counts = dup(A.counts);
   out->names = dup(A.names);
   out->name_off = dup(A.name_off);
