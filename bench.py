@@ -45,6 +45,13 @@ FLAGS = dict(threshold=1000.0, resolve_fraction=0.05, min_overlap=500, format="c
 WORKLOAD = "hiv_bench 6700x1500, -t 1000 -g 0.05 -l 500 -f csv, -a resolve/average/gapmm (all pairs written)"
 
 
+# ncu figures of the pair stage behind the roofline line (profiles/pair_stage_hiv_bench_n4000.md): one launch
+# of count_tc_kernel and one of pair_kernel over the 7,998,000 pairs of the 4,000-sequence prefix, -a resolve
+PAIR_STAGE_PROFILE = {"file": "profiles/count_tc_kernel_hiv_bench_n4000.md", "pairs": 7998000,
+                      "dram_bytes": 104.5e6 + 167.8e6, "tensor_pipe_active": 0.294,
+                      "pair_kernel_inst_per_pair": 507.1e6 * 32 / 7998000, "pair_kernel_issue_active": 0.524}
+
+
 def peaks():
     p = REPO / "MEASURED_PEAKS.json"
     if p.exists():
@@ -151,18 +158,68 @@ def run_reference(names, codes, steps, warmup, sample_modes=MODES, tflag="1000")
         shutil.rmtree(td, ignore_errors=True)
 
 
+def cli_variant(names, codes, steps, warmup):
+    """The product's command line (swifttn93_b200/bin/tn93g) on the workload, as the reference arm runs the
+    reference binary: -q -t 1000 -a MODE -g 0.05 -l 500 -f csv -o /dev/shm/out.csv, one process per mode, wall
+    clock. Also checks that each file and stdout equal the committed reference outputs of this workload."""
+    import hashlib
+
+    from swifttn93_b200 import synth
+
+    cli = REPO / "swifttn93_b200" / "bin" / "tn93g"
+    if not cli.exists():
+        return {"unavailable": "tn93g not built"}
+    want = {}
+    ref_json = REPO / "tests" / "golden" / "ref_outputs.json"
+    if ref_json.exists():
+        want = json.loads(ref_json.read_text())
+    tmpdir = Path("/dev/shm") if Path("/dev/shm").is_dir() else Path(tempfile.gettempdir())
+    td = Path(tempfile.mkdtemp(dir=tmpdir))
+    try:
+        inp = td / "hiv_bench.fa"
+        inp.write_bytes(synth.to_fasta(names, codes))
+        n = codes.shape[0]
+        times, identical = [], True
+        for it in range(warmup + steps):
+            t0 = time.perf_counter()
+            for m in MODES:
+                out = td / "out.csv"
+                r = subprocess.run([str(cli), "-q", "-t", "1000", "-a", m, "-g", "0.05", "-l", "500", "-f", "csv",
+                                    "-o", str(out), str(inp)], stdout=subprocess.PIPE, stderr=subprocess.PIPE)
+                if r.returncode != 0:
+                    return {"error": f"tn93g exited {r.returncode}: {r.stderr[-200:]!r}"}
+                if it == 0 and f"hiv_bench_all_{m}" in want and n == 6700:
+                    w = want[f"hiv_bench_all_{m}"]
+                    identical = identical and hashlib.sha256(out.read_bytes()).hexdigest() == w["file_sha256"] and \
+                        hashlib.sha256(r.stdout).hexdigest() == w["stdout_sha256"]
+                out.unlink()
+            if it >= warmup:
+                times.append(time.perf_counter() - t0)
+        step = float(np.mean(times))
+        return {"value": len(MODES) * n * (n - 1) // 2 / step, "unit": "pairs/s", "s_per_step": step,
+                "outputs_identical_to_reference": identical if n == 6700 else None,
+                "note": "tn93g -q ... -o /dev/shm/out.csv per mode: process start, FASTA parsing, device set-up, "
+                        "run and file write inside the wall clock (the reference arm's measurement)"}
+    finally:
+        shutil.rmtree(td, ignore_errors=True)
+
+
 SERVE_FLAGS = ["-t", "0.015", "-a", "resolve", "-l", "500"]
 
 
-def serving_variant(rates=(20.0, 200.0), seconds=4.0, saturate=1200, ref_sample=8):
+def serving_variant(rates=(20.0, 200.0), seconds=4.0, saturate=1200, ref_sample=8, plain_sample=64,
+                    worker_counts=(2, 4)):
     """The served form: a resident reference of 30,000 x 1,500 (synth.serve_reference) and query FASTAs of 1-512
     sequences (geometric, mean 32), each derived from a random reference sequence at 0.5-3% divergence with 1%
     ambiguity, run as tn93 -s QUERY REF -t 0.015 -a resolve -l 500 through the continuous-batching service
-    (2 workers, 8 GB HBM budget). Poisson streams at each rate for `seconds`, then a saturating burst. Latency is
-    arrival to response (host bytes of the distance file and JSON summary); pairs/s = reference x query sequences
-    answered / (first arrival to last response). The reference binary answers a sample of the same requests one
-    by one (-s QUERY.fa REF.fa from tmpfs, all host cores) for comparison."""
-    from swifttn93_b200 import Options, synth
+    (8 GB HBM budget). Poisson streams at each rate for `seconds` (2 workers), then a saturating burst at each
+    worker count. Latency is arrival to response (host bytes of the distance file and JSON summary); pairs/s =
+    reference x query sequences answered / (first arrival to last response).
+    Beside it, on the same queries: the plain path (one tn93g_upload of reference + query and one tn93g_run per
+    query, the way a caller without the server runs -s), and the reference binary on a sample of them (one
+    process per request, REF.fa from tmpfs, all host cores), whose file and stdout bytes must equal the service's
+    responses (responses_identical)."""
+    from swifttn93_b200 import Engine, Fasta, Options, synth
     from swifttn93_b200.serve import Service, query_stream, run_load
 
     rnames, rcodes = synth.serve_reference()
@@ -172,19 +229,47 @@ def serving_variant(rates=(20.0, 200.0), seconds=4.0, saturate=1200, ref_sample=
     opts = Options(threshold=0.015, mode="resolve", min_overlap=500)
     out = {"workload": "resident reference 30000x1500 (serve_reference), queries 1-512 seqs (geometric, mean 32), "
                        "0.5-3% divergence, 1% ambiguity; tn93 -s QUERY REF -t 0.015 -a resolve -l 500",
-           "unit": "pairs/s", "hbm_budget_bytes": 8 << 30, "workers": 2}
-    with Service(ref, opts, hbm_budget=8 << 30, workers=2) as svc:
-        run_load(svc, qs[:50], 1e7, seed=1)  # warm-up: buffers reach their working sizes
-        out["batch_capacity"] = {"sequences": svc.cap_sequences, "queries": svc.cap_queries}
-        for rate, n in zip(rates, n_req):
-            r = run_load(svc, qs[:n], rate, seed=int(rate))
-            out[f"poisson_{int(rate)}rps"] = {k: r[k] for k in ("requests", "ok", "span_s", "pairs", "pairs_per_s",
-                                                               "p50_ms", "p99_ms")}
-        b0 = svc.stats.batches
-        r = run_load(svc, qs[:saturate], 1e7, seed=9)
-        out["saturated"] = {k: r[k] for k in ("requests", "ok", "span_s", "pairs", "pairs_per_s", "p50_ms", "p99_ms")}
-        out["saturated"]["batches"] = svc.stats.batches - b0
-    out["value"] = out["saturated"]["pairs_per_s"]
+           "unit": "pairs/s", "hbm_budget_bytes": 8 << 30}
+    sample_responses = None
+    for w in worker_counts:
+        with Service(ref, opts, hbm_budget=8 << 30, workers=w) as svc:
+            run_load(svc, qs[:50], 1e7, seed=1)  # warm-up: buffers reach their working sizes
+            if w == worker_counts[0]:
+                out["workers"] = w
+                out["batch_capacity"] = {"sequences": svc.cap_sequences, "queries": svc.cap_queries}
+                for rate, n in zip(rates, n_req):
+                    r = run_load(svc, qs[:n], rate, seed=int(rate))
+                    out[f"poisson_{int(rate)}rps"] = {k: r[k] for k in ("requests", "ok", "span_s", "pairs",
+                                                                       "pairs_per_s", "p50_ms", "p99_ms")}
+            b0 = svc.stats.batches
+            r = run_load(svc, qs[:saturate], 1e7, seed=9)
+            sat = {k: r[k] for k in ("requests", "ok", "span_s", "pairs", "pairs_per_s", "p50_ms", "p99_ms")}
+            sat["batches"] = svc.stats.batches - b0
+            out[f"saturated_{w}_workers"] = sat
+            if w == worker_counts[0]:
+                out["saturated"] = sat
+                sample_responses = r["responses"][:max(ref_sample, 1)]
+    out["value"] = max(out[f"saturated_{w}_workers"]["pairs_per_s"] for w in worker_counts)
+    # the plain path on the same queries: reference + query uploaded and run per request (-s orientation)
+    eng = Engine()
+    R = Fasta(ref)
+    pairs, t_plain = 0, 0.0
+    for q in qs[:plain_sample]:
+        Q = Fasta(q, expect_len=R.L)
+        codes = np.concatenate([R.codes, Q.codes])
+        names = R.names + Q.names
+        counts = np.concatenate([R.counts, Q.counts])
+        t0 = time.perf_counter()
+        s = eng.upload(codes, names, counts)
+        eng.run(s, opts, n1=R.n, sink="discard")
+        eng.free(s)
+        t_plain += time.perf_counter() - t0
+        pairs += R.n * Q.n
+    eng.close()
+    out["plain_path_value"] = pairs / t_plain
+    out["plain_path_note"] = (f"{plain_sample} of the queries, each one tn93g_upload (reference + query codes and "
+                              "names from host arrays; array assembly untimed) and one tn93g_run with n1 = 30000, "
+                              "text to the engine's pinned buffer")
     binary = reference_binary()
     if binary is not None and ref_sample:
         tmpdir = Path("/dev/shm") if Path("/dev/shm").is_dir() else Path(tempfile.gettempdir())
@@ -192,22 +277,27 @@ def serving_variant(rates=(20.0, 200.0), seconds=4.0, saturate=1200, ref_sample=
         try:
             (td / "ref.fa").write_bytes(ref)
             env = {**os.environ, "OMP_NUM_THREADS": str(os.cpu_count())}
-            lat, pairs = [], 0
-            for q in qs[:ref_sample]:
+            lat, pairs, same = [], 0, True
+            for k, q in enumerate(qs[:ref_sample]):
                 (td / "q.fa").write_bytes(q)
                 t0 = time.perf_counter()
                 r = subprocess.run([str(binary), "-q", *SERVE_FLAGS, "-s", str(td / "q.fa"), "-o", str(td / "o.csv"),
-                                    str(td / "ref.fa")], stdout=subprocess.DEVNULL, env=env)
+                                    str(td / "ref.fa")], stdout=subprocess.PIPE, env=env)
                 lat.append(time.perf_counter() - t0)
                 if r.returncode != 0:
                     lat = []
                     break
+                resp = sample_responses[k]
+                same = same and resp.rc == 0 and resp.file == (td / "o.csv").read_bytes() and resp.stdout == r.stdout
                 pairs += rcodes.shape[0] * q.count(b">")
             if lat:
                 out["reference"] = {"binary": binary.name, "cores": os.cpu_count(), "requests": len(lat),
                                     "p50_ms": float(np.percentile(lat, 50)) * 1e3,
                                     "pairs_per_s": pairs / float(np.sum(lat)),
                                     "note": "one process per request, sequentially (the reference re-reads REF.fa)"}
+                out["responses_identical"] = same
+                out["responses_identical_note"] = (f"file and stdout bytes of the first {len(lat)} requests of the "
+                                                   "saturated run against the reference binary's")
         finally:
             shutil.rmtree(td, ignore_errors=True)
     return out
@@ -397,6 +487,7 @@ def main():
     # ---- value: inputs and outputs resident in HBM
     s = eng.upload(codes, names)
     step_ms, stage_ms, launches, out_bytes = [], {}, 0, 0
+    stage_by_mode = {m: {} for m in MODES}
     clocks = Clocks(local)
     for it in range(args.warmup + args.steps):
         timed = it >= args.warmup
@@ -418,6 +509,7 @@ def main():
                 out_bytes += nb
                 for k, v in sm.timings_ms.items():
                     stage_ms[k] = stage_ms.get(k, 0.0) + v
+                    stage_by_mode[o.mode][k] = stage_by_mode[o.mode].get(k, 0.0) + v
         ev1.record(stream)
         ev1.synchronize()
         if timed:
@@ -470,33 +562,41 @@ def main():
             d2h = nbytes
     e2e = pairs_step * ws / (float(np.mean(e2e_ms)) / 1e3) if e2e_ms else None
 
-    # ---- roofline of the dominant stage
+    # ---- roofline of the dominant stage: the pair stage (count_tc_kernel + pair_kernel)
+    # Algorithmic work (the clean-site count contraction): 16 x Lc INT8 one-hot MACs per pair, 25 x Lc when the
+    # N/gap plane is active (gapmm here), 2 ops per MAC, against dense INT8 = 2 x the bf16 tensor peak. The count
+    # kernel is reported alone against the same peak on its 16 x Lc; the pair kernel (CUDA cores: sparse events,
+    # formula, certificate) is issue-bound and reported with its instructions per pair from the profile.
     P = peaks()
-    stages = {k: v for k, v in stage_ms.items() if k in ("pair", "replay", "rows", "write")}
-    dom = max(stages, key=stages.get)
-    per_launch_ms = stages[dom] / (args.steps * len(MODES))
     pairs_run = n * (n - 1) // 2
-    if dom == "pair":
-        classes = 5  # the N/gap plane is active under gapmm; use the larger unit count throughout
-        work = pairs_run * classes * classes * Lc * 2  # INT8 one-hot MAC equivalents (x2 ops)
-        achieved = work / (per_launch_ms / 1e3) / 1e12
-        # DRAM bytes of the pair stage (count_tc_kernel + pair_kernel) from the ncu capture of the 4,000-sequence
-        # prefix (profiles/count_tc_kernel_hiv_bench_n4000.md: 104.5 + 167.8 MB for 7,998,000 pairs), scaled by
-        # pairs to this launch
-        traffic = 272.3e6 * pairs_run / 7998000
-        roof = {"kernel": "count_tc_kernel + pair_kernel", "bound": "tensor", "achieved": achieved,
-                "peak": 2 * P["bf16"], "unit": "TFLOP/s", "frac": achieved / (2 * P["bf16"]), "traffic": traffic,
-                "traffic_note": "bytes per pair stage, ncu on a 4,000-sequence prefix scaled by pairs; mostly the "
-                                "14-byte clean-site aggregates written by the tensor-core kernel and read back",
-                "tensor_pipe_active": 0.295,
-                "peak_note": f"dense INT8 = 2 x {P['src']} bf16 ({P['bf16']} TF/s)",
-                "work_note": f"{classes}x{classes}xLc INT8 MACs per pair, Lc={Lc}"}
-    else:
-        bpp = {"write": out_bytes / (args.steps * len(MODES)) / pairs_run + 8, "rows": 8 + 8, "replay": 8}[dom]
-        achieved = pairs_run * bpp / (per_launch_ms / 1e3) / 1e9
-        roof = {"kernel": f"{dom}_kernel", "bound": "hbm", "achieved": achieved, "peak": P["hbm"], "unit": "GB/s",
-                "frac": achieved / P["hbm"], "traffic": None, "peak_note": f"{P['src']} HBM copy bandwidth",
-                "work_note": f"{bpp:.1f} algorithmic bytes per pair"}
+    per_mode = stage_by_mode
+    work = {m: pairs_run * (25 if m == "gapmm" else 16) * Lc * 2 for m in MODES}
+    pair_ms = {m: per_mode[m]["pair"] / args.steps for m in MODES}
+    count_ms = {m: per_mode[m].get("count", 0.0) / args.steps for m in MODES}
+    achieved = sum(work.values()) / (sum(pair_ms.values()) / 1e3) / 1e12
+    peak_tc = 2 * P["bf16"]
+    tc_work = sum(pairs_run * 16 * Lc * 2 for _ in MODES)
+    tc_ms = sum(count_ms.values())
+    # DRAM bytes of one pair-stage launch (count_tc_kernel + pair_kernel) from the ncu capture named below, scaled
+    # by pairs; algorithmic bytes: the raw distance written once (8 B per pair) and the operands read once (one-hot
+    # image 4 Lc B, bit planes 4 x 8 B per 64 columns, codes and transposed codes 2 Lc B per sequence)
+    prof_pairs, prof_bytes = PAIR_STAGE_PROFILE["pairs"], PAIR_STAGE_PROFILE["dram_bytes"]
+    traffic = prof_bytes * pairs_run / prof_pairs
+    alg_bytes = 8 * pairs_run + n * (4 * Lc + 4 * 8 * ((Lc + 63) // 64) + 2 * Lc)
+    roof = {"kernel": "pair stage: count_tc_kernel + pair_kernel", "bound": "tensor", "achieved": achieved,
+            "peak": peak_tc, "unit": "TFLOP/s", "frac": achieved / peak_tc, "traffic": traffic,
+            "traffic_over_algorithmic": traffic / alg_bytes,
+            "peak_note": f"dense INT8 ops = 2 x {P['src']} bf16 ({P['bf16']} TF/s)",
+            "work_note": f"16 x Lc INT8 MACs per pair (25 x Lc under gapmm), x2 ops; Lc = {Lc}; per 3-mode step",
+            "pair_stage_ms_per_launch": {m: pair_ms[m] for m in MODES},
+            "count_tc_kernel": {"achieved": tc_work / (tc_ms / 1e3) / 1e12 if tc_ms else None, "unit": "TFLOP/s",
+                                "frac": (tc_work / (tc_ms / 1e3) / 1e12) / peak_tc if tc_ms else None,
+                                "ms_per_launch": {m: count_ms[m] for m in MODES},
+                                "tensor_pipe_active": PAIR_STAGE_PROFILE["tensor_pipe_active"]},
+            "pair_kernel": {"ms_per_launch": {m: pair_ms[m] - count_ms[m] for m in MODES}, "bound": "issue",
+                            "instructions_per_pair": PAIR_STAGE_PROFILE["pair_kernel_inst_per_pair"],
+                            "issue_active": PAIR_STAGE_PROFILE["pair_kernel_issue_active"]},
+            "profile": PAIR_STAGE_PROFILE["file"]}
 
     line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -508,6 +608,10 @@ def main():
             "engine": {"Lc": Lc, "ambiguous_log_pairs": int(sum(x.logs_ambiguous for x in summ)),
                        "undecided": int(sum(x.undecided for x in summ)),
                        "replayed": int(sum(x.pairs_replayed for x in summ))}}
+    # the drop-in command line, timed the way the reference arm is: one process per mode on the workload's FASTA,
+    # the distance file written to tmpfs, wall clock (process start, FASTA parsing, device set-up included)
+    if rank == 0 and ws == 1 and not args.no_e2e:
+        line["variant_cli"] = cli_variant(names, codes, args.steps, max(1, args.warmup))
     # the compute-bound variant (HIV-TRACE flags: -t 0.015 -a resolve -g 0.05 -l 500): few pairs are written
     if not args.no_e2e:
         o15 = Options(mode="resolve", threshold=0.015, resolve_fraction=0.05, min_overlap=500, format="csv")
@@ -540,6 +644,7 @@ def main():
 
         o15 = Options(mode="resolve", threshold=0.015, resolve_fraction=0.05, min_overlap=500, format="csv")
         comp = engine_compute(eng, s, o15)
+        exact = engine_compute(eng, s, o15, exact=True)
         band_ms = []
 
         def timed_compute(r0, r1):
@@ -553,10 +658,10 @@ def main():
             return part
 
         try:
-            run_sharded(comp, n, n, False)  # warm-up
+            run_sharded(comp, n, n, False, exact_compute=exact)  # warm-up
             torch.distributed.barrier()
             t0 = time.perf_counter()
-            merged = run_sharded(timed_compute, n, n, False)
+            merged = run_sharded(timed_compute, n, n, False, exact_compute=exact)
             wall = time.perf_counter() - t0
             t = torch.tensor([band_ms[-1]], device=f"cuda:{local}")
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)

@@ -31,6 +31,12 @@ extern "C" {
 #define TN93G_ETOOBIG (-7)  /* alignment too long for the 32-bit x16 count lanes (L >= 2^25) */
 #define TN93G_ESCRATCH (-8) /* input beyond the fixed limits of tn93g_pair_distances_noalloc */
 #define TN93G_EFASTA (-9)   /* tn93g_read_fasta refused the file (tn93's message is returned with it) */
+#define TN93G_EUNDECIDED (-10) /* a printed distance or decision could not be made exact (see tn93g_summary) */
+
+/* Fault injection for tests of the bounded device waits (tn93g_inject_fault). */
+#define TN93G_FAULT_NONE 0
+#define TN93G_FAULT_SKIP_FILL 1 /* the first tile of the next run's tensor-core count launch never receives its
+                                   first operand stage, so its bounded wait runs out (TN93G_ETIMEOUT) */
 
 /* Ambiguity modes, numbered as tn93's RESOLVE/AVERAGE/SKIP/GAPMM/SUBSET (solver/refkernel.h:14-18). */
 #define TN93G_RESOLVE 0
@@ -75,8 +81,17 @@ typedef struct tn93g_summary {
   /* engine counters */
   long pairs_replayed;            /* pairs that took the site-order (non-dyadic) path */
   long logs_ambiguous;            /* pairs with a logarithm inside the C library's rounding band */
-  long undecided;                 /* of those, pairs whose printed bytes or decisions depend on the band */
+  long undecided;                 /* pairs whose printed bytes or decisions still depend on that rounding (0 unless
+                                     the run failed with TN93G_EUNDECIDED) */
   size_t output_bytes;
+  long logs_resolved;             /* pairs finished with the C library's own logarithms: those whose bytes or
+                                     decisions depended on its rounding, and, when the JSON numbers needed it
+                                     (sums_repass), every pair with an ambiguous logarithm */
+  int sums_repass;                /* 1 when the maximum and means came from that second, exact pass */
+  /* per histogram bin (units of a row band's partial sums): over the pairs with an ambiguous logarithm, the
+   * largest low and largest high candidate distance, the sum of (high - low) x copy weight, and their number;
+   * tn93g_summary_certified turns these into a certificate of the printed JSON numbers */
+  double amb_bounds[3][4];
 } tn93g_summary;
 
 typedef struct tn93g_ctx tn93g_ctx;
@@ -120,8 +135,9 @@ void *tn93g_stream(tn93g_ctx *ctx);
 long tn93g_last_launches(tn93g_ctx *ctx);
 
 /* Device time of the last run's stages in milliseconds (CUDA events on the engine's stream):
- * [0] pack, [1] pair kernel, [2] site-order replay, [3] row reductions, [4] output formatting,
- * [5] device->host copies, [6] whole run. Returns the number of entries written (<= n). */
+ * [0] pack, [1] pair stage, [2] site-order replay, [3] row reductions, [4] output formatting,
+ * [5] device->host copies, [6] whole run, [7] the tensor-core count kernel (part of [1]; 0 on the popcount
+ * path). Returns the number of entries written (<= n). */
 int tn93g_last_timings(tn93g_ctx *ctx, double *ms, int n);
 
 /* Selects how the pair stage counts clean-site base combinations in tn93g_run / tn93g_run_rows: 0 = AND/XOR + POPC
@@ -207,9 +223,30 @@ void tn93g_server_destroy(tn93g_server *srv);
 size_t tn93g_summary_json(const tn93g_summary *s, unsigned long n1, unsigned long n2, int second_file, int fst,
                           char *buf, size_t cap);
 
+/* 1 when every number tn93g_summary_json prints from s is the same for every way the C library's log may round
+ * the ambiguous logarithms that s->amb_bounds describes; chain = the longest chain of additions behind a sum (the
+ * longest row plus the number of rows). tn93g_run certifies its own summary (and makes a second, exact pass when
+ * this fails); callers that merge row bands (tn93g_run_rows) call it on the merged summary, whose amb_bounds
+ * combine the bands' (maximum of the largest candidates, sum of the spreads and counts). Replaces: nothing (the
+ * reference computes every logarithm with the C library). */
+int tn93g_summary_certified(const tn93g_summary *s, long chain, int fst);
+
+/* ---- exactness and failure-detection knobs (tests and diagnostics) ----
+ * tn93g_set_log_band: the rounding band (in ulps, kLogBand = 0.03 to 0.5) within which a logarithm counts as
+ * ambiguous, and the distance of its other candidate (1 ulp, or more to exaggerate it). Widening them drives pairs
+ * through the undecided path; every result stays exact. Defaults also from TN93G_LOG_BAND / TN93G_LOG_SPREAD.
+ * tn93g_set_exact_sums: when on, every pair with an ambiguous logarithm is finished with the C library's log, so
+ * the sums need no certificate (row bands whose merged summary failed tn93g_summary_certified run again so).
+ * tn93g_set_wait_limit: the limit of each bounded device wait, in seconds (default 0.2).
+ * tn93g_inject_fault: TN93G_FAULT_* for the next run only. Replaces: nothing in the reference. */
+int tn93g_set_log_band(tn93g_ctx *ctx, double band_ulps, double spread_ulps);
+int tn93g_set_exact_sums(tn93g_ctx *ctx, int on);
+int tn93g_set_wait_limit(tn93g_ctx *ctx, double seconds);
+int tn93g_inject_fault(tn93g_ctx *ctx, int fault);
+
 /* Allocation-free pair distances. This entry point has no counterpart in the reference; it exists for callers
- * that cannot allocate device memory -- code running while a CUDA graph is being captured, plugin hosts whose
- * own allocator owns the whole device, or latency-critical loops that must not enter the driver's allocator.
+ * that cannot allocate device memory: plugin hosts whose own allocator owns the whole device (a second
+ * allocator would fail or fragment it), and latency-critical loops that must not enter the driver's allocator.
  * It runs the same pack, pair and site-order replay kernels as tn93g_run on one alignment, but every
  * intermediate buffer lives in one fixed array inside this library (about 16 MB of device memory, held on
  * every GPU that loads the library until the process exits), so it calls no cudaMalloc, cudaFree or other
@@ -218,15 +255,16 @@ size_t tn93g_summary_json(const tn93g_summary *s, unsigned long n1, unsigned lon
  *   d_dist   device pointer, N x N doubles (row-major), the caller's; for every j > i, d_dist[i*N + j] receives
  *            the raw distance of pair (i, j) as tn93g_run computes it (before tn93's "<= 0 -> 0"), or the bit
  *            pattern 0x7FF4000000000BAD for a pair below the overlap (-l); other entries are not written
- *   stream   a cudaStream_t, or NULL for the default stream; the call returns after the stream is synchronised
- * The first call on a device (with that device current) looks up the array's device address and writes its
- * logarithm table; make that first call before any stream capture. All calls share the array and it keeps
- * the last call's contents (each call clears what must start at zero), so two calls whose GPU work overlaps
- * would race: the library serialises calls from one process with a lock and returns only after the stream
- * has drained; do not overlap them by other means. */
+ *   stream   a cudaStream_t, or NULL for the default stream
+ * Each call copies a few small arrays between host and device to plan its launches and synchronises the given
+ * stream before it returns. The first call on a device (with that device current) also looks up the array's
+ * device address and writes its logarithm table into it. All calls share the array and it keeps the last
+ * call's contents (each call clears what must start at zero), so two calls whose GPU work overlaps would race:
+ * the library serialises calls from one process with a lock and returns only after the stream has drained; do
+ * not overlap them by other means. */
 int tn93g_pair_distances_noalloc(const uint8_t *d_codes, long N, long L, const tn93g_opts *opts, double *d_dist,
                                  void *stream);
-/* message of the last failure of tn93g_pair_distances_noalloc */
+/* message of the last failed tn93g_pair_distances_noalloc call made by the calling thread ("" after a success) */
 const char *tn93g_noalloc_last_error(void);
 
 #ifdef __cplusplus

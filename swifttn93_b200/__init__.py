@@ -30,7 +30,14 @@ EXPORTS = ("tn93g_create", "tn93g_destroy", "tn93g_strerror", "tn93g_last_cuda_e
            "tn93g_free_set", "tn93g_run", "tn93g_run_to_device", "tn93g_stream", "tn93g_last_launches",
            "tn93g_last_timings", "tn93g_pair_distances_noalloc", "tn93g_noalloc_last_error", "tn93g_read_fasta",
            "tn93g_alignment_free", "tn93g_server_create", "tn93g_server_batch", "tn93g_server_destroy",
-           "tn93g_summary_json", "tn93g_run_rows", "tn93g_batch_run", "tn93g_set_count_path")
+           "tn93g_summary_json", "tn93g_run_rows", "tn93g_batch_run", "tn93g_set_count_path",
+           "tn93g_summary_certified", "tn93g_set_log_band", "tn93g_set_exact_sums", "tn93g_set_wait_limit",
+           "tn93g_inject_fault")
+
+# error codes of include/tn93g.h used by the binding
+EUNDECIDED = -10
+ETIMEOUT = -6
+FAULT_SKIP_FILL = 1
 
 
 class _Opts(C.Structure):
@@ -44,7 +51,8 @@ class _Summary(C.Structure):
     _fields_ = [("pairwise", C.c_ulong), ("skipped", C.c_long), ("links", C.c_long), ("max", C.c_double * 3),
                 ("mean", C.c_double * 3), ("weighted", C.c_double * 3), ("hist", (C.c_ulong * 200) * 3),
                 ("pairs_replayed", C.c_long), ("logs_ambiguous", C.c_long), ("undecided", C.c_long),
-                ("output_bytes", C.c_size_t)]
+                ("output_bytes", C.c_size_t), ("logs_resolved", C.c_long), ("sums_repass", C.c_int),
+                ("amb_bounds", (C.c_double * 4) * 3)]
 
 
 class _Alignment(C.Structure):
@@ -103,6 +111,11 @@ def load_library(path: Path | str = LIB_PATH):
     lib.tn93g_summary_json.restype = C.c_size_t
     lib.tn93g_summary_json.argtypes = [C.POINTER(_Summary), C.c_ulong, C.c_ulong, C.c_int, C.c_int, C.c_char_p,
                                        C.c_size_t]
+    lib.tn93g_summary_certified.argtypes = [C.POINTER(_Summary), C.c_long, C.c_int]
+    lib.tn93g_set_log_band.argtypes = [C.c_void_p, C.c_double, C.c_double]
+    lib.tn93g_set_exact_sums.argtypes = [C.c_void_p, C.c_int]
+    lib.tn93g_set_wait_limit.argtypes = [C.c_void_p, C.c_double]
+    lib.tn93g_inject_fault.argtypes = [C.c_void_p, C.c_int]
     _lib = lib
     return lib
 
@@ -156,6 +169,8 @@ class Summary:
     logs_ambiguous: int
     undecided: int
     output_bytes: int
+    logs_resolved: int = 0
+    sums_repass: bool = False
     timings_ms: dict = field(default_factory=dict)
     raw: object = field(default=None, repr=False)
 
@@ -249,7 +264,7 @@ class DeviceSet:
 class Engine:
     """One engine context on a CUDA device (tn93g_create)."""
 
-    STAGES = ("pack", "pair", "replay", "rows", "write", "d2h", "total")
+    STAGES = ("pack", "pair", "replay", "rows", "write", "d2h", "total", "count")
 
     def __init__(self, device: int = 0, hbm_budget: int = 0):
         self.lib = load_library()
@@ -372,14 +387,39 @@ class Engine:
             out.append((b"".join(bodies[k]), _plain_summary(S)))
         return out
 
+    def set_log_band(self, band_ulps: float, spread_ulps: float = 1.0):
+        """Widens the logarithm's ambiguity band (0.03 to 0.5 ulp) and its candidate distance (>= 1 ulp): a test knob
+        that drives pairs through the undecided path; results stay exact (tn93g_set_log_band)."""
+        self._check(self.lib.tn93g_set_log_band(self.ctx, float(band_ulps), float(spread_ulps)))
+
+    def set_exact_sums(self, on: bool):
+        """Every pair with an ambiguous logarithm finished with the C library's log (tn93g_set_exact_sums)."""
+        self._check(self.lib.tn93g_set_exact_sums(self.ctx, int(bool(on))))
+
+    def set_wait_limit(self, seconds: float):
+        """Limit of each bounded device wait (tn93g_set_wait_limit)."""
+        self._check(self.lib.tn93g_set_wait_limit(self.ctx, float(seconds)))
+
+    def inject_fault(self, fault: int):
+        """A TN93G_FAULT_* for the next run only (tn93g_inject_fault)."""
+        self._check(self.lib.tn93g_inject_fault(self.ctx, int(fault)))
+
+    def run_status(self, s: DeviceSet, opts: Options, n1: int | None = None) -> int:
+        """tn93g_run's return code (0 or a negative TN93G_E*), discarding the output: for failure-path tests."""
+        o = opts.to_c()
+        S = _Summary()
+        return self.lib.tn93g_run(self.ctx, s.handle, int(s.N if n1 is None else n1), C.byref(o), _SINK(), None,
+                                  C.byref(S))
+
     def set_count_path(self, path: str):
         """"popc" (CUDA-core bit-plane counts) or "tc" (tcgen05 INT8 tensor-core counts); results are identical."""
         self._check(self.lib.tn93g_set_count_path(self.ctx, {"popc": 0, "tc": 1}[path]))
 
     def last_timings(self) -> dict:
-        """Device milliseconds of the last call's stages (pack, pair, replay, rows, write, d2h, total)."""
-        t = (C.c_double * 7)()
-        k = self.lib.tn93g_last_timings(self.ctx, t, 7)
+        """Device milliseconds of the last call's stages (pack, pair, replay, rows, write, d2h, total, and count:
+        the tensor-core count kernel, part of pair)."""
+        t = (C.c_double * 8)()
+        k = self.lib.tn93g_last_timings(self.ctx, t, 8)
         return {self.STAGES[q]: t[q] for q in range(k)}
 
     @property
@@ -391,12 +431,12 @@ class Engine:
         return self.lib.tn93g_last_launches(self.ctx)
 
     def _summary(self, S):
-        t = (C.c_double * 7)()
-        k = self.lib.tn93g_last_timings(self.ctx, t, 7)
+        t = (C.c_double * 8)()
+        k = self.lib.tn93g_last_timings(self.ctx, t, 8)
         summ = Summary(pairwise=S.pairwise, skipped=S.skipped, links=S.links, max=list(S.max), mean=list(S.mean),
                        weighted=list(S.weighted), hist=_hist(S),
                        pairs_replayed=S.pairs_replayed, logs_ambiguous=S.logs_ambiguous, undecided=S.undecided,
-                       output_bytes=S.output_bytes,
+                       output_bytes=S.output_bytes, logs_resolved=S.logs_resolved, sums_repass=bool(S.sums_repass),
                        timings_ms={self.STAGES[q]: t[q] for q in range(k)}, raw=S)
         return summ
 
@@ -420,7 +460,7 @@ def _plain_summary(S) -> Summary:
     return Summary(pairwise=S.pairwise, skipped=S.skipped, links=S.links, max=list(S.max), mean=list(S.mean),
                    weighted=list(S.weighted), hist=_hist(S),
                    pairs_replayed=S.pairs_replayed, logs_ambiguous=S.logs_ambiguous, undecided=S.undecided,
-                   output_bytes=S.output_bytes, raw=S)
+                   output_bytes=S.output_bytes, logs_resolved=S.logs_resolved, sums_repass=bool(S.sums_repass), raw=S)
 
 
 class ResidentReference:

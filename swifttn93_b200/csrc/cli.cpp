@@ -304,12 +304,15 @@ int main(int argc, char **argv)
   tn93g_summary S;
   rc = tn93g_run(ctx, set, (long)n1, &op, write_sink, o.out, &S);
   if (rc != TN93G_OK) {
+    // a run that could not make every printed byte exact fails loudly (exit 3), like any engine error (exit 2)
     std::cerr << "tn93g: " << tn93g_strerror(rc) << " " << tn93g_last_cuda_error(ctx) << std::endl;
-    return 2;
+    return rc == TN93G_EUNDECIDED ? 3 : 2;
   }
   if (getenv("TN93G_STATS"))
-    fprintf(stderr, "tn93g: replayed %ld, ambiguous-log pairs %ld, undecided %ld\n", S.pairs_replayed,
-            S.logs_ambiguous, S.undecided);
+    fprintf(stderr,
+            "tn93g: replayed %ld, ambiguous-log pairs %ld, finished with the C library's log %ld, undecided %ld, "
+            "exact-sums pass %d\n",
+            S.pairs_replayed, S.logs_ambiguous, S.logs_resolved, S.undecided, S.sums_repass);
   tn93g_free_set(ctx, set);
   tn93g_destroy(ctx);
   fflush(o.out);

@@ -19,10 +19,13 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <math.h>
+
 #include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kernels.cuh"
@@ -180,13 +183,92 @@ __device__ bool certified(const Dist &D, const RunConsts &rc)
   return true;
 }
 
-// formula + certificate for exact formula inputs; returns the raw distance
-__device__ double finish_distance(const LogTable &T, const RunConsts &rc, const double nf[4], double diag, double ag,
-                                  double ct, bool &amb, bool &undecided)
+// Per-lane running totals of the ambiguous pairs' effect on one summary unit (ExactSink::amb): flushed with
+// atomics when the unit changes, and warp by warp at the end of a tile.
+struct AmbLane {
+  int unit;  // -1: empty
+  int n;     // ambiguous pairs
+  double lo, hi, spread;
+};
+
+__device__ __forceinline__ void amb_flush(unsigned long long *acc, int unit, int n, double lo, double hi,
+                                          double spread)
 {
-  const Dist D = tn93_distance(T, nf, diag, ag, ct);
-  amb = D.amb != 0;
-  undecided = amb && !certified(D, rc);
+  unsigned long long *w = acc + 4 * unit;
+  atomicMax(&w[0], (unsigned long long)__double_as_longlong(lo));
+  atomicMax(&w[1], (unsigned long long)__double_as_longlong(hi));
+  atomicAdd(reinterpret_cast<double *>(&w[2]), spread);
+  atomicAdd(&w[3], (unsigned long long)n);
+}
+
+__device__ __forceinline__ void amb_add(unsigned long long *acc, AmbLane &L, int unit, double lo, double hi, double w)
+{
+  if (L.unit != unit) {
+    if (L.unit >= 0) amb_flush(acc, L.unit, L.n, L.lo, L.hi, L.spread);
+    L.unit = unit;
+    L.n = 0;
+    L.lo = L.hi = L.spread = 0.;
+  }
+  L.n++;
+  L.lo = fmax(L.lo, lo);
+  L.hi = fmax(L.hi, hi);
+  L.spread += (hi - lo) * w;
+}
+
+// all 32 lanes: each unit held by some lane is reduced over the warp and added once
+__device__ __forceinline__ void amb_warp_flush(unsigned long long *acc, AmbLane &L)
+{
+  for (;;) {
+    const unsigned act = __ballot_sync(0xffffffffu, L.unit >= 0);
+    if (!act) break;
+    const int u = __shfl_sync(0xffffffffu, L.unit, __ffs(act) - 1);
+    const bool me = L.unit == u;
+    double lo = me ? L.lo : 0., hi = me ? L.hi : 0., sp = me ? L.spread : 0.;
+    int n = me ? L.n : 0;
+    for (int o = 16; o; o >>= 1) {
+      lo = fmax(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+      sp += __shfl_xor_sync(0xffffffffu, sp, o);
+      n += __shfl_xor_sync(0xffffffffu, n, o);
+    }
+    if ((threadIdx.x & 31) == 0) amb_flush(acc, u, n, lo, hi, sp);
+    if (me) L.unit = -1;
+  }
+}
+
+// histogram bin of pair (i, j) under -m (0 within the first file, 1 within the second, 2 between them)
+__device__ __forceinline__ int fst_bin(const RunConsts &rc, long i, long j)
+{
+  return rc.fst ? (i < rc.n1 ? (j >= rc.n1 ? 2 : 0) : 1) : 0;
+}
+
+// The formula and its certificate for exact inputs; returns the raw distance (from the correctly rounded
+// logarithms). A pair whose printed bytes or decisions depend on the C library's rounding (or, in resolve-all
+// mode, any pair with an ambiguous logarithm) is appended to the undecided list, to be finished with the C
+// library's own logarithms; every pair with an ambiguous logarithm widens its summary unit's bounds.
+__device__ double finish_exact(const LogTable &T, const RunConsts &rc, const ExactSink &ex, const double nf[4],
+                               double diag, double ag, double ct, long i, long j, long colbase, int &namb, int &nund,
+                               AmbLane &al)
+{
+  const Dist D = tn93_distance(T, nf, diag, ag, ct, rc.log_band, rc.log_spread);
+  if (D.amb) {
+    namb++;
+    if (rc.resolve_all || !certified(D, rc)) {
+      nund++;
+      if (ex.und_list) {
+        const unsigned idx = atomicAdd(ex.und_n, 1u);
+        if (idx < ex.und_cap) {
+          ex.und_list[2 * (size_t)idx] = (unsigned long long)ex.und_k;
+          ex.und_list[2 * (size_t)idx + 1] = ((unsigned long long)i << 32) | (unsigned long long)j;
+        }
+      }
+    }
+    if (ex.amb) {
+      const int unit = ex.colunit ? ex.colunit[j - colbase] : fst_bin(rc, i, j);
+      const double w = (double)(ex.counts[i] * ex.counts[j]);
+      amb_add(ex.amb, al, unit, D.lo <= 0. ? 0. : D.lo, D.hi <= 0. ? 0. : D.hi, w);
+    }
+  }
   return D.d;
 }
 
@@ -218,7 +300,33 @@ constexpr int kTile = 32;
 constexpr int kRowsPerWarp = kTile / kWarps;
 constexpr int kColAccStride = kTile * 9 + 1;  // ints per tile row (+1: conflict-free in both phases)
 constexpr int kAggInts = (kSparseCodes * kCodes + 5) * kLanes;
-constexpr size_t kPairSmem = (size_t)kAggInts * 4 + (size_t)kTile * kColAccStride * 4;
+// shared-memory tables of a pair block: the x16 table (unpacked runs), or the packed table and the N-plane entries
+constexpr size_t kPackedSmem = sizeof(PackedTables) + 5 * sizeof(AggEntry);
+constexpr size_t kTabSmem = ((size_t)kAggInts * 4 > kPackedSmem ? (size_t)kAggInts * 4 : kPackedSmem + 15) / 16 * 16;
+constexpr size_t kPairSmem = kTabSmem + (size_t)kTile * kColAccStride * 4;
+
+// copies the run's tables into the block's shared memory (all threads; the caller synchronises)
+__device__ __forceinline__ void load_pair_tables(const PairTables *g, unsigned char *smem, bool packed)
+{
+  if (packed) {
+    const int n0 = (int)(sizeof(PackedTables) / 16), n1 = (int)(5 * sizeof(AggEntry) / 16);
+    const uint4 *src = reinterpret_cast<const uint4 *>(&g->packed);
+    const uint4 *src2 = reinterpret_cast<const uint4 *>(&g->agg[kEvEntries]);
+    uint4 *dst = reinterpret_cast<uint4 *>(smem);
+    for (int t = threadIdx.x; t < n0 + n1; t += blockDim.x) dst[t] = t < n0 ? src[t] : src2[t - n0];
+  } else {
+    const uint4 *src = reinterpret_cast<const uint4 *>(g->agg);
+    uint4 *dst = reinterpret_cast<uint4 *>(smem);
+    for (int t = threadIdx.x; t < kAggInts / 4; t += blockDim.x) dst[t] = src[t];
+  }
+}
+
+// the N-plane entries (ew[4], eww) in the block's tables
+__device__ __forceinline__ const AggEntry *ew_entries(const unsigned char *smem, bool packed)
+{
+  return packed ? reinterpret_cast<const AggEntry *>(smem + sizeof(PackedTables))
+                : reinterpret_cast<const AggEntry *>(smem) + kEvEntries;
+}
 
 struct Counts {
   int T, MM, TS, CT, Y1, Y2, L1, L2, T1, T2;
@@ -229,8 +337,8 @@ struct Counts {
 template <bool WPLANE>
 // cl: the clean-site aggregates of the pair (jointly clean sites, matches, A<->G and C<->T transitions, A, C and G
 // base counts over both sequences), from the popcount loop or the tensor-core count kernel; c: N-plane counts
-__device__ __forceinline__ void pair_epilogue(const PairArgs &a, const AggEntry *sagg, const Counts &c, const int cl[7],
-                                              const int acc[9], long i, long j, int &namb, int &nund)
+__device__ __forceinline__ void pair_epilogue(const PairArgs &a, const AggEntry *EW, const Counts &c, const int cl[7],
+                                              const int acc[9], long i, long j, int &namb, int &nund, AmbLane &al)
 {
   const RunConsts &rc = a.rc;
   const int base[7] = {16 * (cl[0] + (int)rc.constT), 16 * (cl[1] + (int)rc.constT), 16 * cl[2], 16 * cl[3],
@@ -244,7 +352,6 @@ __device__ __forceinline__ void pair_epilogue(const PairArgs &a, const AggEntry 
     wb[0] = c.nWc - wb[1] - wb[2] - wb[3];
     nww = c.nWW - c.nGG;
   }
-  const AggEntry *EW = &sagg[kSparseCodes * kCodes];
   int ag[7];
 #pragma unroll
   for (int q = 0; q < 7; q++) {
@@ -270,10 +377,8 @@ __device__ __forceinline__ void pair_epilogue(const PairArgs &a, const AggEntry 
     } else {
       const double nf[4] = {(double)ag[4] / 16.0, (double)ag[5] / 16.0, (double)ag[6] / 16.0,
                             (double)(2 * ag[0] - ag[4] - ag[5] - ag[6]) / 16.0};
-      bool qa, qu;
-      *slot = finish_distance(*a.logt, rc, nf, (double)ag[1] / 16.0, (double)ag[2] / 16.0, (double)ag[3] / 16.0, qa, qu);
-      namb += qa;
-      nund += qu;
+      *slot = finish_exact(*a.logt, rc, a.ex, nf, (double)ag[1] / 16.0, (double)ag[2] / 16.0, (double)ag[3] / 16.0, i,
+                           j, a.colbase, namb, nund, al);
     }
   }
   if (to_replay) {
@@ -282,37 +387,74 @@ __device__ __forceinline__ void pair_epilogue(const PairArgs &a, const AggEntry 
   }
 }
 
+// packed event sums (PackedTables) of one lane: four words of 16-bit lanes and the non-dyadic flag
+struct PackedAcc {
+  uint32_t w0, w1, w2, w3, f;
+};
+
+__device__ __forceinline__ void add_packed(PackedAcc &p, const uint32_t (*tab)[4], const uint32_t *flags, int k)
+{
+  const uint4 t = *reinterpret_cast<const uint4 *>(tab[k]);
+  p.w0 += t.x;
+  p.w1 += t.y;
+  p.w2 += t.z;
+  p.w3 += t.w;
+  p.f |= flags[k];
+}
+
 // One tile of pairs: rows [i0, i0 + 8 * rpw) (rpw = rows per warp, 1..4) x columns [j0, j0 + 32). The block's
-// agg table must be in sagg. All threads of the block call it with the same arguments.
+// tables must be in smem (load_pair_tables). All threads of the block call it with the same arguments.
 template <bool WPLANE, bool GAPMM>
-__device__ __forceinline__ void pair_tile(const PairArgs &a, const AggEntry *sagg, int *colacc, long i0, long j0,
+__device__ __forceinline__ void pair_tile(const PairArgs &a, const unsigned char *smem, int *colacc, long i0, long j0,
                                           int rpw)
 {
   const RunConsts &rc = a.rc;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int trows = kWarps * rpw;
+  const bool packed = rc.packed;
+  const AggEntry *sagg = reinterpret_cast<const AggEntry *>(smem);
+  const PackedTables &PT = *reinterpret_cast<const PackedTables *>(smem);
+  const AggEntry *EW = ew_entries(smem, packed);
   // block-uniform exits: no valid pair in the tile
   if (i0 >= a.r1 || j0 >= rc.N) return;
   if (!rc.cross && j0 + kTile - 1 <= i0) return;
   const long Np = rc.Npad;
   // ---- column-side sparse events: lane = tile row, warp-uniform column; skipped where the row is sparse too
+  // (packed: the column-side table holds zeros there)
   if (lane < trows) {
     const long ib = min(i0 + lane, rc.N - 1);
     for (int cl = warp; cl < kTile; cl += kWarps) {
       const long j = j0 + cl;
-      int acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-      if (j < rc.N) {
-        const uint32_t f0 = a.ev_off[j], f1 = a.ev_off[j + 1];
-        for (uint32_t e = f0; e < f1; e++) {
-          const uint32_t v = __ldg(a.ev + e);
-          const int pc = a.ccT[(size_t)(v >> 5) * Np + ib];
-          if (sparse_code(pc, WPLANE)) continue;
-          add_entry(acc, sagg[((v & 31) - 4) * kCodes + pc].v);
-        }
-      }
       int *dst = colacc + lane * kColAccStride + cl * 9;
+      if (packed) {
+        PackedAcc p = {0u, 0u, 0u, 0u, 0u};
+        if (j < rc.N) {
+          const uint32_t f0 = a.ev_off[j], f1 = a.ev_off[j + 1];
+          for (uint32_t e = f0; e < f1; e++) {
+            const uint32_t v = __ldg(a.ev + e);
+            const int pc = a.ccT[(size_t)(v >> 5) * Np + ib];
+            add_packed(p, PT.col, PT.colf, ((v & 31) - 4) * kCodes + pc);
+          }
+        }
+        dst[0] = (int)p.w0;
+        dst[1] = (int)p.w1;
+        dst[2] = (int)p.w2;
+        dst[3] = (int)p.w3;
+        dst[4] = (int)p.f;
+      } else {
+        int acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (j < rc.N) {
+          const uint32_t f0 = a.ev_off[j], f1 = a.ev_off[j + 1];
+          for (uint32_t e = f0; e < f1; e++) {
+            const uint32_t v = __ldg(a.ev + e);
+            const int pc = a.ccT[(size_t)(v >> 5) * Np + ib];
+            if (sparse_code(pc, WPLANE)) continue;
+            add_entry(acc, sagg[((v & 31) - 4) * kCodes + pc].v);
+          }
+        }
 #pragma unroll
-      for (int q = 0; q < 9; q++) dst[q] = acc[q];
+        for (int q = 0; q < 9; q++) dst[q] = acc[q];
+      }
     }
   }
   __syncthreads();
@@ -321,6 +463,8 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const AggEntry *sag
   const long j = j0 + lane;
   const long jj = j < rc.N ? j : rc.N - 1;
   int namb = 0, nund = 0;
+  AmbLane al;
+  al.unit = -1;
 #pragma unroll 1
   for (int r = 0; r < rpw; r++) {
     const long i = i0 + warp + kWarps * r;
@@ -360,26 +504,56 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const AggEntry *sag
     }
     int acc[9];
     const int *src = colacc + (int)(i - i0) * kColAccStride + lane * 9;
-#pragma unroll
-    for (int q = 0; q < 9; q++) acc[q] = src[q];
     const uint32_t e0 = a.ev_off[i], e1 = a.ev_off[i + 1];
-    for (uint32_t e = e0; e < e1; e++) {
-      const uint32_t v = __ldg(a.ev + e);
-      const int pc = a.ccT[(size_t)(v >> 5) * Np + jj];
-      add_entry(acc, sagg[((v & 31) - 4) * kCodes + pc].v);
+    if (packed) {
+      PackedAcc p = {(uint32_t)src[0], (uint32_t)src[1], (uint32_t)src[2], (uint32_t)src[3], (uint32_t)src[4]};
+      for (uint32_t e = e0; e < e1; e++) {
+        const uint32_t v = __ldg(a.ev + e);
+        const int pc = a.ccT[(size_t)(v >> 5) * Np + jj];
+        add_packed(p, PT.row, PT.rowf, ((v & 31) - 4) * kCodes + pc);
+      }
+      acc[0] = (int)(p.w0 & 0xFFFFu);
+      acc[1] = (int)(p.w0 >> 16);
+      acc[2] = (int)(p.w1 & 0xFFFFu);
+      acc[3] = (int)(p.w1 >> 16);
+      acc[4] = (int)(p.w2 & 0xFFFFu);
+      acc[5] = (int)(p.w2 >> 16);
+      acc[6] = (int)(p.w3 & 0xFFFFu);
+      acc[7] = (int)(p.w3 >> 16);
+      acc[8] = (int)p.f;
+    } else {
+#pragma unroll
+      for (int q = 0; q < 9; q++) acc[q] = src[q];
+      for (uint32_t e = e0; e < e1; e++) {
+        const uint32_t v = __ldg(a.ev + e);
+        const int pc = a.ccT[(size_t)(v >> 5) * Np + jj];
+        add_entry(acc, sagg[((v & 31) - 4) * kCodes + pc].v);
+      }
     }
     int cl[7];
     if (tc) {
+      // the pair's record from the tensor-core kernel (8 lanes, 7 used)
       const long tn = a.tcncols ? a.tcncols : a.ncols, tb = a.tcncols ? a.tccolbase : a.colbase;
       const size_t at = (size_t)(i - a.r0) * tn + (jj - tb);
       if (a.tc16) {
-        const uint16_t *g = (const uint16_t *)a.tcagg + at;
-#pragma unroll
-        for (int q = 0; q < 7; q++) cl[q] = valid ? (int)g[q * a.tcplane] : 0;
+        const uint4 g = valid ? __ldg(reinterpret_cast<const uint4 *>(a.tcagg) + at) : make_uint4(0, 0, 0, 0);
+        cl[0] = (int)(g.x & 0xFFFFu);
+        cl[1] = (int)(g.x >> 16);
+        cl[2] = (int)(g.y & 0xFFFFu);
+        cl[3] = (int)(g.y >> 16);
+        cl[4] = (int)(g.z & 0xFFFFu);
+        cl[5] = (int)(g.z >> 16);
+        cl[6] = (int)(g.w & 0xFFFFu);
       } else {
-        const int32_t *g = (const int32_t *)a.tcagg + at;
-#pragma unroll
-        for (int q = 0; q < 7; q++) cl[q] = valid ? g[q * a.tcplane] : 0;
+        const uint4 *g = reinterpret_cast<const uint4 *>(a.tcagg) + 2 * at;
+        const uint4 g0 = valid ? __ldg(g) : make_uint4(0, 0, 0, 0), g1 = valid ? __ldg(g + 1) : make_uint4(0, 0, 0, 0);
+        cl[0] = (int)g0.x;
+        cl[1] = (int)g0.y;
+        cl[2] = (int)g0.z;
+        cl[3] = (int)g0.w;
+        cl[4] = (int)g1.x;
+        cl[5] = (int)g1.y;
+        cl[6] = (int)g1.z;
       }
     } else {
       const int nfT = c.T1 + c.T2, nfC = c.Y1 + c.Y2 - nfT, nfG = c.L1 + c.L2 - nfT;
@@ -391,23 +565,23 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const AggEntry *sag
       cl[5] = nfC;
       cl[6] = nfG;
     }
-    if (valid) pair_epilogue<WPLANE>(a, sagg, c, cl, acc, i, j, namb, nund);
+    if (valid) pair_epilogue<WPLANE>(a, EW, c, cl, acc, i, j, namb, nund, al);
   }
   count_flags(a.counters, namb, nund);
+  if (a.ex.amb) amb_warp_flush(a.ex.amb, al);
 }
 
 template <bool WPLANE, bool GAPMM, int MINB>
 __global__ void __launch_bounds__(256, MINB) pair_kernel(PairArgs a)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  AggEntry *sagg = reinterpret_cast<AggEntry *>(smem_raw);
-  int *colacc = reinterpret_cast<int *>(smem_raw + (size_t)kAggInts * 4);
+  int *colacc = reinterpret_cast<int *>(smem_raw + kTabSmem);
   const long i0 = a.r0 + blockIdx.y * (long)kTile;
   const long j0 = a.cstart + blockIdx.x * (long)kTile;
   if (i0 >= a.r1 || j0 >= a.rc.N || (!a.rc.cross && j0 + kTile - 1 <= i0)) return;
-  for (int t = threadIdx.x; t < kAggInts; t += blockDim.x) ((int32_t *)sagg)[t] = ((const int32_t *)a.agg)[t];
+  load_pair_tables(a.tab, smem_raw, a.rc.packed);
   __syncthreads();
-  pair_tile<WPLANE, GAPMM>(a, sagg, colacc, i0, j0, kRowsPerWarp);
+  pair_tile<WPLANE, GAPMM>(a, smem_raw, colacc, i0, j0, kRowsPerWarp);
 }
 
 static_assert(sizeof(PairArgs) % 4 == 0, "PairArgs is copied as 32-bit words");
@@ -426,8 +600,7 @@ __global__ void __launch_bounds__(256, MINB)
     pair_batch_kernel(const PairArgs *descs, const BatchTile *tiles, int ntiles, unsigned *next)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  AggEntry *sagg = reinterpret_cast<AggEntry *>(smem_raw);
-  int *colacc = reinterpret_cast<int *>(smem_raw + (size_t)kAggInts * 4);
+  int *colacc = reinterpret_cast<int *>(smem_raw + kTabSmem);
   __shared__ __align__(16) unsigned char sd_raw[sizeof(PairArgs)];
   const PairArgs &sd = *reinterpret_cast<const PairArgs *>(sd_raw);
   __shared__ int s_t;
@@ -442,11 +615,11 @@ __global__ void __launch_bounds__(256, MINB)
       for (int q = threadIdx.x; q < (int)(sizeof(PairArgs) / 4); q += blockDim.x)
         reinterpret_cast<int32_t *>(sd_raw)[q] = reinterpret_cast<const int32_t *>(&descs[T.k])[q];
       __syncthreads();
-      for (int q = threadIdx.x; q < kAggInts; q += blockDim.x) ((int32_t *)sagg)[q] = ((const int32_t *)sd.agg)[q];
+      load_pair_tables(sd.tab, smem_raw, sd.rc.packed);
       cur = T.k;
     }
     __syncthreads();
-    pair_tile<WPLANE, GAPMM>(sd, sagg, colacc, T.i0, T.j0, T.rpw);
+    pair_tile<WPLANE, GAPMM>(sd, smem_raw, colacc, T.i0, T.j0, T.rpw);
     __syncthreads();
   }
 }
@@ -468,116 +641,188 @@ __device__ __forceinline__ int nth_bit32(unsigned x, int n)
   return pos;
 }
 
-// tn93's own per-pair computation for the order-dependent pairs (refkernel.cpp:622-750), one warp per pair:
+// tn93's own per-pair computation (refkernel.cpp:622-750) for one pair, by one warp:
 //   * clean/clean cells: the 4x4 table from the bit planes (lanes over 64-column words);
 //   * every other site in site order: per word, the lanes fetch the codes of the word's non-clean sites (in
 //     order) and lane q adds the site's contribution to float cell q, so each cell is summed in site order as
 //     tn93 does; lanes 16..19 add the integer diagonal resolutions, lane 20 the ambiguity count;
-//   * lane 0: tn93's c1-major merge of float and integer cells, the -l / -g tests and the formula.
+//   * lane 0: tn93's c1-major merge of float and integer cells and the -l / -g tests, leaving the formula's exact
+//     inputs. t = 1 starts in AVERAGE mode (a pair the -g test already sent there).
+// All lanes call it; the result is valid in lane 0.
+struct WalkOut {
+  bool skip;  // below the overlap (-l)
+  double nf[4], diag, ag, ct;
+};
+
+__device__ WalkOut walk_pair(const ReplayArgs &a, long i, long j, int t, unsigned char *sc1, unsigned char *sc2)
+{
+  const int lane = threadIdx.x & 31;
+  const RunConsts &rc = a.rc;
+  const long Np = rc.Npad;
+  const uint64_t last_valid = (rc.Lc & 63) ? ((1ull << (rc.Lc & 63)) - 1ull) : ~0ull;
+  const uint8_t *s1 = a.cc + (size_t)i * rc.Lc, *s2 = a.cc + (size_t)j * rc.Lc;
+  // clean/clean 4x4 counts (the same in every mode)
+  int cnt[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) cnt[q] = 0;
+  for (long w = lane; w < rc.W; w += 32) {
+    const uint64_t *P = a.planes + (size_t)w * rc.NP * Np;
+    const uint64_t hi = P[i], lo = P[Np + i], ci = P[2 * Np + i];
+    const uint64_t hj = P[j], lj = P[Np + j], cj = P[2 * Np + j];
+    const uint64_t xi[4] = {ci & ~hi & ~lo, ci & hi & ~lo, ci & ~hi & lo, ci & hi & lo};
+    const uint64_t xj[4] = {cj & ~hj & ~lj, cj & hj & ~lj, cj & ~hj & lj, cj & hj & lj};
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+#pragma unroll
+      for (int y = 0; y < 4; y++) cnt[x * 4 + y] += popc(xi[x] & xj[y]);
+  }
+#pragma unroll
+  for (int q = 0; q < 16; q++)
+    for (int o = 16; o; o >>= 1) cnt[q] += __shfl_xor_sync(0xffffffffu, cnt[q], o);
+  WalkOut R;
+  R.skip = false;
+  R.diag = R.ag = R.ct = 0.;
+  R.nf[0] = R.nf[1] = R.nf[2] = R.nf[3] = 0.;
+  for (;;) {
+    const SiteEntry *S = a.site + t * kCodes * kCodes;
+    double acc = 0.;  // lane q < 16: float cell q
+    long iacc = 0;    // lanes 16..19: diagonal resolutions, lane 20: ambiguity count
+    for (long w = 0; w < rc.W; w++) {
+      const uint64_t *P = a.planes + (size_t)w * rc.NP * Np;
+      uint64_t E = ~(P[2 * Np + i] & P[2 * Np + j]);
+      if (w == rc.W - 1) E &= last_valid;
+      if (!E) continue;
+      const int ne = __popcll(E), nlo = __popc((unsigned)E);
+      for (int rk = lane; rk < ne; rk += 32) {
+        const int bit = rk < nlo ? nth_bit32((unsigned)E, rk) : 32 + nth_bit32((unsigned)(E >> 32), rk - nlo);
+        const long k = w * 64 + bit;
+        sc1[rk] = s1[k];
+        sc2[rk] = s2[k];
+      }
+      __syncwarp();
+      if (lane < 16) {
+        for (int l = 0; l < ne; l++) {
+          const double v = S[sc1[l] * kCodes + sc2[l]].fc[lane];
+          if (v != 0.) acc = __dadd_rn(acc, v);
+        }
+      } else if (lane < 20) {
+        for (int l = 0; l < ne; l++) iacc += S[sc1[l] * kCodes + sc2[l]].icd[lane - 16];
+      } else if (lane == 20) {
+        for (int l = 0; l < ne; l++) iacc += S[sc1[l] * kCodes + sc2[l]].amb;
+      }
+      __syncwarp();
+    }
+    // lane 0: gather the cells, then tn93's merge and decisions
+    double fc[16];
+    long icd[4];
+#pragma unroll
+    for (int q = 0; q < 16; q++) fc[q] = __shfl_sync(0xffffffffu, acc, q);
+#pragma unroll
+    for (int q = 0; q < 4; q++) icd[q] = __shfl_sync(0xffffffffu, iacc, 16 + q);
+    const long amb = __shfl_sync(0xffffffffu, iacc, 20);
+    int next = 0;  // 0 done, 1 recompute with -a average
+    if (lane == 0) {
+      long ic[16];
+      for (int q = 0; q < 16; q++) ic[q] = cnt[q];
+      for (int x = 0; x < 4; x++) ic[x * 5] += icd[x] + rc.constCnt[x];
+      double tot = 0., nf[4] = {0., 0., 0., 0.};
+      for (int c1 = 0; c1 < 4; c1++)
+        for (int c2 = 0; c2 < 4; c2++) {
+          const double pc = fc[c1 * 4 + c2] = __dadd_rn(fc[c1 * 4 + c2], (double)ic[c1 * 4 + c2]);
+          tot = __dadd_rn(tot, pc);
+          nf[c1] = __dadd_rn(nf[c1], pc);
+          nf[c2] = __dadd_rn(nf[c2], pc);
+        }
+      if (tot <= (double)rc.min_overlap) {
+        R.skip = true;
+      } else if (t == 0 && rc.fallback_avg && __dmul_rn(tot, rc.resolve_fraction) <= (double)(unsigned long)amb) {
+        next = 1;
+      } else {
+        R.diag = __dadd_rn(__dadd_rn(__dadd_rn(fc[0], fc[5]), fc[10]), fc[15]);
+        R.ag = __dadd_rn(fc[2], fc[8]);
+        R.ct = __dadd_rn(fc[7], fc[13]);
+        for (int q = 0; q < 4; q++) R.nf[q] = nf[q];
+      }
+    }
+    next = __shfl_sync(0xffffffffu, next, 0);
+    if (!next) break;
+    t = 1;
+  }
+  return R;
+}
+
+// The order-dependent pairs (a contribution that is not a multiple of 1/16), one warp per pair from the queue.
 __device__ __forceinline__ void replay_run(const ReplayArgs &a)
 {
   __shared__ unsigned char sc1[kWarps][64], sc2[kWarps][64];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned long long n = min((unsigned long long)*a.qn, a.qcap);
   if (blockIdx.x == 0 && threadIdx.x == 0 && n) atomicAdd(&a.counters[2], n);
-  const RunConsts &rc = a.rc;
-  const long Np = rc.Npad;
-  const uint64_t last_valid = (rc.Lc & 63) ? ((1ull << (rc.Lc & 63)) - 1ull) : ~0ull;
+  AmbLane al;
+  al.unit = -1;
   for (unsigned long long idx = (unsigned long long)blockIdx.x * kWarps + warp; idx < n;
        idx += (unsigned long long)gridDim.x * kWarps) {
     const unsigned long long e = a.q[idx];
-    int t = (int)(e >> 63);
+    const int t = (int)(e >> 63);
     const long i = (long)((e >> 31) & 0xFFFFFFFFull), j = (long)(e & 0x7FFFFFFFull);
-    const uint8_t *s1 = a.cc + (size_t)i * rc.Lc, *s2 = a.cc + (size_t)j * rc.Lc;
-    // clean/clean 4x4 counts (the same in every mode)
-    int cnt[16];
-#pragma unroll
-    for (int q = 0; q < 16; q++) cnt[q] = 0;
-    for (long w = lane; w < rc.W; w += 32) {
-      const uint64_t *P = a.planes + (size_t)w * rc.NP * Np;
-      const uint64_t hi = P[i], lo = P[Np + i], ci = P[2 * Np + i];
-      const uint64_t hj = P[j], lj = P[Np + j], cj = P[2 * Np + j];
-      const uint64_t xi[4] = {ci & ~hi & ~lo, ci & hi & ~lo, ci & ~hi & lo, ci & hi & lo};
-      const uint64_t xj[4] = {cj & ~hj & ~lj, cj & hj & ~lj, cj & ~hj & lj, cj & hj & lj};
-#pragma unroll
-      for (int x = 0; x < 4; x++)
-#pragma unroll
-        for (int y = 0; y < 4; y++) cnt[x * 4 + y] += popc(xi[x] & xj[y]);
-    }
-#pragma unroll
-    for (int q = 0; q < 16; q++)
-      for (int o = 16; o; o >>= 1) cnt[q] += __shfl_xor_sync(0xffffffffu, cnt[q], o);
-    double res = 0;
-    bool qamb = false, qund = false;
-    for (;;) {
-      const SiteEntry *S = a.site + t * kCodes * kCodes;
-      double acc = 0.;  // lane q < 16: float cell q
-      long iacc = 0;    // lanes 16..19: diagonal resolutions, lane 20: ambiguity count
-      for (long w = 0; w < rc.W; w++) {
-        const uint64_t *P = a.planes + (size_t)w * rc.NP * Np;
-        uint64_t E = ~(P[2 * Np + i] & P[2 * Np + j]);
-        if (w == rc.W - 1) E &= last_valid;
-        if (!E) continue;
-        const int ne = __popcll(E), nlo = __popc((unsigned)E);
-        for (int rk = lane; rk < ne; rk += 32) {
-          const int bit = rk < nlo ? nth_bit32((unsigned)E, rk) : 32 + nth_bit32((unsigned)(E >> 32), rk - nlo);
-          const long k = w * 64 + bit;
-          sc1[warp][rk] = s1[k];
-          sc2[warp][rk] = s2[k];
-        }
-        __syncwarp();
-        if (lane < 16) {
-          for (int l = 0; l < ne; l++) {
-            const double v = S[sc1[warp][l] * kCodes + sc2[warp][l]].fc[lane];
-            if (v != 0.) acc = __dadd_rn(acc, v);
-          }
-        } else if (lane < 20) {
-          for (int l = 0; l < ne; l++) iacc += S[sc1[warp][l] * kCodes + sc2[warp][l]].icd[lane - 16];
-        } else if (lane == 20) {
-          for (int l = 0; l < ne; l++) iacc += S[sc1[warp][l] * kCodes + sc2[warp][l]].amb;
-        }
-        __syncwarp();
-      }
-      // lane 0: gather the cells, then tn93's merge and decisions
-      double fc[16];
-      long icd[4];
-#pragma unroll
-      for (int q = 0; q < 16; q++) fc[q] = __shfl_sync(0xffffffffu, acc, q);
-#pragma unroll
-      for (int q = 0; q < 4; q++) icd[q] = __shfl_sync(0xffffffffu, iacc, 16 + q);
-      const long amb = __shfl_sync(0xffffffffu, iacc, 20);
-      int next = 0;  // 0 done, 1 recompute with -a average
-      if (lane == 0) {
-        long ic[16];
-        for (int q = 0; q < 16; q++) ic[q] = cnt[q];
-        for (int x = 0; x < 4; x++) ic[x * 5] += icd[x] + rc.constCnt[x];
-        double tot = 0., nf[4] = {0., 0., 0., 0.};
-        for (int c1 = 0; c1 < 4; c1++)
-          for (int c2 = 0; c2 < 4; c2++) {
-            const double pc = fc[c1 * 4 + c2] = __dadd_rn(fc[c1 * 4 + c2], (double)ic[c1 * 4 + c2]);
-            tot = __dadd_rn(tot, pc);
-            nf[c1] = __dadd_rn(nf[c1], pc);
-            nf[c2] = __dadd_rn(nf[c2], pc);
-          }
-        if (tot <= (double)rc.min_overlap) {
-          res = __longlong_as_double((long long)kSkipBits);
-        } else if (t == 0 && rc.fallback_avg && __dmul_rn(tot, rc.resolve_fraction) <= (double)(unsigned long)amb) {
-          next = 1;
-        } else {
-          const double diag = __dadd_rn(__dadd_rn(__dadd_rn(fc[0], fc[5]), fc[10]), fc[15]);
-          res = finish_distance(*a.logt, rc, nf, diag, __dadd_rn(fc[2], fc[8]), __dadd_rn(fc[7], fc[13]), qamb, qund);
-        }
-      }
-      next = __shfl_sync(0xffffffffu, next, 0);
-      if (!next) break;
-      t = 1;
-    }
+    const WalkOut W = walk_pair(a, i, j, t, sc1[warp], sc2[warp]);
     if (lane == 0) {
+      int qa = 0, qu = 0;
+      const double res = W.skip ? __longlong_as_double((long long)kSkipBits)
+                                : finish_exact(*a.logt, a.rc, a.ex, W.nf, W.diag, W.ag, W.ct, i, j, a.colbase, qa,
+                                               qu, al);
       a.dist[(size_t)(i - a.r0) * a.ncols + (j - a.colbase)] = res;
-      if (qamb) atomicAdd(&a.counters[0], 1ull);
-      if (qund) atomicAdd(&a.counters[1], 1ull);
+      if (qa) atomicAdd(&a.counters[0], 1ull);
+      if (qu) atomicAdd(&a.counters[1], 1ull);
     }
   }
+  if (a.ex.amb && lane == 0 && al.unit >= 0) amb_flush(a.ex.amb, al.unit, al.n, al.lo, al.hi, al.spread);
+}
+
+// Undecided pairs, step 1 (one warp per listed pair): the site-order walk gives the formula's exact inputs in any
+// mode (for a pair the pair kernel finished, its x16 aggregates and the walk's float sums are the same numbers),
+// then the arguments of its logarithms. descs[k] describes run k of the list's entries.
+__global__ void __launch_bounds__(256) und_args_kernel(const ReplayArgs *descs, const unsigned long long *list,
+                                                       unsigned n, UndEntry *out)
+{
+  __shared__ unsigned char sc1[kWarps][64], sc2[kWarps][64];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (unsigned idx = blockIdx.x * kWarps + warp; idx < n; idx += gridDim.x * kWarps) {
+    const int k = (int)list[2 * (size_t)idx];
+    const unsigned long long ij = list[2 * (size_t)idx + 1];
+    const long i = (long)(ij >> 32), j = (long)(ij & 0xFFFFFFFFull);
+    const ReplayArgs &a = descs[k];
+    const WalkOut W = walk_pair(a, i, j, 0, sc1[warp], sc2[warp]);
+    if (lane == 0) {
+      UndEntry &E = out[idx];
+      E.k = k;
+      E.slot = (long)((i - a.r0) * a.ncols + (j - a.colbase));
+      E.state = W.skip ? 1 : 0;
+      E.nlog = 0;
+      for (int q = 0; q < 4; q++) E.in[q] = W.nf[q];
+      E.in[4] = W.diag;
+      E.in[5] = W.ag;
+      E.in[6] = W.ct;
+      E.arg[0] = E.arg[1] = E.arg[2] = 1.0;
+      if (!W.skip) {
+        const Prep P = tn93_prep(W.nf, W.diag, W.ag, W.ct);
+        E.nlog = P.nlog;
+        for (int q = 0; q < 3; q++) E.arg[q] = P.arg[q];
+      }
+    }
+  }
+}
+
+// Undecided pairs, step 2 (one thread per pair): the formula from the C library's logarithms (UndEntry::lg)
+__global__ void und_finish_kernel(const ReplayArgs *descs, const UndEntry *e, unsigned n)
+{
+  const unsigned idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const UndEntry &E = e[idx];
+  if (E.state) return;
+  const double nf[4] = {E.in[0], E.in[1], E.in[2], E.in[3]};
+  const Prep P = tn93_prep(nf, E.in[4], E.in[5], E.in[6]);
+  descs[E.k].dist[E.slot] = tn93_combine(P, E.lg[0], E.lg[1], E.lg[2]);
 }
 
 __global__ void __launch_bounds__(256) replay_kernel(ReplayArgs a) { replay_run(a); }
@@ -1250,34 +1495,47 @@ __global__ void fill_nan_kernel(double *p, size_t n)
     p[k] = __longlong_as_double(0x7FF8000000000000ll);
 }
 
-// True the first time it is called for the current device with this flag word. Kernel attributes (the opt-in to
-// more than 48 KB of dynamic shared memory) belong to each device's context, so they are set once per device.
-bool first_on_device(std::atomic<unsigned long long> &done)
-{
-  int d = 0;
-  cudaGetDevice(&d);
-  const unsigned long long bit = 1ull << (d & 63);
-  return !(done.fetch_or(bit) & bit);
-}
+// Kernel attributes (the opt-in to more than 48 KB of dynamic shared memory) belong to each device's context, so
+// they are set once per device. PerDevice::once runs set() for the current device unless it already succeeded
+// there; callers on other threads wait for it (the lock is held while set() runs), and a failed set() is retried
+// by the next call, so no launch can see the flag before the attribute is in place.
+struct PerDevice {
+  std::mutex mu;
+  std::atomic<unsigned long long> done{0};
+  template <class F>
+  cudaError_t once(F set)
+  {
+    int d = 0;
+    cudaError_t e = cudaGetDevice(&d);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = 1ull << (d & 63);
+    if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+    std::lock_guard<std::mutex> g(mu);
+    if (done.load(std::memory_order_relaxed) & bit) return cudaSuccess;
+    e = set();
+    if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_release);
+    return e;
+  }
+};
 
 // pair kernel launch (dynamic shared memory above the 48 KB default needs the opt-in attribute once per device).
 // Two register budgets are built: 2 blocks per SM (128 registers, no spills) and 3 (80 registers, some spills).
 template <int MINB>
 cudaError_t launch_pair_t(const PairArgs &A, dim3 g, cudaStream_t st)
 {
-  static std::atomic<unsigned long long> attr_done{0};
-  if (first_on_device(attr_done)) {
-    cudaError_t e;
-    if ((e = cudaFuncSetAttribute(pair_kernel<false, false, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  static PerDevice attr;
+  cudaError_t e = attr.once([] {
+    cudaError_t r;
+    if ((r = cudaFuncSetAttribute(pair_kernel<false, false, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kPairSmem)) != cudaSuccess)
-      return e;
-    if ((e = cudaFuncSetAttribute(pair_kernel<true, false, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      return r;
+    if ((r = cudaFuncSetAttribute(pair_kernel<true, false, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kPairSmem)) != cudaSuccess)
-      return e;
-    if ((e = cudaFuncSetAttribute(pair_kernel<true, true, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kPairSmem)) != cudaSuccess)
-      return e;
-  }
+      return r;
+    return cudaFuncSetAttribute(pair_kernel<true, true, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kPairSmem);
+  });
+  if (e != cudaSuccess) return e;
   if (A.rc.wplane) {
     if (A.rc.gapmm)
       pair_kernel<true, true, MINB><<<g, 256, kPairSmem, st>>>(A);
@@ -1302,6 +1560,14 @@ cudaError_t launch_pair(const PairArgs &A, long ncolblocks, long nrows, cudaStre
   return minb == 3 ? launch_pair_t<3>(A, g, st) : launch_pair_t<2>(A, g, st);
 }
 
+// the tensor-core count kernel's opt-in to its dynamic shared memory, once per device
+cudaError_t tc_attr_once()
+{
+  static PerDevice attr;
+  return attr.once(
+      [] { return cudaFuncSetAttribute(count_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem); });
+}
+
 }  // namespace
 
 //================================================================================================== host side
@@ -1310,6 +1576,8 @@ struct DevBuf {
   void *p = nullptr;
   size_t n = 0;
 };
+
+constexpr int kBatchBufs = 56;
 
 struct tn93g_set {
   long N = 0, L = 0;
@@ -1329,6 +1597,7 @@ struct tn93g_ctx {
   std::string err;
   LogTable *d_logt = nullptr;
   Tables *h_tab = nullptr;
+  PairTables *h_ptab = nullptr;  // host staging of the pair stage's tables
   DevBuf seen, nN, varcol, planes, cc, ccT, evcount, evoff, ev, agg, site, dist, rq, rqn, counters, rbytes, rsum, rw,
       rmax, rlinks, rskip, hist, roff, out, hy;
   void *pinned = nullptr;
@@ -1336,7 +1605,8 @@ struct tn93g_ctx {
   cudaEvent_t evs[16];
   cudaStream_t copy_stream = nullptr;  // device->host copies of finished bands
   cudaEvent_t evw0[2], evw1[2], evc0[2], evc1[2];
-  cudaEvent_t evk[2][5];  // per band parity: start, after pair, after replay, after stats+sums+scan, stats on host
+  cudaEvent_t evk[2][6];  // per band parity: start, after pair, after replay, after stats+sums+scan, stats on host,
+                          // after the tensor-core count kernel
   DevBuf out2[2], total;
   void *pin2[2] = {nullptr, nullptr};
   size_t pin2_n[2] = {0, 0};
@@ -1347,10 +1617,17 @@ struct tn93g_ctx {
   double timings[8] = {0};
   long launches = 0;
   size_t dev_out_n = 0;
-  DevBuf bb[48];  // buffers of tn93g_batch_run (indexed by BatchBuf)
+  DevBuf bb[kBatchBufs];  // buffers of tn93g_batch_run (indexed by BatchBuf)
   int count_path = 1;  // clean-site counts: 0 popcounts on the CUDA cores, 1 tensor cores (tcgen05)
   int sms = 148;       // streaming multiprocessors of the device (persistent and grid-stride launches)
   DevBuf ohimg, tcagg, tcerr;
+  uint64_t wait_ns = kTcWaitNs;  // limit of each bounded device wait
+  bool exact_sums = false;       // tn93g_set_exact_sums
+  int fault = TN93G_FAULT_NONE;  // test hook for the next run (tn93g_inject_fault)
+  // exactness: undecided lists and counts per band parity, the summary units' bounds, the resolver's entries and
+  // run descriptors, and the logarithm's band and candidate spread (tn93g_set_log_band)
+  DevBuf und[2], undn, amb, undwork, rdesc;
+  double log_band = kLogBand, log_spread = kLogSpread;
 };
 
 namespace {
@@ -1437,7 +1714,70 @@ int ensure_keep(tn93g_ctx *ctx, DevBuf &b, size_t bytes, size_t keep)
     if (r_ != TN93G_OK) return r_; \
   } while (0)
 
+// The host's C library log of every listed argument: the decision oracle for pairs whose printed bytes or
+// decisions depend on how that log rounds (the reference calls the same function, swifttn93.cpp:1954-2001).
+// Large lists (resolve-all passes) are split over the host's threads.
+void host_logs(std::vector<UndEntry> &E)
+{
+  auto work = [&E](size_t b, size_t e) {
+    for (size_t k = b; k < e; k++)
+      for (int q = 0; q < 3; q++) E[k].lg[q] = q < E[k].nlog ? log(E[k].arg[q]) : 0.;
+  };
+  const size_t n = E.size();
+  const unsigned nt = std::max(1u, std::min(std::thread::hardware_concurrency(), (unsigned)(n / 65536 + 1)));
+  if (nt == 1) {
+    work(0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < nt; t++) th.emplace_back(work, n * t / nt, n * (t + 1) / nt);
+  for (auto &t : th) t.join();
+}
+
+// Finishes the n listed pairs (entries (k, i << 32 | j), run k described by d_descs[k] in device memory) with the
+// C library's logarithms: the site-order walk gives each pair's formula arguments on the device, the host takes
+// their logs, and the device evaluates the formula with them into the pair's raw-distance slot.
+int resolve_listed(tn93g_ctx *ctx, const ReplayArgs *d_descs, const unsigned long long *d_list, unsigned n,
+                   cudaStream_t st)
+{
+  if (!n) return TN93G_OK;
+  TRY(ensure(ctx, ctx->undwork, (size_t)n * sizeof(UndEntry)));
+  UndEntry *dw = (UndEntry *)ctx->undwork.p;
+  und_args_kernel<<<(unsigned)std::min<unsigned long>((n + kWarps - 1) / kWarps, 8ul * ctx->sms), 256, 0, st>>>(
+      d_descs, d_list, n, dw);
+  CU(cudaGetLastError());
+  std::vector<UndEntry> h(n);
+  CU(cudaMemcpyAsync(h.data(), dw, (size_t)n * sizeof(UndEntry), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  host_logs(h);
+  CU(cudaMemcpyAsync(dw, h.data(), (size_t)n * sizeof(UndEntry), cudaMemcpyHostToDevice, st));
+  und_finish_kernel<<<(n + 255) / 256, 256, 0, st>>>(d_descs, dw, n);
+  CU(cudaGetLastError());
+  ctx->launches += 2;
+  return TN93G_OK;
+}
+
+// the pair stage's tables for a run: the x16 event table (with the N-plane entries) and its packed form
+void fill_pair_tables(const Tables &T, bool wplane, PairTables *out)
+{
+  memcpy(out->agg, T.ev, sizeof out->agg);
+  pack_tables(T, wplane, &out->packed);
+}
+
+// the summary units' bounds (ExactSink::amb words) as doubles: {largest low, largest high, spread, count}
+void amb_bounds(const unsigned long long *w, double out[4])
+{
+  memcpy(&out[0], &w[0], 8);
+  memcpy(&out[1], &w[1], 8);
+  memcpy(&out[2], &w[2], 8);
+  out[3] = (double)w[3];
+}
+
 }  // namespace
+
+namespace tn93 {
+bool summary_certified(const tn93g_summary *s, const double bounds[3][4], long chain, int fst);
+}
 
 extern "C" {
 
@@ -1454,6 +1794,7 @@ const char *tn93g_strerror(int code)
     case TN93G_ETOOBIG: return "alignment too long (L >= 2^25)";
     case TN93G_ESCRATCH: return "alignment exceeds the allocation-free entry point's limits (N <= 512, L <= 4096)";
     case TN93G_EFASTA: return "the FASTA reader refused the input";
+    case TN93G_EUNDECIDED: return "a distance could not be decided exactly";
     default: return "unknown error";
   }
 }
@@ -1464,6 +1805,36 @@ int tn93g_set_count_path(tn93g_ctx *ctx, int path)
 {
   if (!ctx || path < 0 || path > 1) return TN93G_EINVAL;
   ctx->count_path = path;
+  return TN93G_OK;
+}
+
+int tn93g_set_log_band(tn93g_ctx *ctx, double band_ulps, double spread_ulps)
+{
+  if (!ctx || !(band_ulps >= kLogBand && band_ulps <= 0.5) || !(spread_ulps >= 1.0 && spread_ulps <= 0x1p40))
+    return TN93G_EINVAL;
+  ctx->log_band = band_ulps;
+  ctx->log_spread = floor(spread_ulps);
+  return TN93G_OK;
+}
+
+int tn93g_set_exact_sums(tn93g_ctx *ctx, int on)
+{
+  if (!ctx) return TN93G_EINVAL;
+  ctx->exact_sums = on != 0;
+  return TN93G_OK;
+}
+
+int tn93g_set_wait_limit(tn93g_ctx *ctx, double seconds)
+{
+  if (!ctx || !(seconds > 0. && seconds <= 60.)) return TN93G_EINVAL;
+  ctx->wait_ns = (uint64_t)(seconds * 1e9);
+  return TN93G_OK;
+}
+
+int tn93g_inject_fault(tn93g_ctx *ctx, int fault)
+{
+  if (!ctx || fault < TN93G_FAULT_NONE || fault > TN93G_FAULT_SKIP_FILL) return TN93G_EINVAL;
+  ctx->fault = fault;
   return TN93G_OK;
 }
 
@@ -1497,6 +1868,10 @@ int tn93g_create(tn93g_ctx **out, int device, size_t hbm_budget)
     }
     if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) rc = TN93G_ECUDA;
     if (const char *e = getenv("TN93G_COUNT")) ctx->count_path = strcmp(e, "popc") == 0 ? 0 : 1;
+    {
+      const char *b = getenv("TN93G_LOG_BAND"), *p = getenv("TN93G_LOG_SPREAD");
+      if (b || p) tn93g_set_log_band(ctx, b ? atof(b) : kLogBand, p ? atof(p) : kLogSpread);
+    }
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0)
       ctx->sms = sms;
@@ -1506,6 +1881,7 @@ int tn93g_create(tn93g_ctx **out, int device, size_t hbm_budget)
         cudaMemcpy(ctx->d_logt, &h, sizeof h, cudaMemcpyHostToDevice) != cudaSuccess)
       rc = TN93G_ECUDA;
     ctx->h_tab = new Tables();
+    ctx->h_ptab = new PairTables();
   } while (0);
   if (rc != TN93G_OK) {
     tn93g_destroy(ctx);
@@ -1527,7 +1903,8 @@ void tn93g_destroy(tn93g_ctx *ctx)
     if (b->p) cudaFree(b->p);
   for (DevBuf &b : ctx->bb)
     if (b.p) cudaFree(b.p);
-  for (DevBuf *b : {&ctx->ohimg, &ctx->tcagg, &ctx->tcerr})
+  for (DevBuf *b : {&ctx->ohimg, &ctx->tcagg, &ctx->tcerr, &ctx->und[0], &ctx->und[1], &ctx->undn, &ctx->amb,
+                    &ctx->undwork, &ctx->rdesc})
     if (b->p) cudaFree(b->p);
   if (ctx->d_logt) cudaFree(ctx->d_logt);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
@@ -1547,6 +1924,7 @@ void tn93g_destroy(tn93g_ctx *ctx)
     if (e) cudaEventDestroy(e);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx->h_tab;
+  delete ctx->h_ptab;
   delete ctx;
 }
 
@@ -1631,7 +2009,7 @@ void tn93g_free_set(tn93g_ctx *ctx, tn93g_set *s)
 int tn93g_last_timings(tn93g_ctx *ctx, double *ms, int n)
 {
   if (!ctx || !ms) return 0;
-  const int k = std::min(n, 7);
+  const int k = std::min(n, 8);
   for (int q = 0; q < k; q++) ms[q] = ctx->timings[q];
   return k;
 }
@@ -1640,9 +2018,11 @@ void *tn93g_stream(tn93g_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr;
 
 long tn93g_last_launches(tn93g_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
+// flags of run_impl: a second, exact pass for the JSON numbers (every ambiguous logarithm taken from the C library)
+constexpr int kRunResolveAll = 1;
 static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_opts *opts, tn93g_sink sink, void *user,
                     tn93g_summary *sum, bool to_device, long row_begin = 0, long row_end = -1,
-                    double *row_sums = nullptr);
+                    double *row_sums = nullptr, int flags = 0);
 
 int tn93g_run(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_opts *opts, tn93g_sink sink, void *user,
               tn93g_summary *sum)
@@ -1668,7 +2048,7 @@ int tn93g_run_to_device(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn9
 }
 
 static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_opts *opts, tn93g_sink sink, void *user,
-                    tn93g_summary *sum, bool to_device, long row_begin, long row_end, double *row_sums)
+                    tn93g_summary *sum, bool to_device, long row_begin, long row_end, double *row_sums, int flags)
 {
   if (!ctx || !set || !opts || !sum || n1 <= 0 || n1 > set->N) return TN93G_EINVAL;
   if (opts->mode < 0 || opts->mode > 4 || opts->format < 0 || opts->format > 2) return TN93G_EINVAL;
@@ -1697,6 +2077,11 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   rc.min_distance = opts->min_distance;
   rc.resolve_fraction = opts->resolve_fraction;
   rc.min_overlap = opts->min_overlap;
+  rc.log_band = ctx->log_band;
+  rc.log_spread = ctx->log_spread;
+  rc.resolve_all = (flags & kRunResolveAll) != 0 || ctx->exact_sums;
+  const int fault = ctx->fault;
+  ctx->fault = TN93G_FAULT_NONE;  // a fault is injected into one run only
   const bool hyphy = rc.emit && opts->format == TN93G_HYPHY;
   cudaEvent_t *E = ctx->evs;
   CU(cudaEventRecord(E[0], st));
@@ -1776,7 +2161,12 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   CU(cudaMemcpyAsync(evc.data(), ctx->evcount.p, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   CU(cudaStreamSynchronize(st));
   evoff[0] = 0;
-  for (long i = 0; i < N; i++) evoff[i + 1] = evoff[i] + evc[i];
+  uint32_t max_ev = 0;
+  for (long i = 0; i < N; i++) {
+    evoff[i + 1] = evoff[i] + evc[i];
+    max_ev = std::max(max_ev, evc[i]);
+  }
+  rc.packed = max_ev <= (uint32_t)kPackedMaxEvents;
   TRY(ensure(ctx, ctx->ev, std::max<size_t>(evoff[N], 1) * sizeof(uint32_t)));
   CU(cudaMemcpyAsync(ctx->evoff.p, evoff.data(), (N + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
   pa.ev = (uint32_t *)ctx->ev.p;
@@ -1787,10 +2177,10 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   }
   // tables of this mode
   build_tables(ctx->h_tab, opts->mode, opts->subset);
-  const size_t agg_n = kSparseCodes * kCodes + 5;
-  TRY(ensure(ctx, ctx->agg, agg_n * sizeof(AggEntry)));
+  fill_pair_tables(*ctx->h_tab, rc.wplane, ctx->h_ptab);
+  TRY(ensure(ctx, ctx->agg, sizeof(PairTables)));
   TRY(ensure(ctx, ctx->site, sizeof(ctx->h_tab->site)));
-  CU(cudaMemcpyAsync(ctx->agg.p, ctx->h_tab->ev, agg_n * sizeof(AggEntry), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(ctx->agg.p, ctx->h_ptab, sizeof(PairTables), cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync(ctx->site.p, ctx->h_tab->site, sizeof(ctx->h_tab->site), cudaMemcpyHostToDevice, st));
   // tensor-core count path: the one-hot operand image of every sequence (an extra 32-sequence block at the end,
   // which the last 64-column tile reads)
@@ -1805,9 +2195,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
                                                                   (uint8_t *)ctx->ohimg.p, 0, tc_NB * 32);
     CU(cudaGetLastError());
     ctx->launches++;
-    static std::atomic<unsigned long long> attr{0};
-    if (first_on_device(attr))
-      CU(cudaFuncSetAttribute(count_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    CU(tc_attr_once());
   }
   CU(cudaEventRecord(E[1], st));
 
@@ -1830,19 +2218,30 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     const char *e = getenv("TN93G_BAND_PAIRS");  // tuning knob: pairs per band when streaming text
     return e && atol(e) > 0 ? atol(e) : (3l << 20);
   }();
-  const long target_pairs = stream_text ? band_pairs : (1l << 62);
-  const long cap_slots = stream_text ? (16l << 20) : (64l << 20);
+  const long target_pairs = (stream_text || rc.resolve_all) ? band_pairs : (1l << 62);
+  const long cap_slots = (stream_text || rc.resolve_all) ? (16l << 20) : (64l << 20);
+  // When the text streams to the host, the bands ramp up (1/8, 1/4, 1/2 of the target) and taper at the end
+  // (half of what is left, down to 1/8), so that the first copy starts early and the last one, which nothing
+  // overlaps, is short.
   std::vector<std::pair<long, long>> bands;
   long maxrows = 1;
+  long left = 0;
+  for (long r = row_begin; r < upper; r++) left += rc.cross ? ncols : (N - r - 1);
   for (long r0 = row_begin; r0 < upper;) {
+    long tgt = target_pairs;
+    if (stream_text) {
+      const long k = (long)bands.size();
+      if (k < 3) tgt = target_pairs >> (3 - k);
+      if (left < 2 * target_pairs) tgt = std::min(tgt, std::max(target_pairs / 8, left / 2));
+    }
     long r = r0, pairs = 0;
-    while (r < upper && (r == r0 || ((r - r0 + 1) * ncols <= cap_slots && pairs < target_pairs &&
-                                     r - r0 < 65535l * kTile))) {
+    while (r < upper && (r == r0 || ((r - r0 + 1) * ncols <= cap_slots && pairs < tgt && r - r0 < 65535l * kTile))) {
       pairs += rc.cross ? ncols : (N - r - 1);
       r++;
     }
     bands.push_back({r0, r});
     maxrows = std::max(maxrows, r - r0);
+    left -= pairs;
     r0 = r;
   }
   const long band = maxrows;
@@ -1858,7 +2257,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   const size_t dslots = (size_t)band * ncols;
   TRY(ensure(ctx, ctx->dist, 2 * dslots * sizeof(double)));
   const int tc16 = 2 * Lc < 65536;
-  if (use_tc) TRY(ensure(ctx, ctx->tcagg, 7 * dslots * (tc16 ? sizeof(uint16_t) : sizeof(int32_t))));
+  if (use_tc) TRY(ensure(ctx, ctx->tcagg, dslots * (tc16 ? 16 : 32)));
   TRY(ensure(ctx, ctx->rq, dslots * sizeof(unsigned long long)));
   TRY(ensure(ctx, ctx->rqn, sizeof(unsigned)));
   TRY(ensure(ctx, ctx->counters, 4 * sizeof(unsigned long long)));
@@ -1869,22 +2268,32 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   TRY(ensure(ctx, ctx->rmax, 2 * nseg * 3 * sizeof(double)));
   TRY(ensure(ctx, ctx->rlinks, 2 * nseg * sizeof(long long)));
   TRY(ensure(ctx, ctx->rskip, 2 * nseg * sizeof(long long)));
-  TRY(ensure(ctx, ctx->hist, 3 * kHistBins * sizeof(unsigned long long)));
+  // per band parity: its histogram (added on the host, so a band's row stage can run again), its undecided list
+  TRY(ensure(ctx, ctx->hist, 2 * 3 * kHistBins * sizeof(unsigned long long)));
   TRY(ensure(ctx, ctx->total, 2 * sizeof(unsigned long long)));
+  const unsigned und_cap = (unsigned)std::min<size_t>(rc.resolve_all ? dslots : std::max<size_t>(4096, dslots / 64),
+                                                      0xFFFFFFF0u);
+  for (int q = 0; q < 2; q++) TRY(ensure(ctx, ctx->und[q], (size_t)und_cap * 2 * sizeof(unsigned long long)));
+  TRY(ensure(ctx, ctx->undn, 2 * sizeof(unsigned long long)));
+  TRY(ensure(ctx, ctx->amb, 3 * 4 * sizeof(unsigned long long)));
+  TRY(ensure(ctx, ctx->rdesc, 2 * sizeof(ReplayArgs)));
+  CU(cudaMemsetAsync(ctx->amb.p, 0, 3 * 4 * sizeof(unsigned long long), st));
   // pinned staging of a band's statistics: row sums and weights (3 each), segment maxima (3 each), segment links
-  // and skips, total bytes
+  // and skips, total bytes, the band's histogram, its undecided count and the count kernel's error word
   const size_t stat_stride = (size_t)band * 6 * sizeof(double) +
-                             (size_t)nseg * (3 * sizeof(double) + 2 * sizeof(long long)) + sizeof(unsigned long long);
+                             (size_t)nseg * (3 * sizeof(double) + 2 * sizeof(long long)) +
+                             (3 + 3 * kHistBins) * sizeof(unsigned long long);
   TRY(ensure_pinned_at(ctx, ctx->pstats, ctx->pstats_n, 2 * stat_stride));
   CU(cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(unsigned long long), st));
-  CU(cudaMemsetAsync(ctx->hist.p, 0, 3 * kHistBins * sizeof(unsigned long long), st));
   double max_[3] = {0, 0, 0}, mean[3] = {0, 0, 0}, wc[3] = {0, 0, 0};
-  long links = 0, skipped = 0;
+  unsigned long long hist_total[3 * kHistBins];
+  memset(hist_total, 0, sizeof hist_total);
+  long links = 0, skipped = 0, resolved = 0;
   float ms = 0;
   struct HostStats {
     double *sum, *w, *max;
     long long *links, *skip;
-    unsigned long long *total;
+    unsigned long long *total, *hist, *und, *tcerr;
   };
   auto host_stats = [&](int par) {
     char *base = (char *)ctx->pstats + par * stat_stride;
@@ -1895,8 +2304,12 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     h.links = (long long *)(h.max + nseg * 3);
     h.skip = h.links + nseg;
     h.total = (unsigned long long *)(h.skip + nseg);
+    h.hist = h.total + 1;
+    h.und = h.hist + 3 * kHistBins;
+    h.tcerr = h.und + 1;
     return h;
   };
+  ReplayArgs rdesc_h[2];
   auto row_args = [&](int bi) {
     const int par = bi & 1;
     RowArgs RA;
@@ -1917,7 +2330,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     RA.seg_max = (double *)ctx->rmax.p + par * nseg * 3;
     RA.row_sum = (double *)ctx->rsum.p + par * band * 3;
     RA.row_w = (double *)ctx->rw.p + par * band * 3;
-    RA.hist = (unsigned long long *)ctx->hist.p;
+    RA.hist = (unsigned long long *)ctx->hist.p + par * 3 * kHistBins;
     RA.seg_off = (const unsigned long long *)ctx->roff.p + par * nseg;
     RA.seg_cols = nullptr;
     RA.nrows = RA.r1 - RA.r0;
@@ -1926,13 +2339,57 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     RA.err = (unsigned long long *)ctx->counters.p + 3;
     return RA;
   };
-  // pair -> replay -> stats -> sums -> scan of band bi, then its statistics to the host (on the compute stream)
+  // stats -> sums -> scan of band bi, then its statistics to the host (on the compute stream)
+  auto enqueue_rows = [&](int bi) -> int {
+    const int par = bi & 1;
+    const long nr = bands[bi].second - bands[bi].first;
+    cudaEvent_t *K = ctx->evk[par];
+    RowArgs RA = row_args(bi);
+    CU(cudaMemsetAsync(RA.hist, 0, 3 * kHistBins * sizeof(unsigned long long), st));
+    stats_kernel<<<dim3((unsigned)((nr + kWarps - 1) / kWarps), (unsigned)maxseg), 256, 0, st>>>(RA);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    sum_kernel<<<(unsigned)((nr + kWarps - 1) / kWarps), 256, 0, st>>>(RA);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    unsigned long long *dtot = (unsigned long long *)ctx->total.p + par;
+    scan_kernel<<<1, 1024, 0, st>>>(RA.seg_bytes, (unsigned long long *)RA.seg_off, nr * maxseg, dtot);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    CU(cudaEventRecord(K[3], st));
+    const HostStats h = host_stats(par);
+    CU(cudaMemcpyAsync(h.sum, RA.row_sum, nr * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(h.w, RA.row_w, nr * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(h.max, RA.seg_max, nr * maxseg * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(h.links, RA.seg_links, nr * maxseg * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(h.skip, RA.seg_skip, nr * maxseg * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(h.total, dtot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(h.hist, RA.hist, 3 * kHistBins * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(h.und, (unsigned long long *)ctx->undn.p + par, sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, st));
+    if (use_tc)
+      CU(cudaMemcpyAsync(h.tcerr, ctx->tcerr.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    else
+      *h.tcerr = 0;
+    CU(cudaEventRecord(K[4], st));
+    return TN93G_OK;
+  };
+  // pair -> replay of band bi, then its row stage
   auto enqueue_compute = [&](int bi) -> int {
     const int par = bi & 1;
     const long r0 = bands[bi].first, r1 = bands[bi].second, nr = r1 - r0;
     cudaEvent_t *K = ctx->evk[par];
     CU(cudaEventRecord(K[0], st));
     CU(cudaMemsetAsync(ctx->rqn.p, 0, sizeof(unsigned), st));
+    CU(cudaMemsetAsync((unsigned long long *)ctx->undn.p + par, 0, sizeof(unsigned long long), st));
+    ExactSink ex;
+    ex.und_list = (unsigned long long *)ctx->und[par].p;
+    ex.und_n = (unsigned *)((unsigned long long *)ctx->undn.p + par);
+    ex.und_cap = und_cap;
+    ex.und_k = 0;
+    ex.amb = (unsigned long long *)ctx->amb.p;
+    ex.counts = set->d_counts;
+    ex.colunit = nullptr;
     PairArgs A;
     A.rc = rc;
     A.planes = (const uint64_t *)ctx->planes.p;
@@ -1940,7 +2397,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     A.ccT = (const uint8_t *)ctx->ccT.p;
     A.ev_off = (const uint32_t *)ctx->evoff.p;
     A.ev = (const uint32_t *)ctx->ev.p;
-    A.agg = (const AggEntry *)ctx->agg.p;
+    A.tab = (const PairTables *)ctx->agg.p;
     A.r0 = r0;
     A.r1 = r1;
     A.ncols = ncols;
@@ -1951,6 +2408,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     A.replay_cap = (unsigned long long)dslots;
     A.counters = (unsigned long long *)ctx->counters.p;
     A.logt = ctx->d_logt;
+    A.ex = ex;
     // columns: the smallest lower bound of the band's rows onwards
     const long cstart = rc.cross ? n1 : r0 + 1;
     const long cblk0 = (cstart - colbase) / 32;
@@ -1973,15 +2431,17 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
       T.agg = ctx->tcagg.p;
       T.agg16 = tc16;
       T.err = (unsigned long long *)ctx->tcerr.p;
+      T.wait_ns = ctx->wait_ns;
+      T.skip_fill_block = fault == TN93G_FAULT_SKIP_FILL && bi == 0 ? 0 : -1;
       const long rt0 = r0 / kTcRows * kTcRows;
       const dim3 g((unsigned)((N - T.cstart + kTcCols - 1) / kTcCols), (unsigned)((r1 - rt0 + kTcRows - 1) / kTcRows));
       count_tc_kernel<<<g, 128, kTcSmem, st>>>(T);
       CU(cudaGetLastError());
       ctx->launches++;
       A.tcagg = ctx->tcagg.p;
-      A.tcplane = (size_t)nr * ncols;
       A.tc16 = tc16;
     }
+    CU(cudaEventRecord(K[5], st));
     if (cblks > 0) {
       A.cstart = colbase + cblk0 * 32;
       CU(launch_pair(A, cblks, nr, st));
@@ -2002,31 +2462,13 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     R.dist = A.dist;
     R.counters = (unsigned long long *)ctx->counters.p;
     R.logt = ctx->d_logt;
+    R.ex = ex;
+    rdesc_h[par] = R;
     replay_kernel<<<2 * ctx->sms, 256, 0, st>>>(R);
     CU(cudaGetLastError());
     ctx->launches++;
     CU(cudaEventRecord(K[2], st));
-    RowArgs RA = row_args(bi);
-    stats_kernel<<<dim3((unsigned)((nr + kWarps - 1) / kWarps), (unsigned)maxseg), 256, 0, st>>>(RA);
-    CU(cudaGetLastError());
-    ctx->launches++;
-    sum_kernel<<<(unsigned)((nr + kWarps - 1) / kWarps), 256, 0, st>>>(RA);
-    CU(cudaGetLastError());
-    ctx->launches++;
-    unsigned long long *dtot = (unsigned long long *)ctx->total.p + par;
-    scan_kernel<<<1, 1024, 0, st>>>(RA.seg_bytes, (unsigned long long *)RA.seg_off, nr * maxseg, dtot);
-    CU(cudaGetLastError());
-    ctx->launches++;
-    CU(cudaEventRecord(K[3], st));
-    const HostStats h = host_stats(par);
-    CU(cudaMemcpyAsync(h.sum, RA.row_sum, nr * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(h.w, RA.row_w, nr * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(h.max, RA.seg_max, nr * maxseg * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(h.links, RA.seg_links, nr * maxseg * sizeof(long long), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(h.skip, RA.seg_skip, nr * maxseg * sizeof(long long), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(h.total, dtot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
-    CU(cudaEventRecord(K[4], st));
-    return TN93G_OK;
+    return enqueue_rows(bi);
   };
   // bands whose text is on its way to the host: parities, oldest first
   int pend_par[2] = {0, 0}, pend_n = 0;
@@ -2053,11 +2495,35 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     CU(cudaEventSynchronize(K[4]));
     CU(cudaEventElapsedTime(&ms, K[0], K[1]));
     ctx->timings[1] += ms;
+    CU(cudaEventElapsedTime(&ms, K[0], K[5]));
+    ctx->timings[7] += ms;
     CU(cudaEventElapsedTime(&ms, K[1], K[2]));
     ctx->timings[2] += ms;
     CU(cudaEventElapsedTime(&ms, K[2], K[3]));
     ctx->timings[3] += ms;
     const HostStats h = host_stats(par);
+    if (*h.tcerr) {
+      // the next band's kernels may still be queued: let them drain so the context is idle for the next run
+      cudaStreamSynchronize(st);
+      ctx->err = "the tensor-core count kernel timed out waiting for its pipeline";
+      return TN93G_ETIMEOUT;
+    }
+    if (*h.und) {
+      // pairs whose bytes or decisions depend on the C library's rounding of a logarithm: finish them with its
+      // logarithms, then run the band's row stage again
+      if (*h.und > und_cap) {
+        cudaStreamSynchronize(st);
+        ctx->err = "more undecided pairs in a band than its list holds";
+        return TN93G_EUNDECIDED;
+      }
+      ReplayArgs *dd = (ReplayArgs *)ctx->rdesc.p + par;
+      CU(cudaMemcpyAsync(dd, &rdesc_h[par], sizeof(ReplayArgs), cudaMemcpyHostToDevice, st));
+      TRY(resolve_listed(ctx, dd, (const unsigned long long *)ctx->und[par].p, (unsigned)*h.und, st));
+      resolved += (long)*h.und;
+      TRY(enqueue_rows(bi));
+      CU(cudaEventSynchronize(K[4]));
+    }
+    for (int q = 0; q < 3 * kHistBins; q++) hist_total[q] += h.hist[q];
     // rows in order (swifttn93.cpp:2838-2848)
     for (long r = 0; r < nr; r++) {
       for (long g = r * maxseg; g < (r + 1) * maxseg; g++) {
@@ -2163,9 +2629,9 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     dev_off = tot;
     if (!to_device && sink && sink(user, (const char *)ctx->pinned, tot)) return TN93G_ESINK;
   }
-  unsigned long long hist[3 * kHistBins], counters[4];
-  CU(cudaMemcpyAsync(hist, ctx->hist.p, sizeof hist, cudaMemcpyDeviceToHost, st));
+  unsigned long long counters[4], ambw[12];
   CU(cudaMemcpyAsync(counters, ctx->counters.p, sizeof counters, cudaMemcpyDeviceToHost, st));
+  CU(cudaMemcpyAsync(ambw, ctx->amb.p, sizeof ambw, cudaMemcpyDeviceToHost, st));
   CU(cudaEventRecord(E[9], st));
   CU(cudaStreamSynchronize(st));
   CU(cudaEventElapsedTime(&ms, E[0], E[1]));
@@ -2176,12 +2642,13 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     sum->max[q] = max_[q];
     sum->mean[q] = mean[q];
     sum->weighted[q] = wc[q];
-    for (int k = 0; k < kHistBins; k++) sum->hist[q][k] = hist[q * kHistBins + k];
+    for (int k = 0; k < kHistBins; k++) sum->hist[q][k] = hist_total[q * kHistBins + k];
   }
   sum->links = links;
   sum->skipped = skipped;
   sum->logs_ambiguous = (long)counters[0];
-  sum->undecided = (long)counters[1];
+  sum->logs_resolved = resolved;
+  sum->undecided = (long)counters[1] - resolved;
   sum->pairs_replayed = (long)counters[2];
   ctx->dev_out_n = dev_off;
   if (use_tc) {
@@ -2195,6 +2662,36 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   if (counters[3]) {
     ctx->err = "internal error: a row's text did not match its counted length";
     return TN93G_ECUDA;
+  }
+  if (sum->undecided) {
+    ctx->err = "a pair's distance could not be decided exactly";
+    return TN93G_EUNDECIDED;
+  }
+  // The JSON numbers (maximum, means): certain for every rounding of the C library's log, or taken from a second
+  // pass that finishes every pair with an ambiguous logarithm with the C library's own (rows in the same order).
+  // (A proper range of rows is a part of a larger run: its caller certifies the merged summary.)
+  for (int u = 0; u < 3; u++) amb_bounds(ambw + 4 * u, sum->amb_bounds[u]);
+  if (rc.resolve_all) memset(sum->amb_bounds, 0, sizeof sum->amb_bounds);  // every ambiguous pair was finished exactly
+  const long chain = (rc.cross ? N - n1 : N) + (row_end - row_begin) + 2;
+  const bool whole = row_begin == 0 && row_end == all_rows;
+  if (!rc.resolve_all && whole && !summary_certified(sum, sum->amb_bounds, chain, rc.fst)) {
+    tn93g_opts o2 = *opts;
+    o2.count_only = 1;
+    tn93g_summary s2;
+    std::vector<double> rs2(row_sums ? (size_t)(row_end - row_begin) * 6 : 0);
+    const double t6 = ctx->timings[6];
+    TRY(run_impl(ctx, set, n1, &o2, nullptr, nullptr, &s2, false, row_begin, row_end,
+                 row_sums ? rs2.data() : nullptr, kRunResolveAll));
+    for (int q = 0; q < 3; q++) {
+      sum->max[q] = s2.max[q];
+      sum->mean[q] = s2.mean[q];
+    }
+    if (row_sums) memcpy(row_sums, rs2.data(), rs2.size() * sizeof(double));
+    sum->logs_resolved += s2.logs_resolved;
+    sum->sums_repass = 1;
+    memset(sum->amb_bounds, 0, sizeof sum->amb_bounds);
+    ctx->timings[6] += t6;
+    ctx->dev_out_n = dev_off;
   }
   return TN93G_OK;
 }
@@ -2213,7 +2710,7 @@ constexpr long kNaW = (kNaMaxL + 63) / 64;
 constexpr size_t na_al(size_t x) { return (x + 255) / 256 * 256; }
 constexpr size_t kNaLog = 0;
 constexpr size_t kNaAgg = kNaLog + na_al(sizeof(LogTable));
-constexpr size_t kNaSite = kNaAgg + na_al((kSparseCodes * kCodes + 5) * sizeof(AggEntry));
+constexpr size_t kNaSite = kNaAgg + na_al(sizeof(PairTables));
 constexpr size_t kNaSeen = kNaSite + na_al(2 * kCodes * kCodes * sizeof(SiteEntry));
 constexpr size_t kNaNN = kNaSeen + na_al(kNaMaxL * sizeof(uint32_t));
 constexpr size_t kNaVarcol = kNaNN + na_al(sizeof(unsigned long long));
@@ -2237,8 +2734,8 @@ constexpr int kNaMaxDevices = 64;
 std::mutex g_na_mu;
 unsigned char *g_na_base[kNaMaxDevices];
 
-// message of the last failure (written with g_na_mu held)
-char g_na_err[256];
+// message of the last failure of a call made by this thread
+thread_local char g_na_err[256];
 
 void na_error(const char *what, cudaError_t e)
 {
@@ -2271,7 +2768,8 @@ int noalloc_setup(int dev, unsigned char **base)
   return TN93G_OK;
 }
 
-Tables g_na_tables;  // host staging of the contribution tables (static storage; used with g_na_mu held)
+Tables g_na_tables;     // host staging of the contribution tables (static storage; used with g_na_mu held)
+PairTables g_na_ptab;  // and of the pair stage's form of them
 
 // caller holds g_na_mu
 int noalloc_run(const uint8_t *d_codes, long N, long L, const tn93g_opts *opts, double *d_dist, cudaStream_t st)
@@ -2303,6 +2801,9 @@ int noalloc_run(const uint8_t *d_codes, long N, long L, const tn93g_opts *opts, 
   rc.min_distance = opts->min_distance;
   rc.resolve_fraction = opts->resolve_fraction;
   rc.min_overlap = opts->min_overlap;
+  rc.log_band = kLogBand;
+  rc.log_spread = kLogSpread;
+  rc.resolve_all = false;
   uint32_t *seen = (uint32_t *)(S + kNaSeen);
   unsigned long long *nN = (unsigned long long *)(S + kNaNN);
   NA(cudaMemsetAsync(seen, 0, L * sizeof(uint32_t), st));
@@ -2362,15 +2863,20 @@ int noalloc_run(const uint8_t *d_codes, long N, long L, const tn93g_opts *opts, 
   NA(cudaMemcpyAsync(h_evc, pa.evcount, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   NA(cudaStreamSynchronize(st));
   h_evoff[0] = 0;
-  for (long i = 0; i < N; i++) h_evoff[i + 1] = h_evoff[i] + h_evc[i];
+  uint32_t max_ev = 0;
+  for (long i = 0; i < N; i++) {
+    h_evoff[i + 1] = h_evoff[i] + h_evc[i];
+    max_ev = std::max(max_ev, h_evc[i]);
+  }
+  rc.packed = max_ev <= (uint32_t)kPackedMaxEvents;
   NA(cudaMemcpyAsync(S + kNaEvoff, h_evoff, (N + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
   if (W && h_evoff[N]) {
     events_kernel<<<(unsigned)((N + kWarps - 1) / kWarps), 256, 0, st>>>(pa);
     NA(cudaGetLastError());
   }
   build_tables(&g_na_tables, opts->mode, opts->subset);
-  NA(cudaMemcpyAsync(S + kNaAgg, g_na_tables.ev, (kSparseCodes * kCodes + 5) * sizeof(AggEntry),
-                     cudaMemcpyHostToDevice, st));
+  fill_pair_tables(g_na_tables, rc.wplane, &g_na_ptab);
+  NA(cudaMemcpyAsync(S + kNaAgg, &g_na_ptab, sizeof(PairTables), cudaMemcpyHostToDevice, st));
   NA(cudaMemcpyAsync(S + kNaSite, g_na_tables.site, sizeof(g_na_tables.site), cudaMemcpyHostToDevice, st));
   unsigned *rqn = (unsigned *)(S + kNaRqn);
   unsigned long long *counters = (unsigned long long *)(S + kNaCounters);
@@ -2383,7 +2889,7 @@ int noalloc_run(const uint8_t *d_codes, long N, long L, const tn93g_opts *opts, 
   A.ccT = S + kNaCCT;
   A.ev_off = pa.ev_off;
   A.ev = pa.ev;
-  A.agg = (const AggEntry *)(S + kNaAgg);
+  A.tab = (const PairTables *)(S + kNaAgg);
   A.r0 = 0;
   A.r1 = N;
   A.ncols = N;
@@ -2395,6 +2901,7 @@ int noalloc_run(const uint8_t *d_codes, long N, long L, const tn93g_opts *opts, 
   A.replay_cap = (unsigned long long)kNaMaxN * kNaMaxN;
   A.counters = counters;
   A.logt = (const LogTable *)(S + kNaLog);
+  memset(&A.ex, 0, sizeof A.ex);  // raw distances only: no undecided list, no summary bounds
   NA(launch_pair(A, (N + 31) / 32, N, st));
   unsigned nq = 0;
   NA(cudaMemcpyAsync(&nq, rqn, sizeof nq, cudaMemcpyDeviceToHost, st));
@@ -2414,6 +2921,7 @@ int noalloc_run(const uint8_t *d_codes, long N, long L, const tn93g_opts *opts, 
     R.dist = d_dist;
     R.counters = counters;
     R.logt = A.logt;
+    R.ex = A.ex;
     replay_kernel<<<(unsigned)std::min<unsigned>(296, (nq + kWarps - 1) / kWarps), 256, 0, st>>>(R);
     NA(cudaGetLastError());
   }
@@ -2429,8 +2937,15 @@ extern "C" {
 int tn93g_pair_distances_noalloc(const uint8_t *d_codes, long N, long L, const tn93g_opts *opts, double *d_dist,
                                  void *stream)
 {
-  if (!d_codes || !opts || !d_dist || N <= 0 || L <= 0) return TN93G_EINVAL;
-  if (opts->mode < 0 || opts->mode > 4) return TN93G_EINVAL;
+  if (!d_codes || !opts || !d_dist || N <= 0 || L <= 0) {
+    snprintf(g_na_err, sizeof g_na_err, "invalid argument: a null pointer or a size <= 0 (N = %ld, L = %ld)", N, L);
+    return TN93G_EINVAL;
+  }
+  if (opts->mode < 0 || opts->mode > 4) {
+    snprintf(g_na_err, sizeof g_na_err, "invalid argument: ambiguity mode %d", opts->mode);
+    return TN93G_EINVAL;
+  }
+  g_na_err[0] = 0;
   std::lock_guard<std::mutex> g(g_na_mu);
   if (N > kNaMaxN || L > kNaMaxL) {
     snprintf(g_na_err, sizeof g_na_err,
@@ -2639,6 +3154,11 @@ struct tn93g_server {
   int tc16 = 0;
   long tc_NB = 0, tc_KS = 0;
   DevBuf ohimg, tcagg, tcerr;
+  // exactness: the undecided list (capacity und_cap entries; grown for an exact-sums pass), its count, the
+  // per-query bounds, the query of each column, the replay descriptor the resolver reads
+  DevBuf und, undn, amb, colunit, rdesc;
+  unsigned und_cap = 0;
+  uint32_t ref_max_ev = 0;  // most sparse events of a reference sequence (the packed sums need <= kPackedMaxEvents)
 };
 
 namespace {
@@ -2647,7 +3167,7 @@ constexpr long kServerTcChunk = 1024;  // query columns per tensor-core count la
 // opt-in to the count kernel's dynamic shared memory on the current device
 int tc_attr(tn93g_ctx *ctx)
 {
-  CU(cudaFuncSetAttribute(count_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+  CU(tc_attr_once());
   return TN93G_OK;
 }
 }  // namespace
@@ -2663,7 +3183,8 @@ void tn93g_server_destroy(tn93g_server *srv)
                     &srv->varcol, &srv->qcodes, &srv->counts, &srv->names, &srv->name_off, &srv->name_len,
                     &srv->dist, &srv->rq, &srv->rqn, &srv->counters, &srv->segcols, &srv->sbytes, &srv->soff,
                     &srv->slinks, &srv->sskip, &srv->smax, &srv->rsum, &srv->rw, &srv->hist, &srv->total,
-                    &srv->out, &srv->qout, &srv->qlinks, &srv->scantmp, &srv->ohimg, &srv->tcagg, &srv->tcerr};
+                    &srv->out, &srv->qout, &srv->qlinks, &srv->scantmp, &srv->ohimg, &srv->tcagg, &srv->tcerr,
+                    &srv->und, &srv->undn, &srv->amb, &srv->colunit, &srv->rdesc};
   for (DevBuf *b : bufs)
     if (b->p) {
       cudaFree(b->p);
@@ -2719,6 +3240,9 @@ int tn93g_server_create(tn93g_ctx *ctx, tn93g_server **out, const uint8_t *codes
   rc.min_distance = opts->min_distance;
   rc.resolve_fraction = opts->resolve_fraction;
   rc.min_overlap = opts->min_overlap;
+  rc.log_band = ctx->log_band;
+  rc.log_spread = ctx->log_spread;
+  rc.resolve_all = ctx->exact_sums;
   srv->Nref = N;
   srv->L = L;
   srv->W = (L + 63) / 64;
@@ -2781,7 +3305,10 @@ int tn93g_server_create(tn93g_ctx *ctx, tn93g_server **out, const uint8_t *codes
   SVC(cudaMemcpyAsync(evc.data(), srv->evcount.p, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   SVC(cudaStreamSynchronize(st));
   evo[0] = 0;
-  for (long i = 0; i < N; i++) evo[i + 1] = evo[i] + evc[i];
+  for (long i = 0; i < N; i++) {
+    evo[i + 1] = evo[i] + evc[i];
+    srv->ref_max_ev = std::max(srv->ref_max_ev, evc[i]);
+  }
   srv->ev_ref = evo[N];
   srv->ev_cap = srv->ev_ref + (size_t)max_batch_sequences * L;
   SV(ensure(ctx, srv->ev, std::max<size_t>(srv->ev_cap, 1) * sizeof(uint32_t)));
@@ -2794,10 +3321,10 @@ int tn93g_server_create(tn93g_ctx *ctx, tn93g_server **out, const uint8_t *codes
   }
   // tables of the server's mode
   build_tables(ctx->h_tab, opts->mode, opts->subset);
-  const size_t agg_n = kSparseCodes * kCodes + 5;
-  SV(ensure(ctx, srv->agg, agg_n * sizeof(AggEntry)));
+  fill_pair_tables(*ctx->h_tab, rc.wplane, ctx->h_ptab);
+  SV(ensure(ctx, srv->agg, sizeof(PairTables)));
   SV(ensure(ctx, srv->site, sizeof(ctx->h_tab->site)));
-  SVC(cudaMemcpyAsync(srv->agg.p, ctx->h_tab->ev, agg_n * sizeof(AggEntry), cudaMemcpyHostToDevice, st));
+  SVC(cudaMemcpyAsync(srv->agg.p, ctx->h_ptab, sizeof(PairTables), cudaMemcpyHostToDevice, st));
   SVC(cudaMemcpyAsync(srv->site.p, ctx->h_tab->site, sizeof(ctx->h_tab->site), cudaMemcpyHostToDevice, st));
   // names, name offsets and lengths, copy numbers of every sequence (the reference's now, the queries' per batch)
   size_t nbytes = 0;
@@ -2836,6 +3363,12 @@ int tn93g_server_create(tn93g_ctx *ctx, tn93g_server **out, const uint8_t *codes
     SV(ensure(ctx, srv->qout, (size_t)nq * 9 * sizeof(double)));
     SV(ensure(ctx, srv->qlinks, (size_t)nq * 2 * sizeof(long long)));
     SV(ensure(ctx, srv->scantmp, (2 * (nslot / kScanTile + 1) + 1) * sizeof(unsigned long long)));
+    srv->und_cap = (unsigned)std::min<size_t>(std::max<size_t>(4096, dslots / 64), 0xFFFFFFF0u);
+    SV(ensure(ctx, srv->und, (size_t)srv->und_cap * 2 * sizeof(unsigned long long)));
+    SV(ensure(ctx, srv->undn, sizeof(unsigned long long)));
+    SV(ensure(ctx, srv->amb, (size_t)nq * 4 * sizeof(unsigned long long)));
+    SV(ensure(ctx, srv->colunit, (size_t)max_batch_sequences * sizeof(int)));
+    SV(ensure(ctx, srv->rdesc, sizeof(ReplayArgs)));
     // a first text buffer (device and pinned host), so that early batches do not stall on growth
     const size_t text0 = 32u << 20;
     SV(ensure(ctx, srv->out, text0));
@@ -2850,7 +3383,7 @@ int tn93g_server_create(tn93g_ctx *ctx, tn93g_server **out, const uint8_t *codes
     srv->tc_KS = (L + kTcStageK - 1) / kTcStageK;
     srv->tc16 = 2 * L < 65536;
     const size_t img = (size_t)srv->tc_KS * srv->tc_NB * kTcBlockBytes;
-    const size_t agg = (size_t)7 * N * kServerTcChunk * (srv->tc16 ? 2 : 4);
+    const size_t agg = (size_t)N * kServerTcChunk * (srv->tc16 ? 16 : 32);
     if (ensure(ctx, srv->ohimg, img) == TN93G_OK && ensure(ctx, srv->tcagg, agg) == TN93G_OK &&
         ensure(ctx, srv->tcerr, sizeof(unsigned long long)) == TN93G_OK) {
       srv->tc = true;
@@ -2967,7 +3500,12 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
   CU(cudaMemcpyAsync(evc.data(), pa.evcount, Q * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   CU(cudaStreamSynchronize(st));
   evo[0] = (uint32_t)srv->ev_ref;
-  for (long k = 0; k < Q; k++) evo[k + 1] = evo[k] + evc[k];
+  uint32_t max_ev = srv->ref_max_ev;
+  for (long k = 0; k < Q; k++) {
+    evo[k + 1] = evo[k] + evc[k];
+    max_ev = std::max(max_ev, evc[k]);
+  }
+  rc.packed = max_ev <= (uint32_t)kPackedMaxEvents;
   CU(cudaMemcpyAsync((uint32_t *)srv->evoff.p + Nref, evo.data(), (Q + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice,
                      st));
   pa.ev_off = (const uint32_t *)srv->evoff.p + Nref;
@@ -2981,34 +3519,20 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
   // the cross run: rows = reference, columns = the batch's queries
   const size_t dslots = (size_t)Nref * Q;
   const size_t nslot = (size_t)nq * Nref;
-  CU(cudaMemsetAsync(srv->rqn.p, 0, sizeof(unsigned), st));
   CU(cudaMemsetAsync(srv->counters.p, 0, 4 * sizeof(unsigned long long), st));
-  CU(cudaMemsetAsync(srv->hist.p, 0, (size_t)nq * 3 * kHistBins * sizeof(unsigned long long), st));
+  CU(cudaMemsetAsync(srv->amb.p, 0, (size_t)nq * 4 * sizeof(unsigned long long), st));
   std::vector<long> segc(nq + 1);
   for (int q = 0; q <= nq; q++) segc[q] = Nref + qstart[q];
   CU(cudaMemcpyAsync(srv->segcols.p, segc.data(), (nq + 1) * sizeof(long), cudaMemcpyHostToDevice, st));
-  PairArgs A;
-  A.rc = rc;
-  A.planes = (const uint64_t *)srv->planes.p;
-  A.cc = (const uint8_t *)srv->cc.p;
-  A.ccT = (const uint8_t *)srv->ccT.p;
-  A.ev_off = (const uint32_t *)srv->evoff.p;
-  A.ev = (const uint32_t *)srv->ev.p;
-  A.agg = (const AggEntry *)srv->agg.p;
-  A.r0 = 0;
-  A.r1 = Nref;
-  A.ncols = Q;
-  A.colbase = Nref;
-  A.cstart = Nref;
-  A.dist = (double *)srv->dist.p;
-  A.replay_q = (unsigned long long *)srv->rq.p;
-  A.replay_n = (unsigned *)srv->rqn.p;
-  A.replay_cap = dslots;
-  A.counters = (unsigned long long *)srv->counters.p;
-  A.logt = ctx->d_logt;
+  {
+    std::vector<int> cu(Q);
+    for (int q = 0; q < nq; q++)
+      for (long k = qstart[q]; k < qstart[q + 1]; k++) cu[k] = q;
+    CU(cudaMemcpyAsync(srv->colunit.p, cu.data(), Q * sizeof(int), cudaMemcpyHostToDevice, st));
+  }
   if (srv->tc) {
     // the image blocks from the one shared by the reference's last rows and the first queries, through one zero
-    // block past the last query; then per chunk of query columns: counts on the tensor cores, then the pair kernel
+    // block past the last query
     const long b0 = Nref / 32, b1 = (Nref + Q + 31) / 32 + 1;
     const long nthr = (b1 - b0) * 32 * srv->tc_KS * (kTcStageK / 16);
     CU(cudaMemsetAsync(srv->tcerr.p, 0, sizeof(unsigned long long), st));
@@ -3017,63 +3541,104 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
                                                                   (b1 - b0) * 32);
     CU(cudaGetLastError());
     ctx->launches++;
-    for (long c0 = Nref; c0 < Nref + Q; c0 += kServerTcChunk) {
-      const long c1 = std::min(Nref + Q, c0 + kServerTcChunk);
-      TcArgs T;
-      T.onehot = (const uint8_t *)srv->ohimg.p;
-      T.NB = srv->tc_NB;
-      T.KS = srv->tc_KS;
-      T.N = Nref + Q;
-      T.n1 = Nref;
-      T.cross = true;
-      T.r0 = 0;
-      T.r1 = Nref;
-      T.ncols = kServerTcChunk;
-      T.colbase = c0;
-      T.cstart = c0 / kTcCols * kTcCols;
-      T.cend = c1;
-      T.agg = srv->tcagg.p;
-      T.agg16 = srv->tc16;
-      T.err = (unsigned long long *)srv->tcerr.p;
-      const dim3 g((unsigned)((c1 - T.cstart + kTcCols - 1) / kTcCols), (unsigned)((Nref + kTcRows - 1) / kTcRows));
-      count_tc_kernel<<<g, 128, kTcSmem, st>>>(T);
-      CU(cudaGetLastError());
-      PairArgs AC = A;
-      AC.tcagg = srv->tcagg.p;
-      AC.tcplane = (size_t)Nref * kServerTcChunk;
-      AC.tc16 = srv->tc16;
-      AC.tcncols = kServerTcChunk;
-      AC.tccolbase = c0;
-      AC.cstart = c0;
-      CU(launch_pair(AC, (c1 - c0 + 31) / 32, Nref, st));
-      ctx->launches += 2;
-    }
-  } else {
-    CU(launch_pair(A, (Q + 31) / 32, Nref, st));
-    ctx->launches++;
   }
-  CU(cudaEventRecord(E[2], st));
   ReplayArgs R;
-  R.rc = rc;
-  R.cc = A.cc;
-  R.planes = A.planes;
-  R.site = (const SiteEntry *)srv->site.p;
-  R.q = A.replay_q;
-  R.qn = A.replay_n;
-  R.qcap = dslots;
-  R.r0 = 0;
-  R.ncols = Q;
-  R.colbase = Nref;
-  R.dist = A.dist;
-  R.counters = A.counters;
-  R.logt = ctx->d_logt;
-  replay_kernel<<<2 * ctx->sms, 256, 0, st>>>(R);
-  CU(cudaGetLastError());
-  ctx->launches++;
-  CU(cudaEventRecord(E[3], st));
+  // pair stage (and the site-order replay) of the whole batch; resolve_all: an exact-sums pass
+  auto enqueue_pairs = [&](bool resolve_all) -> int {
+    RunConsts rcp = rc;
+    rcp.resolve_all = rc.resolve_all || resolve_all;
+    CU(cudaMemsetAsync(srv->rqn.p, 0, sizeof(unsigned), st));
+    CU(cudaMemsetAsync(srv->undn.p, 0, sizeof(unsigned long long), st));
+    ExactSink ex;
+    ex.und_list = (unsigned long long *)srv->und.p;
+    ex.und_n = (unsigned *)srv->undn.p;
+    ex.und_cap = srv->und_cap;
+    ex.und_k = 0;
+    ex.amb = resolve_all ? nullptr : (unsigned long long *)srv->amb.p;
+    ex.counts = (const long *)srv->counts.p;
+    ex.colunit = (const int *)srv->colunit.p;
+    PairArgs A;
+    A.rc = rcp;
+    A.planes = (const uint64_t *)srv->planes.p;
+    A.cc = (const uint8_t *)srv->cc.p;
+    A.ccT = (const uint8_t *)srv->ccT.p;
+    A.ev_off = (const uint32_t *)srv->evoff.p;
+    A.ev = (const uint32_t *)srv->ev.p;
+    A.tab = (const PairTables *)srv->agg.p;
+    A.r0 = 0;
+    A.r1 = Nref;
+    A.ncols = Q;
+    A.colbase = Nref;
+    A.cstart = Nref;
+    A.dist = (double *)srv->dist.p;
+    A.replay_q = (unsigned long long *)srv->rq.p;
+    A.replay_n = (unsigned *)srv->rqn.p;
+    A.replay_cap = dslots;
+    A.counters = (unsigned long long *)srv->counters.p;
+    A.logt = ctx->d_logt;
+    A.ex = ex;
+    if (srv->tc) {
+      // per chunk of query columns: counts on the tensor cores, then the pair kernel
+      for (long c0 = Nref; c0 < Nref + Q; c0 += kServerTcChunk) {
+        const long c1 = std::min(Nref + Q, c0 + kServerTcChunk);
+        TcArgs T;
+        T.onehot = (const uint8_t *)srv->ohimg.p;
+        T.NB = srv->tc_NB;
+        T.KS = srv->tc_KS;
+        T.N = Nref + Q;
+        T.n1 = Nref;
+        T.cross = true;
+        T.r0 = 0;
+        T.r1 = Nref;
+        T.ncols = kServerTcChunk;
+        T.colbase = c0;
+        T.cstart = c0 / kTcCols * kTcCols;
+        T.cend = c1;
+        T.agg = srv->tcagg.p;
+        T.agg16 = srv->tc16;
+        T.err = (unsigned long long *)srv->tcerr.p;
+        T.wait_ns = ctx->wait_ns;
+        T.skip_fill_block = -1;
+        const dim3 g((unsigned)((c1 - T.cstart + kTcCols - 1) / kTcCols), (unsigned)((Nref + kTcRows - 1) / kTcRows));
+        count_tc_kernel<<<g, 128, kTcSmem, st>>>(T);
+        CU(cudaGetLastError());
+        PairArgs AC = A;
+        AC.tcagg = srv->tcagg.p;
+        AC.tc16 = srv->tc16;
+        AC.tcncols = kServerTcChunk;
+        AC.tccolbase = c0;
+        AC.cstart = c0;
+        CU(launch_pair(AC, (c1 - c0 + 31) / 32, Nref, st));
+        ctx->launches += 2;
+      }
+    } else {
+      CU(launch_pair(A, (Q + 31) / 32, Nref, st));
+      ctx->launches++;
+    }
+    CU(cudaEventRecord(E[2], st));
+    R.rc = rcp;
+    R.cc = A.cc;
+    R.planes = A.planes;
+    R.site = (const SiteEntry *)srv->site.p;
+    R.q = A.replay_q;
+    R.qn = A.replay_n;
+    R.qcap = dslots;
+    R.r0 = 0;
+    R.ncols = Q;
+    R.colbase = Nref;
+    R.dist = A.dist;
+    R.counters = A.counters;
+    R.logt = ctx->d_logt;
+    R.ex = ex;
+    replay_kernel<<<2 * ctx->sms, 256, 0, st>>>(R);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    CU(cudaEventRecord(E[3], st));
+    return TN93G_OK;
+  };
   RowArgs RA;
   RA.rc = rc;
-  RA.dist = A.dist;
+  RA.dist = (const double *)srv->dist.p;
   RA.r0 = 0;
   RA.r1 = Nref;
   RA.ncols = Q;
@@ -3097,31 +3662,98 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
   RA.err = (unsigned long long *)srv->counters.p + 3;
   RA.out = nullptr;
   const dim3 g2((unsigned)((Nref + 255) / 256), (unsigned)nq);
-  qstats_kernel<<<g2, 256, 0, st>>>(RA);
-  CU(cudaGetLastError());
-  ctx->launches++;
-  CU(launch_scan(RA.seg_bytes, (unsigned long long *)RA.seg_off, (long)nslot, (unsigned long long *)srv->total.p,
-                 (unsigned long long *)srv->scantmp.p, st));
-  ctx->launches++;
-  query_reduce_kernel<<<(unsigned)nq, 256, 0, st>>>(RA, nq, (double *)srv->qout.p, (long long *)srv->qlinks.p);
-  CU(cudaGetLastError());
-  ctx->launches++;
-  CU(cudaEventRecord(E[4], st));
-  unsigned long long total = 0;
+  unsigned long long total = 0, und = 0;
   std::vector<double> qo((size_t)nq * 9);
   std::vector<long long> ql((size_t)nq * 2);
-  std::vector<unsigned long long> qoff(nq + 1);
-  CU(cudaMemcpyAsync(&total, srv->total.p, sizeof total, cudaMemcpyDeviceToHost, st));
-  CU(cudaMemcpyAsync(qo.data(), srv->qout.p, qo.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
-  CU(cudaMemcpyAsync(ql.data(), srv->qlinks.p, ql.size() * sizeof(long long), cudaMemcpyDeviceToHost, st));
-  for (int q = 0; q < nq; q++)
-    CU(cudaMemcpyAsync(&qoff[q], (unsigned long long *)srv->soff.p + (size_t)q * Nref, sizeof(unsigned long long),
-                       cudaMemcpyDeviceToHost, st));
-  std::vector<unsigned long long> hist((size_t)nq * 3 * kHistBins);
-  CU(cudaMemcpyAsync(hist.data(), srv->hist.p, hist.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  std::vector<unsigned long long> qoff(nq + 1), hist((size_t)nq * 3 * kHistBins), ambw((size_t)nq * 4);
   unsigned long long counters[4];
-  CU(cudaMemcpyAsync(counters, srv->counters.p, sizeof counters, cudaMemcpyDeviceToHost, st));
-  CU(cudaStreamSynchronize(st));
+  // row stage (per-query statistics and row sums, scan, per-query reduction) and its results on the host
+  auto rows_and_read = [&]() -> int {
+    CU(cudaMemsetAsync(srv->hist.p, 0, (size_t)nq * 3 * kHistBins * sizeof(unsigned long long), st));
+    qstats_kernel<<<g2, 256, 0, st>>>(RA);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    CU(launch_scan(RA.seg_bytes, (unsigned long long *)RA.seg_off, (long)nslot, (unsigned long long *)srv->total.p,
+                   (unsigned long long *)srv->scantmp.p, st));
+    ctx->launches++;
+    query_reduce_kernel<<<(unsigned)nq, 256, 0, st>>>(RA, nq, (double *)srv->qout.p, (long long *)srv->qlinks.p);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    CU(cudaEventRecord(E[4], st));
+    CU(cudaMemcpyAsync(&total, srv->total.p, sizeof total, cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(qo.data(), srv->qout.p, qo.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(ql.data(), srv->qlinks.p, ql.size() * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    for (int q = 0; q < nq; q++)
+      CU(cudaMemcpyAsync(&qoff[q], (unsigned long long *)srv->soff.p + (size_t)q * Nref, sizeof(unsigned long long),
+                         cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(hist.data(), srv->hist.p, hist.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       st));
+    CU(cudaMemcpyAsync(counters, srv->counters.p, sizeof counters, cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(&und, srv->undn.p, sizeof und, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    return TN93G_OK;
+  };
+  // finishes the listed undecided pairs with the C library's logarithms and runs the row stage again
+  long resolved = 0;
+  auto resolve_and_reread = [&]() -> int {
+    if (und > srv->und_cap) {
+      ctx->err = "more undecided pairs in a batch than its list holds";
+      return TN93G_EUNDECIDED;
+    }
+    CU(cudaMemcpyAsync(srv->rdesc.p, &R, sizeof R, cudaMemcpyHostToDevice, st));
+    TRY(resolve_listed(ctx, (const ReplayArgs *)srv->rdesc.p, (const unsigned long long *)srv->und.p, (unsigned)und,
+                       st));
+    resolved += (long)und;
+    return rows_and_read();
+  };
+  TRY(enqueue_pairs(false));
+  TRY(rows_and_read());
+  if (srv->tc) {
+    unsigned long long tcerr = 0;
+    CU(cudaMemcpy(&tcerr, srv->tcerr.p, sizeof tcerr, cudaMemcpyDeviceToHost));
+    if (tcerr) {
+      ctx->err = "the tensor-core count kernel timed out waiting for its pipeline";
+      return TN93G_ETIMEOUT;
+    }
+  }
+  const long undecided0 = (long)counters[1], ambiguous0 = (long)counters[0];
+  if (und) TRY(resolve_and_reread());
+  // per query: the JSON numbers certain for every rounding of the C library's log, or an exact-sums pass
+  CU(cudaMemcpy(ambw.data(), srv->amb.p, ambw.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  std::vector<tn93g_summary> S(nq);
+  auto fill_summaries = [&]() {
+    for (int q = 0; q < nq; q++) {
+      tn93g_summary &X = S[q];
+      memset(&X, 0, sizeof X);
+      X.pairwise = (unsigned long)Nref * (unsigned long)queries[q].n;
+      X.links = (long)ql[q * 2];
+      X.skipped = (long)ql[q * 2 + 1];
+      for (int k = 0; k < 3; k++) {
+        X.max[k] = qo[q * 9 + k];
+        X.mean[k] = qo[q * 9 + 3 + k];
+        X.weighted[k] = qo[q * 9 + 6 + k];
+        for (int b = 0; b < kHistBins; b++) X.hist[k][b] = hist[((size_t)q * 3 + k) * kHistBins + b];
+      }
+    }
+  };
+  fill_summaries();
+  bool repass = false;
+  for (int q = 0; q < nq && !rc.resolve_all; q++) {
+    amb_bounds(&ambw[(size_t)q * 4], S[q].amb_bounds[0]);
+    if (!summary_certified(&S[q], S[q].amb_bounds, Nref + queries[q].n + 2, 0)) repass = true;
+  }
+  if (repass) {
+    // every pair with an ambiguous logarithm finished with the C library's log (the list must hold all of them)
+    const unsigned cap = (unsigned)std::min<size_t>(dslots, 0xFFFFFFF0u);
+    if (cap > srv->und_cap) {
+      TRY(ensure(ctx, srv->und, (size_t)cap * 2 * sizeof(unsigned long long)));
+      srv->und_cap = cap;
+    }
+    TRY(enqueue_pairs(true));
+    TRY(rows_and_read());
+    if (und) TRY(resolve_and_reread());
+    fill_summaries();
+  }
   qoff[nq] = total;
   if (rc.emit && total) {
     if (srv->out.n < total) TRY(ensure(ctx, srv->out, total + total / 2));
@@ -3169,31 +3801,17 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
     ctx->err = "internal error: a query's text did not match its counted length";
     return TN93G_ECUDA;
   }
-  if (srv->tc) {
-    unsigned long long tcerr = 0;
-    CU(cudaMemcpy(&tcerr, srv->tcerr.p, sizeof tcerr, cudaMemcpyDeviceToHost));
-    if (tcerr) {
-      ctx->err = "the tensor-core count kernel timed out waiting for its pipeline";
-      return TN93G_ETIMEOUT;
-    }
-  }
   for (int q = 0; q < nq; q++) {
-    tn93g_summary &S = sums[q];
-    memset(&S, 0, sizeof S);
-    S.pairwise = (unsigned long)Nref * (unsigned long)queries[q].n;
-    S.links = (long)ql[q * 2];
-    S.skipped = (long)ql[q * 2 + 1];
-    for (int k = 0; k < 3; k++) {
-      S.max[k] = qo[q * 9 + k];
-      S.mean[k] = qo[q * 9 + 3 + k];
-      S.weighted[k] = qo[q * 9 + 6 + k];
-      for (int b = 0; b < kHistBins; b++) S.hist[k][b] = hist[((size_t)q * 3 + k) * kHistBins + b];
-    }
-    S.output_bytes = qoff[q + 1] - qoff[q];
+    tn93g_summary &X = sums[q];
+    X = S[q];
+    if (repass) memset(X.amb_bounds, 0, sizeof X.amb_bounds);
+    X.output_bytes = qoff[q + 1] - qoff[q];
     if (q == 0) {
-      S.pairs_replayed = (long)counters[2];
-      S.logs_ambiguous = (long)counters[0];
-      S.undecided = (long)counters[1];
+      X.pairs_replayed = (long)counters[2];
+      X.logs_ambiguous = ambiguous0;
+      X.logs_resolved = resolved;
+      X.undecided = undecided0 - std::min<long>(undecided0, resolved);
+      X.sums_repass = repass ? 1 : 0;
     }
     if (rc.emit && sink && sink(user, q, (const char *)srv->pin + qoff[q], (size_t)(qoff[q + 1] - qoff[q])))
       return TN93G_ESINK;
@@ -3215,9 +3833,9 @@ enum BatchBuf {
   BB_NAMES, BB_NAMEOFF, BB_NAMELEN, BB_COUNTS, BB_DIST, BB_RQ, BB_RQN, BB_COUNTERS, BB_PDESC, BB_RDESC, BB_ROWDESC,
   BB_TILES, BB_NEXT, BB_BLOCKS, BB_SBYTES, BB_SOFF, BB_SLINKS, BB_SSKIP, BB_SMAX, BB_RSUM, BB_RW, BB_HIST, BB_TOTAL,
   BB_SCANTMP, BB_RED, BB_REDC, BB_FIRST, BB_FIRSTIDX, BB_OUT, BB_OH, BB_TCAGG, BB_TCDESC, BB_TCTILES, BB_TCERR,
-  BB_COUNT
+  BB_UND, BB_UNDN, BB_AMB, BB_COUNT
 };
-static_assert(BB_COUNT <= 48, "batch buffer table");
+static_assert(BB_COUNT <= kBatchBufs, "batch buffer table");
 
 __global__ void gather_u64_kernel(const unsigned long long *src, const long *idx, unsigned long long *dst, int n)
 {
@@ -3229,20 +3847,26 @@ template <int MINB>
 cudaError_t launch_pair_batch_t(int sms, bool wplane, bool gapmm, const PairArgs *descs, const BatchTile *tiles,
                                 int ntiles, unsigned *next, cudaStream_t st)
 {
+  static PerDevice attr;
+  const cudaError_t e = attr.once([] {
+    cudaError_t r;
+    if ((r = cudaFuncSetAttribute(pair_batch_kernel<true, true, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kPairSmem)) != cudaSuccess)
+      return r;
+    if ((r = cudaFuncSetAttribute(pair_batch_kernel<true, false, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kPairSmem)) != cudaSuccess)
+      return r;
+    return cudaFuncSetAttribute(pair_batch_kernel<false, false, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kPairSmem);
+  });
+  if (e != cudaSuccess) return e;
   const dim3 g((unsigned)(sms * MINB));
-  if (gapmm) {
-    cudaFuncSetAttribute(pair_batch_kernel<true, true, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)kPairSmem);
+  if (gapmm)
     pair_batch_kernel<true, true, MINB><<<g, 256, kPairSmem, st>>>(descs, tiles, ntiles, next);
-  } else if (wplane) {
-    cudaFuncSetAttribute(pair_batch_kernel<true, false, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)kPairSmem);
+  else if (wplane)
     pair_batch_kernel<true, false, MINB><<<g, 256, kPairSmem, st>>>(descs, tiles, ntiles, next);
-  } else {
-    cudaFuncSetAttribute(pair_batch_kernel<false, false, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)kPairSmem);
+  else
     pair_batch_kernel<false, false, MINB><<<g, 256, kPairSmem, st>>>(descs, tiles, ntiles, next);
-  }
   return cudaGetLastError();
 }
 
@@ -3347,6 +3971,9 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
     rc.min_distance = o->min_distance;
     rc.resolve_fraction = o->resolve_fraction;
     rc.min_overlap = o->min_overlap;
+    rc.log_band = ctx->log_band;
+    rc.log_spread = ctx->log_spread;
+    rc.resolve_all = ctx->exact_sums;
     for (long p = 0; p < L; p++) {
       const uint32_t m = seen[seen_off[k] + p];
       if (m && !(m & (m - 1)) && m < 16) {
@@ -3411,11 +4038,14 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
   CU(cudaStreamSynchronize(st));
   size_t nev = 0;
   for (int k = 0; k < K; k++) {
+    uint32_t max_ev = 0;
     for (long i = 0; i < alns[k].n; i++) {
       evo[evo_off[k] + i] = (uint32_t)nev;
       nev += evc[row_base[k] + i];
+      max_ev = std::max(max_ev, evc[row_base[k] + i]);
     }
     evo[evo_off[k] + alns[k].n] = (uint32_t)nev;
+    RC[k].packed = max_ev <= (uint32_t)kPackedMaxEvents;
   }
   if (nev >= (1ull << 32)) return TN93G_ETOOBIG;
   TRY(ensure(ctx, bb[BB_EV], std::max<size_t>(nev, 1) * sizeof(uint32_t)));
@@ -3428,33 +4058,40 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
       ctx->launches++;
     }
   }
-  // tables: one copy per distinct (mode, ambiguity subset)
-  const size_t agg_n = kSparseCodes * kCodes + 5;
-  std::vector<int> tab_of(K);
-  std::vector<std::pair<int, std::string>> keys;
-  std::vector<AggEntry> h_agg;
+  // tables: one copy per distinct (mode, ambiguity subset, N plane); the site tables per (mode, subset)
+  std::vector<int> tab_of(K), site_of(K);
+  std::vector<std::pair<int, std::string>> keys, site_keys;
+  std::vector<PairTables> h_agg;
   std::vector<SiteEntry> h_site;
   for (int k = 0; k < K; k++) {
     const std::string sub((const char *)opts[k].subset, sizeof opts[k].subset);
-    const std::pair<int, std::string> key(opts[k].mode, opts[k].mode == TN93G_SUBSET ? sub : std::string());
-    int t = -1;
+    const std::string sk = opts[k].mode == TN93G_SUBSET ? sub : std::string();
+    const std::pair<int, std::string> key(opts[k].mode * 2 + (RC[k].wplane ? 1 : 0), sk), skey(opts[k].mode, sk);
+    int t = -1, u = -1;
     for (size_t q = 0; q < keys.size(); q++)
       if (keys[q] == key) t = (int)q;
+    for (size_t q = 0; q < site_keys.size(); q++)
+      if (site_keys[q] == skey) u = (int)q;
+    if (t < 0 || u < 0) build_tables(ctx->h_tab, opts[k].mode, opts[k].subset);
     if (t < 0) {
-      build_tables(ctx->h_tab, opts[k].mode, opts[k].subset);
-      const AggEntry *tab = reinterpret_cast<const AggEntry *>(ctx->h_tab);  // ev, ew, eww (contiguous)
-      h_agg.insert(h_agg.end(), tab, tab + agg_n);
-      const SiteEntry *se = &ctx->h_tab->site[0][0];
-      h_site.insert(h_site.end(), se, se + sizeof(ctx->h_tab->site) / sizeof(SiteEntry));
+      h_agg.emplace_back();
+      fill_pair_tables(*ctx->h_tab, RC[k].wplane, &h_agg.back());
       t = (int)keys.size();
       keys.push_back(key);
     }
+    if (u < 0) {
+      const SiteEntry *se = &ctx->h_tab->site[0][0];
+      h_site.insert(h_site.end(), se, se + sizeof(ctx->h_tab->site) / sizeof(SiteEntry));
+      u = (int)site_keys.size();
+      site_keys.push_back(skey);
+    }
     tab_of[k] = t;
+    site_of[k] = u;
   }
   const size_t site_n = sizeof(ctx->h_tab->site) / sizeof(SiteEntry);
-  TRY(ensure(ctx, bb[BB_AGG], h_agg.size() * sizeof(AggEntry)));
+  TRY(ensure(ctx, bb[BB_AGG], h_agg.size() * sizeof(PairTables)));
   TRY(ensure(ctx, bb[BB_SITE], h_site.size() * sizeof(SiteEntry)));
-  CU(cudaMemcpyAsync(bb[BB_AGG].p, h_agg.data(), h_agg.size() * sizeof(AggEntry), cudaMemcpyHostToDevice, st));
+  CU(cudaMemcpyAsync(bb[BB_AGG].p, h_agg.data(), h_agg.size() * sizeof(PairTables), cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync(bb[BB_SITE].p, h_site.data(), h_site.size() * sizeof(SiteEntry), cudaMemcpyHostToDevice, st));
   CU(cudaEventRecord(E[1], st));
   //------------------------------------------------------------------ pair stage
@@ -3474,6 +4111,13 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
   TRY(ensure(ctx, bb[BB_COUNTERS], (size_t)K * 4 * sizeof(unsigned long long)));
   CU(cudaMemsetAsync(bb[BB_RQN].p, 0, K * sizeof(unsigned), st));
   CU(cudaMemsetAsync(bb[BB_COUNTERS].p, 0, (size_t)K * 4 * sizeof(unsigned long long), st));
+  // one undecided list for every alignment (entries carry the alignment), per-alignment summary bounds
+  const unsigned und_cap = (unsigned)std::min<size_t>(std::max<size_t>(4096, q_off[K] / 64), 0xFFFFFFF0u);
+  TRY(ensure(ctx, bb[BB_UND], (size_t)und_cap * 2 * sizeof(unsigned long long)));
+  TRY(ensure(ctx, bb[BB_UNDN], sizeof(unsigned long long)));
+  TRY(ensure(ctx, bb[BB_AMB], (size_t)K * 4 * sizeof(unsigned long long)));
+  CU(cudaMemsetAsync(bb[BB_UNDN].p, 0, sizeof(unsigned long long), st));
+  CU(cudaMemsetAsync(bb[BB_AMB].p, 0, (size_t)K * 4 * sizeof(unsigned long long), st));
   std::vector<PairArgs> PD(K);
   std::vector<ReplayArgs> RD(K);
   for (int k = 0; k < K; k++) {
@@ -3485,7 +4129,7 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
     A.ccT = (const uint8_t *)bb[BB_CCT].p + cct_off[k];
     A.ev_off = (const uint32_t *)bb[BB_EVOFF].p + evo_off[k];
     A.ev = (const uint32_t *)bb[BB_EV].p;
-    A.agg = (const AggEntry *)bb[BB_AGG].p + (size_t)tab_of[k] * agg_n;
+    A.tab = (const PairTables *)bb[BB_AGG].p + tab_of[k];
     A.r0 = 0;
     A.r1 = alns[k].n;
     A.ncols = alns[k].n;
@@ -3497,12 +4141,19 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
     A.replay_cap = q_off[k + 1] - q_off[k];
     A.counters = (unsigned long long *)bb[BB_COUNTERS].p + 4 * k;
     A.logt = ctx->d_logt;
+    A.ex.und_list = (unsigned long long *)bb[BB_UND].p;
+    A.ex.und_n = (unsigned *)bb[BB_UNDN].p;
+    A.ex.und_cap = und_cap;
+    A.ex.und_k = k;
+    A.ex.amb = (unsigned long long *)bb[BB_AMB].p + 4 * k;
+    A.ex.counts = (const long *)bb[BB_COUNTS].p + row_base[k];
+    A.ex.colunit = nullptr;
     ReplayArgs &R = RD[k];
     memset(&R, 0, sizeof R);
     R.rc = RC[k];
     R.cc = A.cc;
     R.planes = A.planes;
-    R.site = (const SiteEntry *)bb[BB_SITE].p + (size_t)tab_of[k] * site_n;
+    R.site = (const SiteEntry *)bb[BB_SITE].p + (size_t)site_of[k] * site_n;
     R.q = A.replay_q;
     R.qn = A.replay_n;
     R.qcap = A.replay_cap;
@@ -3512,6 +4163,7 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
     R.dist = A.dist;
     R.counters = A.counters;
     R.logt = ctx->d_logt;
+    R.ex = A.ex;
   }
   std::vector<int> order(K);
   for (int k = 0; k < K; k++) order[k] = k;
@@ -3529,8 +4181,8 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
       const long NB = (N + 31) / 32 + 1, KS = (RC[k].Lc + kTcStageK - 1) / kTcStageK;
       oh_off[k + 1] = oh_off[k] + (on ? (size_t)KS * NB * kTcBlockBytes : 0);
       // byte offsets, each alignment's block 16-byte aligned
-      const size_t esz = 2 * RC[k].Lc < 65536 ? sizeof(uint16_t) : sizeof(int32_t);
-      ag_off[k + 1] = ag_off[k] + (on ? ((size_t)7 * N * N * esz + 15) / 16 * 16 : 0);
+      const size_t rec = 2 * RC[k].Lc < 65536 ? 16 : 32;  // bytes of a pair's record
+      ag_off[k + 1] = ag_off[k] + (on ? (size_t)N * N * rec : 0);
       TcArgs &T = TD[k];
       memset(&T, 0, sizeof T);
       T.NB = NB;
@@ -3556,6 +4208,8 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
       T.agg = (char *)bb[BB_TCAGG].p + ag_off[k];
       T.agg16 = 2 * RC[k].Lc < 65536;
       T.err = (unsigned long long *)bb[BB_TCERR].p;
+      T.wait_ns = ctx->wait_ns;
+      T.skip_fill_block = -1;
       const long nthr = T.NB * 32 * T.KS * (kTcStageK / 16);
       onehot_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>(PA[k].cc, T.N, RC[k].Lc, T.NB, T.KS,
                                                                     (uint8_t *)bb[BB_OH].p + oh_off[k], 0, T.NB * 32);
@@ -3564,7 +4218,6 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
       for (long i0 = 0; i0 < T.N - 1; i0 += kTcRows)
         for (long j0 = (i0 + 1) / kTcCols * kTcCols; j0 < T.N; j0 += kTcCols) tct.push_back(make_int4(k, (int)i0, (int)j0, 0));
       PD[k].tcagg = T.agg;
-      PD[k].tcplane = (size_t)T.N * T.N;
       PD[k].tc16 = T.agg16;
     }
     if (!tct.empty()) {
@@ -3572,9 +4225,10 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
       TRY(ensure(ctx, bb[BB_TCTILES], tct.size() * sizeof(int4)));
       CU(cudaMemcpyAsync(bb[BB_TCDESC].p, TD.data(), K * sizeof(TcArgs), cudaMemcpyHostToDevice, st));
       CU(cudaMemcpyAsync(bb[BB_TCTILES].p, tct.data(), tct.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
-      static std::atomic<unsigned long long> attr{0};
-      if (first_on_device(attr))
-        CU(cudaFuncSetAttribute(count_tc_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+      static PerDevice attr;
+      CU(attr.once([] {
+        return cudaFuncSetAttribute(count_tc_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+      }));
       count_tc_batch_kernel<<<(unsigned)tct.size(), 128, kTcSmem, st>>>((const TcArgs *)bb[BB_TCDESC].p,
                                                                       (const int4 *)bb[BB_TCTILES].p);
       CU(cudaGetLastError());
@@ -3687,31 +4341,50 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
   CU(cudaMemcpyAsync(bb[BB_FIRSTIDX].p, first_idx.data(), K * sizeof(long), cudaMemcpyHostToDevice, st));
   const RowArgs *rd = (const RowArgs *)bb[BB_ROWDESC].p;
   const int2 *bp = (const int2 *)bb[BB_BLOCKS].p;
-  stats_batch_kernel<<<dim3((unsigned)blocks.size(), (unsigned)segmax), 256, 0, st>>>(rd, bp);
-  CU(cudaGetLastError());
-  sum_batch_kernel<<<(unsigned)blocks.size(), 256, 0, st>>>(rd, bp);
-  CU(cudaGetLastError());
-  CU(launch_scan((const unsigned long long *)bb[BB_SBYTES].p, (unsigned long long *)bb[BB_SOFF].p, (long)NS,
-                 (unsigned long long *)bb[BB_TOTAL].p, (unsigned long long *)bb[BB_SCANTMP].p, st));
-  aln_reduce_kernel<<<K, 256, 0, st>>>(rd, (double *)bb[BB_RED].p, (long long *)bb[BB_REDC].p);
-  CU(cudaGetLastError());
-  gather_u64_kernel<<<(K + 255) / 256, 256, 0, st>>>((const unsigned long long *)bb[BB_SOFF].p,
-                                                     (const long *)bb[BB_FIRSTIDX].p,
-                                                     (unsigned long long *)bb[BB_FIRST].p, K);
-  CU(cudaGetLastError());
-  ctx->launches += 5;
-  CU(cudaEventRecord(E[4], st));
-  unsigned long long total = 0;
+  unsigned long long total = 0, und = 0;
   std::vector<double> red((size_t)K * 3);
   std::vector<long long> redc((size_t)K * 2);
   std::vector<unsigned long long> first(K + 1), hist((size_t)K * 3 * kHistBins), counters((size_t)K * 4);
-  CU(cudaMemcpyAsync(&total, bb[BB_TOTAL].p, sizeof total, cudaMemcpyDeviceToHost, st));
-  CU(cudaMemcpyAsync(red.data(), bb[BB_RED].p, red.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
-  CU(cudaMemcpyAsync(redc.data(), bb[BB_REDC].p, redc.size() * sizeof(long long), cudaMemcpyDeviceToHost, st));
-  CU(cudaMemcpyAsync(first.data(), bb[BB_FIRST].p, K * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
-  CU(cudaMemcpyAsync(hist.data(), bb[BB_HIST].p, hist.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                     st));
-  CU(cudaStreamSynchronize(st));
+  auto rows_and_read = [&]() -> int {
+    CU(cudaMemsetAsync(bb[BB_HIST].p, 0, (size_t)K * 3 * kHistBins * sizeof(unsigned long long), st));
+    stats_batch_kernel<<<dim3((unsigned)blocks.size(), (unsigned)segmax), 256, 0, st>>>(rd, bp);
+    CU(cudaGetLastError());
+    sum_batch_kernel<<<(unsigned)blocks.size(), 256, 0, st>>>(rd, bp);
+    CU(cudaGetLastError());
+    CU(launch_scan((const unsigned long long *)bb[BB_SBYTES].p, (unsigned long long *)bb[BB_SOFF].p, (long)NS,
+                   (unsigned long long *)bb[BB_TOTAL].p, (unsigned long long *)bb[BB_SCANTMP].p, st));
+    aln_reduce_kernel<<<K, 256, 0, st>>>(rd, (double *)bb[BB_RED].p, (long long *)bb[BB_REDC].p);
+    CU(cudaGetLastError());
+    gather_u64_kernel<<<(K + 255) / 256, 256, 0, st>>>((const unsigned long long *)bb[BB_SOFF].p,
+                                                       (const long *)bb[BB_FIRSTIDX].p,
+                                                       (unsigned long long *)bb[BB_FIRST].p, K);
+    CU(cudaGetLastError());
+    ctx->launches += 5;
+    CU(cudaEventRecord(E[4], st));
+    CU(cudaMemcpyAsync(&total, bb[BB_TOTAL].p, sizeof total, cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(red.data(), bb[BB_RED].p, red.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(redc.data(), bb[BB_REDC].p, redc.size() * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(first.data(), bb[BB_FIRST].p, K * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(hist.data(), bb[BB_HIST].p, hist.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       st));
+    CU(cudaMemcpyAsync(&und, bb[BB_UNDN].p, sizeof und, cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    return TN93G_OK;
+  };
+  TRY(rows_and_read());
+  long resolved = 0;
+  if (und) {
+    // pairs whose bytes or decisions depend on the C library's rounding of a logarithm: finished with its
+    // logarithms, then the row stage runs again
+    if (und > und_cap) {
+      ctx->err = "more undecided pairs in a batch than its list holds";
+      return TN93G_EUNDECIDED;
+    }
+    TRY(resolve_listed(ctx, (const ReplayArgs *)bb[BB_RDESC].p, (const unsigned long long *)bb[BB_UND].p,
+                       (unsigned)und, st));
+    resolved = (long)und;
+    TRY(rows_and_read());
+  }
   first[K] = total;
   bool any_emit = false;
   for (int k = 0; k < K; k++) any_emit |= RC[k].emit;
@@ -3762,9 +4435,37 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
     for (int q = 0; q < 3; q++)
       for (int b = 0; b < kHistBins; b++) S.hist[q][b] = hist[((size_t)k * 3 + q) * kHistBins + b];
     S.logs_ambiguous = (long)counters[4 * k];
-    S.undecided = (long)counters[4 * k + 1];
+    S.logs_resolved = (long)counters[4 * k + 1];  // every listed pair was finished (resolved = the list's total)
+    S.undecided = 0;
     S.pairs_replayed = (long)counters[4 * k + 2];
     S.output_bytes = RC[k].emit ? first[k + 1] - first[k] : 0;
+  }
+  (void)resolved;
+  // Per alignment: the JSON numbers certain for every rounding of the C library's log, or the alignment runs
+  // again alone through tn93g_run's path, whose exact-sums pass gives its maximum and mean (its text and counts
+  // are certified pair by pair already).
+  {
+    std::vector<unsigned long long> ambw((size_t)K * 4);
+    CU(cudaMemcpy(ambw.data(), bb[BB_AMB].p, ambw.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < K; k++) {
+      tn93g_summary &S = sums[k];
+      amb_bounds(&ambw[(size_t)k * 4], S.amb_bounds[0]);
+      if (summary_certified(&S, S.amb_bounds, 2 * alns[k].n + 2, 0)) continue;
+      const tn93g_alignment &A = alns[k];
+      tn93g_set *set = nullptr;
+      TRY(tn93g_upload(ctx, &set, A.codes, A.n, A.L, A.copy_counts, A.names, A.name_off, A.name_len));
+      tn93g_opts o = opts[k];
+      o.count_only = 1;
+      tn93g_summary S2;
+      const int r = run_impl(ctx, set, A.n, &o, nullptr, nullptr, &S2, false, 0, -1, nullptr, kRunResolveAll);
+      tn93g_free_set(ctx, set);
+      TRY(r);
+      S.max[0] = S2.max[0];
+      S.mean[0] = S2.mean[0];
+      S.logs_resolved += S2.logs_resolved;
+      S.sums_repass = 1;
+      memset(S.amb_bounds, 0, sizeof S.amb_bounds);
+    }
   }
   if (any_emit && sink)
     for (int k = 0; k < K; k++)

@@ -44,6 +44,34 @@ struct RunConsts {
   double threshold, min_distance, resolve_fraction;
   long min_overlap;
   long constT, constNf[4], constCnt[4];
+  double log_band, log_spread;  // the logarithm's ambiguity band and candidate distance in ulps (tlog)
+  bool resolve_all;             // every pair with an ambiguous logarithm goes to the undecided list
+  bool packed;                  // no sequence has more than kPackedMaxEvents events: the packed event sums apply
+};
+
+// The pair stage's tables in device memory: the x16 event table with the N-plane entries after it (Tables::ev,
+// ew[4], eww) and its packed form (PackedTables, built for the run's N-plane setting).
+struct PairTables {
+  AggEntry agg[kEvEntries + 5];
+  PackedTables packed;
+};
+
+// Where the pair stage reports exactness problems:
+//   * the undecided list: pairs whose printed bytes, histogram bin or link decision depend on which candidate the
+//     C library's log returns; entries are two words, (und_k, (i << 32) | j); the host takes those logarithms from
+//     the C library and the pairs are finished again on the device;
+//   * amb: per summary unit (a histogram bin of the run, or a query of a server batch) four words over the pairs
+//     with an ambiguous logarithm: [0] the largest low candidate and [1] the largest high candidate (non-negative
+//     doubles as ordered bit patterns), [2] the sum of (high - low) x copy weight (a double), [3] unused. The host
+//     uses them to certify the maximum and the mean the JSON summary prints.
+struct ExactSink {
+  unsigned long long *und_list;  // nullptr: not listed (the allocation-free entry point)
+  unsigned *und_n;
+  unsigned und_cap;
+  int und_k;                     // first word of this run's entries (the alignment of a batch)
+  unsigned long long *amb;       // nullptr: not tracked
+  const long *counts;            // copy numbers (the weights of the mean)
+  const int *colunit;            // per column (from colbase): its summary unit; nullptr: the histogram bin
 };
 
 struct PairArgs {
@@ -51,7 +79,7 @@ struct PairArgs {
   const uint64_t *planes;
   const uint8_t *cc, *ccT;
   const uint32_t *ev_off, *ev;
-  const AggEntry *agg;  // Tables::ev, then ew[4], eww
+  const PairTables *tab;
   long r0, r1;          // band rows
   long ncols, colbase;  // row stride of dist and the first global column it holds
   long cstart;          // first column of the launch grid (a multiple of 32 past colbase)
@@ -61,8 +89,9 @@ struct PairArgs {
   unsigned long long replay_cap;
   unsigned long long *counters;  // [0] pairs with an ambiguous log, [1] undecided pairs
   const LogTable *logt;
-  const void *tcagg = nullptr;  // clean-site aggregates from the tensor-core kernel ([7][band rows][ncols])
-  size_t tcplane = 0;           // (band rows) x ncols
+  ExactSink ex;
+  const void *tcagg = nullptr;  // clean-site aggregates from the tensor-core kernel: one record per pair slot of
+                                // [band rows][ncols], 8 uint16 (16 bytes) or 8 int32 (32 bytes), 7 used
   int tc16 = 0;                 // the aggregates are uint16 (every value fits: 2 Lc < 65536), else int32
   long tcncols = 0, tccolbase = 0;  // row stride and first column of the aggregates when they hold a chunk of the
                                     // columns (0: the same as ncols and colbase)
@@ -80,6 +109,19 @@ struct ReplayArgs {
   double *dist;
   unsigned long long *counters;
   const LogTable *logt;
+  ExactSink ex;
+};
+
+// One undecided pair on its way through the host: the walk writes the formula's exact inputs and the arguments of
+// its logarithms, the host writes the C library's log of each argument, and the finish kernel writes the distance.
+struct UndEntry {
+  double in[7];   // nf[4], diag, ag, ct
+  double arg[3];  // arguments of the logarithms (Prep::arg)
+  double lg[3];   // log(arg[q]) from the host's C library
+  int nlog;       // logarithms the formula takes (0: the maximum distance)
+  int state;      // 0 formula, 1 skipped by -l (nothing to write)
+  long slot;      // index of the pair's raw distance in its run's dist
+  int k, pad;     // run (alignment) of the pair
 };
 
 struct RowArgs {

@@ -171,4 +171,23 @@ void build_tables(Tables *T, int mode, const unsigned char subset[kCodes])
   }
 }
 
+void pack_tables(const Tables &T, bool w_plane, PackedTables *P)
+{
+  memset(P, 0, sizeof *P);
+  for (int c = kSparse0; c < kGap; c++)
+    for (int o = 0; o < kCodes; o++) {
+      const int k = (c - kSparse0) * kCodes + o;
+      const int32_t *v = T.ev[k].v;
+      const uint32_t w[4] = {(uint32_t)v[0] | (uint32_t)v[1] << 16, (uint32_t)v[2] | (uint32_t)v[3] << 16,
+                             (uint32_t)v[4] | (uint32_t)v[5] << 16, (uint32_t)v[6] | (uint32_t)v[7] << 16};
+      const bool partner_sparse = is_sparse_code(o, w_plane);
+      for (int q = 0; q < 4; q++) {
+        P->row[k][q] = w[q];
+        P->col[k][q] = partner_sparse ? 0u : w[q];
+      }
+      P->rowf[k] = (uint32_t)v[8];
+      P->colf[k] = partner_sparse ? 0u : (uint32_t)v[8];
+    }
+}
+
 }  // namespace tn93

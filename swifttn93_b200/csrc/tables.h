@@ -47,6 +47,22 @@ static_assert(offsetof(Tables, ew) == sizeof(AggEntry) * kSparseCodes * kCodes &
 // mode: 0 resolve, 1 average, 2 skip, 3 gapmm, 4 subset; subset[c] = 1 for codes listed in -a LIST
 void build_tables(Tables *T, int mode, const unsigned char subset[kCodes]);
 
+// The pair kernel's copy of the event table, packed: per (sparse code c of one sequence, code o of the other) the
+// main-mode x16 lanes two to a 32-bit word, w[0] = T | D << 16, w[1] = AG | CT << 16, w[2] = nfA | nfC << 16,
+// w[3] = nfG | amb << 16, and a separate flag word (1: not a multiple of 1/16). No lane of an entry exceeds 32, so
+// packed sums stay exact for fewer than 2048 events per pair; the engine packs when no sequence has more than
+// kPackedMaxEvents events. col[] is row[] with zeros where o is itself a sparse event code (such a site is counted
+// once, from the row's side), so the column side needs no test.
+constexpr int kPackedMaxEvents = 1023;
+constexpr int kEvEntries = kSparseCodes * kCodes;
+struct PackedTables {
+  uint32_t row[kEvEntries][4];
+  uint32_t col[kEvEntries][4];
+  uint32_t rowf[kEvEntries];
+  uint32_t colf[kEvEntries];
+};
+void pack_tables(const Tables &T, bool w_plane, PackedTables *P);
+
 // true if code c is a "sparse event" code: not clean, not a gap, and not N when N has its own plane
 inline bool is_sparse_code(int c, bool w_plane) { return c >= kSparse0 && c < kGap && !(w_plane && c == kN); }
 

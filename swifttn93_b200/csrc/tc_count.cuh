@@ -6,8 +6,9 @@
 // tcgen05.mma of kind::i8 (M = 128, N = 256, K = 32, u8 x u8 -> s32 in tensor memory) per 32 columns
 // accumulates D = A' B'^T, whose 4x4 blocks are the pairs' tables. The epilogue turns each table into the seven
 // clean-site aggregates the pair kernel needs (jointly clean sites, matches, A<->G and C<->T transitions, and the
-// A, C, G base counts over both sequences) and stores them as [7][band rows][band columns], uint16 when twice the
-// column count fits in 16 bits (the largest aggregate is a base count over both sequences), else int32.
+// A, C, G base counts over both sequences) and stores one record per pair slot of [band rows][band columns]: eight
+// uint16 (16 bytes, the eighth unused) when twice the column count fits in 16 bits (the largest aggregate is a base
+// count over both sequences), else eight int32 (32 bytes). The pair kernel reads a record with one vector load.
 //
 // Operand image in HBM (built by onehot_kernel from the compressed codes): per 128-column stage s and 32-sequence
 // block b a 16 KB block at (s * NB + b) * 16 KB, in the canonical K-major layout without swizzle: row r =
@@ -18,7 +19,10 @@
 // One CTA per tile of 32 rows x 64 columns, 128 threads: thread 0 issues the bulk copies (cp.async.bulk with
 // mbarrier transaction counts) into a 2-stage ring, thread 32 issues the MMAs and commits each stage back to its
 // producer barrier, then all four warps read the accumulator (warp w holds TMEM lanes 32w..32w+31). Every wait
-// is bounded; on a timeout the CTA records an error word, drains its copies and frees its tensor memory.
+// is bounded by a deadline on the global nanosecond timer (TcArgs::wait_ns per wait). When a wait gives up, the
+// CTA records an error word, lets its copies in flight land, waits (bounded again) for the MMAs it issued to
+// complete, and only then frees its tensor memory; its aggregates are not stored and the run reports the
+// error.
 #pragma once
 #include <stdint.h>
 
@@ -31,7 +35,7 @@ constexpr int kTcBlockBytes = 32 * 4 * kTcStageK;  // one 32-sequence block of o
 constexpr int kTcStages = 2;
 constexpr int kTcStageBytes = 3 * kTcBlockBytes;   // A (one block) + B (two blocks)
 constexpr size_t kTcSmem = (size_t)kTcStages * kTcStageBytes + 1024;
-constexpr uint32_t kTcWaitLimit = 1u << 26;     // spin iterations before a wait gives up
+constexpr uint64_t kTcWaitNs = 200ull * 1000 * 1000;  // default limit of one bounded wait: 200 ms
 
 struct TcArgs {
   const uint8_t *onehot;  // operand image
@@ -43,9 +47,11 @@ struct TcArgs {
   long ncols, colbase;    // output row stride and first column it holds
   long cstart;            // first column tile (a multiple of 64 past 0)
   long cend;              // columns at or past cend are not stored (a chunk of the columns; N for all of them)
-  void *agg;              // [7][r1 - r0][ncols], uint16 when agg16 (every aggregate < 65536) else int32
+  void *agg;              // [r1 - r0][ncols] records of 8 uint16 when agg16 (every aggregate < 65536), else 8 int32
   int agg16;
   unsigned long long *err;  // set when a wait gave up
+  uint64_t wait_ns;         // limit of each bounded wait (global timer nanoseconds)
+  long skip_fill_block;     // test hook: this block skips its first stage copy (-1: none), so a wait runs out
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -68,11 +74,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
   return ok != 0;
 }
 
-// bounded wait: false when it gave up
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+__device__ __forceinline__ uint64_t global_ns()
 {
-  for (uint32_t it = 0; it < kTcWaitLimit; it++)
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// bounded wait: false when limit_ns passed on the global timer first (the timer is read every 64 polls; a cap on
+// the polls themselves bounds the wait even if the timer were to stall)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint64_t limit_ns)
+{
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 0; it < (1u << 30); it++) {
     if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 63) == 63 && global_ns() - t0 > limit_ns) return false;
+  }
   return false;
 }
 
@@ -193,15 +210,19 @@ __device__ __forceinline__ void count_tc_tile(const TcArgs &a, long i0, long j0)
   const long KS = a.KS;
   const long ab = (i0 / 32), bb = (j0 / 32);
   int fills[kTcStages] = {0, 0};
+  const uint64_t lim = a.wait_ns;
   if (threadIdx.x == 0) {
     // producer: stage ring of A (16 KB) + B (32 KB)
+    const bool skip_first = a.skip_fill_block >= 0 &&
+                            (long)blockIdx.y * gridDim.x + blockIdx.x == a.skip_fill_block;
     for (long k = 0; k < KS; k++) {
       const int s = (int)(k % kTcStages);
-      if (k >= kTcStages && !mbar_wait(&empty[s], (uint32_t)(((k / kTcStages) - 1) & 1))) {
+      if (k >= kTcStages && !mbar_wait(&empty[s], (uint32_t)(((k / kTcStages) - 1) & 1), lim)) {
         atomicExch(&abort_flag, 1);
         break;
       }
       if (*(volatile int *)&abort_flag) break;
+      if (k == 0 && skip_first) continue;  // test hook: stage 0 never fills, so the MMA issuer's wait runs out
       unsigned char *dst = ring + (size_t)s * kTcStageBytes;
       mbar_arrive_expect_tx(&full[s], (uint32_t)kTcStageBytes);
       bulk_g2s(dst, a.onehot + ((size_t)k * a.NB + ab) * kTcBlockBytes, kTcBlockBytes, &full[s]);
@@ -213,7 +234,7 @@ __device__ __forceinline__ void count_tc_tile(const TcArgs &a, long i0, long j0)
     long k = 0;
     for (; k < KS; k++) {
       const int s = (int)(k % kTcStages);
-      if (!mbar_wait(&full[s], (uint32_t)((k / kTcStages) & 1))) {
+      if (!mbar_wait(&full[s], (uint32_t)((k / kTcStages) & 1), lim)) {
         atomicExch(&abort_flag, 1);
         break;
       }
@@ -229,14 +250,12 @@ __device__ __forceinline__ void count_tc_tile(const TcArgs &a, long i0, long j0)
   }
   // epilogue: all four warps (reconverged: tcgen05.ld is warp-collective)
   __syncwarp();
-  const bool ok = __all_sync(0xffffffffu, mbar_wait(&done, 0));
+  const bool ok = __all_sync(0xffffffffu, mbar_wait(&done, 0, lim));
   tc_fence_after();
   const bool go = __all_sync(0xffffffffu, ok && !*(volatile int *)&abort_flag);
   if (go) {
     const int il = warp * 8 + lane / 4, cls = lane & 3;
     const long i = i0 + il;
-    const long rows = a.r1 - a.r0;
-    const size_t plane = (size_t)rows * a.ncols;
     for (int c16 = 0; c16 < 256 / 16; c16++) {
       uint32_t v[16];
       tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c16 * 16), v);
@@ -290,23 +309,26 @@ __device__ __forceinline__ void count_tc_tile(const TcArgs &a, long i0, long j0)
       if (i >= a.r0 && i < a.r1 && j >= lb && j >= a.colbase && j < a.N && j < a.cend) {
         const size_t at = (size_t)(i - a.r0) * a.ncols + (j - a.colbase);
         if (a.agg16) {
-          uint16_t *dst = (uint16_t *)a.agg + at;
-#pragma unroll
-          for (int q = 0; q < 7; q++) dst[q * plane] = (uint16_t)out[q];
+          reinterpret_cast<uint4 *>(a.agg)[at] =
+              make_uint4((uint32_t)out[0] | (uint32_t)out[1] << 16, (uint32_t)out[2] | (uint32_t)out[3] << 16,
+                         (uint32_t)out[4] | (uint32_t)out[5] << 16, (uint32_t)out[6]);
         } else {
-          int32_t *dst = (int32_t *)a.agg + at;
-#pragma unroll
-          for (int q = 0; q < 7; q++) dst[q * plane] = out[q];
+          uint4 *dst = reinterpret_cast<uint4 *>(a.agg) + 2 * at;
+          dst[0] = make_uint4((uint32_t)out[0], (uint32_t)out[1], (uint32_t)out[2], (uint32_t)out[3]);
+          dst[1] = make_uint4((uint32_t)out[4], (uint32_t)out[5], (uint32_t)out[6], 0u);
         }
       }
     }
   }
-  // on a timeout: report it, and let the last fill of each stage land before the ring is released (a stage is
-  // refilled only after its previous fill was consumed, so only the last fill can still be in flight)
+  // On a timeout: report it, let the last fill of each stage land before the ring is released (a stage is
+  // refilled only after its previous fill was consumed, so only the last fill can still be in flight), and make
+  // sure every MMA this CTA issued has completed before its tensor memory is freed: the issuer commits `done`
+  // after its last MMA on every path, so a second bounded wait on it drains them when the first one gave up.
   if (!go && threadIdx.x == 0) {
     atomicAdd(a.err, 1ull);
     for (int s = 0; s < kTcStages; s++)
-      if (fills[s]) mbar_wait(&full[s], (uint32_t)((fills[s] - 1) & 1));
+      if (fills[s]) mbar_wait(&full[s], (uint32_t)((fills[s] - 1) & 1), lim);
+    if (!ok) mbar_wait(&done, 0, lim);
   }
   tc_fence_before();
   __syncthreads();

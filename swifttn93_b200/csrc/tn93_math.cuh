@@ -70,8 +70,12 @@ struct LogTable {
 };
 
 // The C library's log may differ from the correctly rounded value when the exact value lies within
-// (0.519 - 0.5) ulp of a midpoint; values within this band (with a margin) are reported as ambiguous.
+// (0.519 - 0.5) ulp of a midpoint; values within this band (with a margin) are reported as ambiguous. The band
+// is a run parameter (at least kLogBand, at most 0.5 ulp: every log ambiguous), and so is the distance of the
+// other candidate (kLogSpread = 1 ulp, the most the C library can differ by). Tests widen both to drive pairs
+// through the certificate's failure path; the defaults are what every run uses otherwise.
 constexpr double kLogBand = 0.03;
+constexpr double kLogSpread = 1.0;
 
 struct LogR {
   double y;    // correctly rounded log (best estimate)
@@ -91,8 +95,8 @@ TN_HD void fast_two_sum(double a, double b, double &s, double &e)
   e = TSUB(b, TSUB(s, a));
 }
 
-// log of a positive finite x (callers never pass anything else)
-TN_HD LogR tlog(const LogTable &T, double x)
+// log of a positive finite x (callers never pass anything else); band and spread in ulps (see kLogBand)
+TN_HD LogR tlog(const LogTable &T, double x, double band = kLogBand, double spread = kLogSpread)
 {
   LogR R;
   R.amb = 0;
@@ -156,11 +160,12 @@ TN_HD LogR tlog(const LogTable &T, double x)
   const double e_away = hi < 0 ? -lo2 : lo2;
   const double half = (e_away >= 0 || !pow2) ? TMUL(0.5, ulp) : TMUL(0.25, ulp);
   const double margin = TSUB(TSUB(half, e_away < 0 ? -e_away : e_away), E);
-  if (margin <= TMUL(kLogBand, ulp)) {
+  if (margin <= TMUL(band, ulp)) {
     R.amb = 1;
-    // neighbour of hi on the side of the remainder
+    // neighbour of hi on the side of the remainder (spread ulps away; 1 unless a test widens it)
     const bool away = e_away >= 0;
-    R.alt = TDBL(away ? hb + 1 : hb - 1);
+    const uint64_t sp = (uint64_t)spread;
+    R.alt = TDBL(away ? hb + sp : hb - sp);
   }
   return R;
 }
@@ -174,65 +179,90 @@ struct Dist {
   int amb;       // number of ambiguous logarithms
 };
 
-// tn93's formula (refkernel.cpp:752-803, swifttn93.cpp:1954-2001) with every IEEE operation in its order.
-TN_HD Dist tn93_distance(const LogTable &T, const double nf[4], double diag, double ag_in, double ct_in)
+// The formula up to its logarithms: whether it is K2P (a base absent from both sequences), its coefficients, and
+// the arguments of its two (K2P) or three logarithms. nlog = 0 when an argument is not positive (tn93 then
+// reports the maximum distance).
+struct Prep {
+  int nlog;
+  bool k2p;
+  double K1, K2, K3;
+  double arg[3];
+};
+
+// tn93's formula (refkernel.cpp:752-803, swifttn93.cpp:1954-2001) with every IEEE operation in its order, split
+// at the logarithms: tn93_prep computes their arguments, tn93_combine the distance from their values.
+TN_HD Prep tn93_prep(const double nf[4], double diag, double ag_in, double ct_in)
 {
-  Dist D;
-  D.amb = 0;
+  Prep P;
   const double s = TADD(TADD(TADD(nf[0], nf[1]), nf[2]), nf[3]);
-  const double tng = TDIV(2.0, s);
+  // tn93 divides 2 by s and 1 by s; scaling by 2 commutes with rounding, so 2 x (1 / s) is the same double
   const double auxd = TDIV(1.0, s);
+  const double tng = TMUL(2.0, auxd);
   double f0 = TMUL(nf[0], auxd), f1 = TMUL(nf[1], auxd), f2 = TMUL(nf[2], auxd), f3 = TMUL(nf[3], auxd);
   const double fR = TADD(f0, f2), fY = TADD(f1, f3);
-  const bool k2p = nf[0] == 0 || nf[1] == 0 || nf[2] == 0 || nf[3] == 0;
-  double K1 = 0, K2 = 0, K3 = 0;
-  if (!k2p) {
-    K1 = TDIV(TMUL(TMUL(2.0, f0), f2), fR);
-    K2 = TDIV(TMUL(TMUL(2.0, f1), f3), fY);
-    K3 = TMUL(2.0, TSUB(TSUB(TMUL(fR, fY), TDIV(TMUL(TMUL(f0, f2), fY), fR)), TDIV(TMUL(TMUL(f1, f3), fR), fY)));
+  P.k2p = nf[0] == 0 || nf[1] == 0 || nf[2] == 0 || nf[3] == 0;
+  P.K1 = P.K2 = P.K3 = 0;
+  if (!P.k2p) {
+    P.K1 = TDIV(TMUL(TMUL(2.0, f0), f2), fR);
+    P.K2 = TDIV(TMUL(TMUL(2.0, f1), f3), fY);
+    P.K3 = TMUL(2.0, TSUB(TSUB(TMUL(fR, fY), TDIV(TMUL(TMUL(f0, f2), fY), fR)), TDIV(TMUL(TMUL(f1, f3), fR), fY)));
   }
   double AG = TMUL(ag_in, tng), CT = TMUL(ct_in, tng);
   double tv = TSUB(1.0, TADD(TADD(TMUL(diag, tng), AG), CT));
-  if (k2p) {
+  if (P.k2p) {
     const double ti = TADD(AG, CT);
     AG = TSUB(TSUB(1.0, TMUL(2.0, ti)), tv);
     CT = TSUB(1.0, TMUL(2.0, tv));
-    if (AG > 0. && CT > 0.) {
-      const LogR a = tlog(T, AG), c = tlog(T, CT);
-      D.d = TSUB(TMUL(-0.5, a.y), TMUL(0.25, c.y));
-      D.lo = D.hi = D.d;
-      D.amb = a.amb + c.amb;
-      if (D.amb) {
-        for (int m = 1; m < 4; m++) {
-          const double la = (m & 1) ? a.alt : a.y, lc = (m & 2) ? c.alt : c.y;
-          const double v = TSUB(TMUL(-0.5, la), TMUL(0.25, lc));
-          D.lo = v < D.lo ? v : D.lo;
-          D.hi = v > D.hi ? v : D.hi;
-        }
-      }
-    } else {
-      D.d = D.lo = D.hi = kMaxDist;
-    }
+    P.arg[0] = AG;
+    P.arg[1] = CT;
+    P.arg[2] = 1.0;
+    P.nlog = (AG > 0. && CT > 0.) ? 2 : 0;
   } else {
-    AG = TSUB(TSUB(1.0, TDIV(AG, K1)), TDIV(TMUL(0.5, tv), fR));
-    CT = TSUB(TSUB(1.0, TDIV(CT, K2)), TDIV(TMUL(0.5, tv), fY));
+    AG = TSUB(TSUB(1.0, TDIV(AG, P.K1)), TDIV(TMUL(0.5, tv), fR));
+    CT = TSUB(TSUB(1.0, TDIV(CT, P.K2)), TDIV(TMUL(0.5, tv), fY));
     tv = TSUB(1.0, TDIV(TDIV(TMUL(0.5, tv), fY), fR));
-    if (AG > 0. && CT > 0. && tv > 0) {
-      const LogR a = tlog(T, AG), c = tlog(T, CT), t = tlog(T, tv);
-      const double nK1 = -K1;
-      D.d = TSUB(TSUB(TMUL(nK1, a.y), TMUL(K2, c.y)), TMUL(K3, t.y));
-      D.lo = D.hi = D.d;
-      D.amb = a.amb + c.amb + t.amb;
-      if (D.amb) {
-        for (int m = 1; m < 8; m++) {
-          const double la = (m & 1) ? a.alt : a.y, lc = (m & 2) ? c.alt : c.y, lt = (m & 4) ? t.alt : t.y;
-          const double v = TSUB(TSUB(TMUL(nK1, la), TMUL(K2, lc)), TMUL(K3, lt));
-          D.lo = v < D.lo ? v : D.lo;
-          D.hi = v > D.hi ? v : D.hi;
-        }
-      }
-    } else {
-      D.d = D.lo = D.hi = kMaxDist;
+    P.arg[0] = AG;
+    P.arg[1] = CT;
+    P.arg[2] = tv;
+    P.nlog = (AG > 0. && CT > 0. && tv > 0) ? 3 : 0;
+  }
+  return P;
+}
+
+// the distance from the logarithms of P's arguments (lg[0..nlog)); the maximum distance when nlog = 0
+TN_HD double tn93_combine(const Prep &P, double la, double lc, double lt)
+{
+  if (P.nlog == 0) return kMaxDist;
+  if (P.k2p) return TSUB(TMUL(-0.5, la), TMUL(0.25, lc));
+  const double nK1 = -P.K1;
+  return TSUB(TSUB(TMUL(nK1, la), TMUL(P.K2, lc)), TMUL(P.K3, lt));
+}
+
+TN_HD Dist tn93_distance(const LogTable &T, const double nf[4], double diag, double ag_in, double ct_in,
+                         double band = kLogBand, double spread = kLogSpread)
+{
+  Dist D;
+  D.amb = 0;
+  const Prep P = tn93_prep(nf, diag, ag_in, ct_in);
+  if (P.nlog == 0) {
+    D.d = D.lo = D.hi = kMaxDist;
+    return D;
+  }
+  const LogR a = tlog(T, P.arg[0], band, spread), c = tlog(T, P.arg[1], band, spread);
+  LogR t;
+  t.y = t.alt = 0.0;
+  t.amb = 0;
+  if (P.nlog == 3) t = tlog(T, P.arg[2], band, spread);
+  D.d = tn93_combine(P, a.y, c.y, t.y);
+  D.lo = D.hi = D.d;
+  D.amb = a.amb + c.amb + t.amb;
+  if (D.amb) {
+    // every combination of candidates (the distance is monotone in each logarithm, so the corners bound it)
+    for (int m = 1; m < 8; m++) {
+      const double la = (m & 1) ? a.alt : a.y, lc = (m & 2) ? c.alt : c.y, lt = (m & 4) ? t.alt : t.y;
+      const double v = tn93_combine(P, la, lc, lt);
+      D.lo = v < D.lo ? v : D.lo;
+      D.hi = v > D.hi ? v : D.hi;
     }
   }
   return D;

@@ -9,6 +9,7 @@ for byte. No collective runs on the data path.
 """
 from __future__ import annotations
 
+import ctypes as C
 from dataclasses import dataclass
 
 import numpy as np
@@ -47,12 +48,18 @@ class Partial:
     replayed: int = 0
     ambiguous: int = 0
     undecided: int = 0
+    resolved: int = 0
+    # per bin, over the band's pairs with an ambiguous logarithm: largest low and high candidate, spread, count
+    amb_bounds: np.ndarray = None
 
 
 def partial_from_run(r0, r1, text, summ: Summary, row_sums) -> Partial:
+    bounds = np.zeros((3, 4))
+    if summ.raw is not None and hasattr(summ.raw, "amb_bounds"):
+        bounds = np.array([[summ.raw.amb_bounds[u][q] for q in range(4)] for u in range(3)])
     return Partial(r0, r1, text, summ.pairwise, summ.skipped, summ.links, list(summ.max),
                    np.asarray(summ.hist, dtype=np.uint64), np.asarray(row_sums, dtype=np.float64),
-                   summ.pairs_replayed, summ.logs_ambiguous, summ.undecided)
+                   summ.pairs_replayed, summ.logs_ambiguous, summ.undecided, summ.logs_resolved, bounds)
 
 
 def merge(parts: list) -> tuple:
@@ -83,6 +90,15 @@ def merge(parts: list) -> tuple:
     S.pairs_replayed = sum(p.replayed for p in parts)
     S.logs_ambiguous = sum(p.ambiguous for p in parts)
     S.undecided = sum(p.undecided for p in parts)
+    S.logs_resolved = sum(p.resolved for p in parts)
+    # the bands' bounds combine: largest candidates by maximum, spreads and counts by sum
+    for u in range(3):
+        b = [p.amb_bounds[u] for p in parts if p.amb_bounds is not None]
+        if b:
+            S.amb_bounds[u][0] = max(x[0] for x in b)
+            S.amb_bounds[u][1] = max(x[1] for x in b)
+            S.amb_bounds[u][2] = sum(x[2] for x in b)
+            S.amb_bounds[u][3] = sum(x[3] for x in b)
     text = b"".join(p.text for p in parts)
     S.output_bytes = len(text)
     from . import _plain_summary
@@ -90,9 +106,24 @@ def merge(parts: list) -> tuple:
     return text, _plain_summary(S)
 
 
-def run_sharded(compute, N: int, n1: int, cross: bool, group=None):
+def certified(S, N: int, n1: int, cross: bool, fst: bool = False) -> bool:
+    """Whether every number the merged JSON summary prints is certain for every rounding of the C library's log
+    (tn93g_summary_certified over the combined bounds). Without the library, only a run with no ambiguous
+    logarithm is certain."""
+    if all(S.raw.amb_bounds[u][3] == 0 for u in range(3)):
+        return True
+    from . import load_library
+
+    rows = n1 if cross else N
+    chain = (N - n1 if cross else N) + rows + 2
+    return bool(load_library().tn93g_summary_certified(C.byref(S.raw), chain, int(fst)))
+
+
+def run_sharded(compute, N: int, n1: int, cross: bool, group=None, exact_compute=None, fst: bool = False):
     """Runs this rank's band with compute(r0, r1) -> Partial and gathers the bands to rank 0, which returns the
-    merged (text, Summary); other ranks return None. Every rank takes the same collective step."""
+    merged (text, Summary); other ranks return None. When the merged JSON numbers are not certain and
+    exact_compute is given, every rank runs its band again with exact sums (exact_compute(r0, r1) -> Partial) and
+    rank 0 takes the maximum and means from those. Every rank takes the same collective steps."""
     import torch.distributed as dist
 
     rank, world = dist.get_rank(group), dist.get_world_size(group)
@@ -100,15 +131,42 @@ def run_sharded(compute, N: int, n1: int, cross: bool, group=None):
     part = compute(r0, r1)
     out = [None] * world if rank == 0 else None
     dist.gather_object(part, out, dst=0, group=group)
-    if rank != 0:
-        return None
-    return merge(out)
+    merged, again = None, [False]
+    if rank == 0:
+        merged = merge(out)
+        again[0] = exact_compute is not None and not certified(merged[1], N, n1, cross, fst)
+    dist.broadcast_object_list(again, src=0, group=group)
+    if again[0]:
+        part2 = exact_compute(r0, r1)
+        out2 = [None] * world if rank == 0 else None
+        dist.gather_object(part2, out2, dst=0, group=group)
+        if rank == 0:
+            _, S2 = merge(out2)
+            for q in range(3):
+                merged[1].max[q] = S2.max[q]
+                merged[1].mean[q] = S2.mean[q]
+                merged[1].raw.max[q] = S2.max[q]
+                merged[1].raw.mean[q] = S2.mean[q]
+            merged[1].sums_repass = True
+            merged[1].raw.sums_repass = 1
+    return merged if rank == 0 else None
 
 
-def engine_compute(engine, dset, opts, n1=None):
-    """compute(r0, r1) for run_sharded on this rank's GPU (tn93g_run_rows)."""
+def engine_compute(engine, dset, opts, n1=None, exact=False):
+    """compute(r0, r1) for run_sharded on this rank's GPU (tn93g_run_rows); exact=True: the exact-sums pass
+    (every pair with an ambiguous logarithm finished with the C library's log, no text)."""
     def compute(r0, r1):
-        text, summ, rows = engine.run_rows(dset, opts, r0, r1, n1=n1)
+        o = opts
+        if exact:
+            from dataclasses import replace
+
+            o = replace(opts, count_only=True)
+            engine.set_exact_sums(True)
+        try:
+            text, summ, rows = engine.run_rows(dset, o, r0, r1, n1=n1)
+        finally:
+            if exact:
+                engine.set_exact_sums(False)
         return partial_from_run(r0, r1, text, summ, rows)
 
     return compute

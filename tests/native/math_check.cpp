@@ -125,9 +125,14 @@ int main(int argc, char **argv)
     double diag = (T16 - mm) / 16.0, agv = (ts - ct) / 16.0, ctv = ct / 16.0;
     Dist D = tn93_distance(T, nf, diag, agv, ctv);
     double ref = ref_formula(nf, diag, agv, ctv);
+    // the resolution path: the formula's arguments, the C library's log of each, then the combination
+    const Prep P = tn93_prep(nf, diag, agv, ctv);
+    const double res = tn93_combine(P, P.nlog ? log(P.arg[0]) : 0., P.nlog ? log(P.arg[1]) : 0.,
+                                    P.nlog == 3 ? log(P.arg[2]) : 0.);
     d_n++;
     d_amb += D.amb != 0;
     bool ok = D.amb ? (ref >= D.lo && ref <= D.hi) : (memcmp(&ref, &D.d, 8) == 0);
+    ok = ok && memcmp(&ref, &res, 8) == 0;
     if (!ok) {
       if (d_bad < 5) fprintf(stderr, "dist mismatch: got %a [%a,%a] amb %d want %a\n", D.d, D.lo, D.hi, D.amb, ref);
       d_bad++;

@@ -256,3 +256,37 @@ def test_service_scheduling_with_a_stand_in_engine(monkeypatch):
     done = sorted(n for b in _FakeReference.batches for n in b)
     assert done == [1, 2, 3, 4, 7]
     assert all(len(b) <= 3 and sum(b) <= 8 for b in _FakeReference.batches)
+
+
+@pytest.mark.gpu
+def test_full_size_reference_queries_match_oracle(oracle_bin, tmp_path):
+    """The served workload at full size: the 30,000 x 1,500 resident reference, a batch of four queries of 1-200
+    sequences at the serving flags; each response equals the oracle's `-s QUERY REF` run byte for byte."""
+    from swifttn93_b200 import Engine, Fasta, Options, ResidentReference, synth
+    from swifttn93_b200.serve import header_line
+
+    rnames, rcodes = synth.serve_reference()
+    ref = synth.to_fasta(rnames, rcodes)
+    refp = tmp_path / "ref.fa"
+    refp.write_bytes(ref)
+    rng = np.random.default_rng(30000)
+    queries = []
+    for k, q in enumerate((1, 32, 200, 7)):
+        names, codes = synth.serve_query(rng, rcodes, q, f"f{k}")
+        queries.append(synth.to_fasta(names, codes))
+    opts = Options(threshold=0.015, mode="resolve", min_overlap=500)
+    eng = Engine()
+    R = Fasta(ref)
+    res = ResidentReference(eng, R, opts, max_batch_sequences=512, max_batch_queries=8)
+    out = res.batch([Fasta(q, expect_len=R.L) for q in queries])
+    flags = ["-t", "0.015", "-a", "resolve", "-l", "500"]
+    for k, qfa in enumerate(queries):
+        qp = tmp_path / f"q{k}.fa"
+        qp.write_bytes(qfa)
+        rc, fb, so, _ = run_tn93(oracle_bin, flags + ["-s", str(qp)], refp, tmp_path)
+        assert rc == 0
+        body, summ = out[k]
+        assert header_line(opts) + body == fb, (k, len(body), len(fb))
+        assert summ.json(R.n, Fasta(qfa).n, second_file=True) == so, k
+    res.close()
+    eng.close()

@@ -1,6 +1,6 @@
 """The allocation-free entry point, tn93g_pair_distances_noalloc, for callers that cannot allocate device
-memory (for example code running during CUDA graph capture, or a host application whose own allocator owns the
-device). The test is the caller: it allocates the input and output buffers itself (with torch) and calls the
+memory (a host application whose own allocator owns the device, or a loop that must not enter the driver's
+allocator). The test is the caller: it allocates the input and output buffers itself (with torch) and calls the
 entry point through the C ABI; the engine allocates nothing.
 
 Each call's distances, turned into tn93's text exactly as tn93g_run does (clamp at 0, -t/-w link test,
