@@ -1578,6 +1578,8 @@ struct DevBuf {
 };
 
 constexpr int kBatchBufs = 56;
+constexpr int kMaxTcChunks = 48;         // row chunks of a band on the tensor-core count path
+constexpr long kTcChunkPairs = 2l << 20;  // pairs per chunk: 32 MB of 16-byte records, L2-resident
 
 struct tn93g_set {
   long N = 0, L = 0;
@@ -1605,8 +1607,8 @@ struct tn93g_ctx {
   cudaEvent_t evs[16];
   cudaStream_t copy_stream = nullptr;  // device->host copies of finished bands
   cudaEvent_t evw0[2], evw1[2], evc0[2], evc1[2];
-  cudaEvent_t evk[2][6];  // per band parity: start, after pair, after replay, after stats+sums+scan, stats on host,
-                          // after the tensor-core count kernel
+  cudaEvent_t evk[2][5];  // per band parity: start, after pair, after replay, after stats+sums+scan, stats on host
+  cudaEvent_t evcnt[2][2 * kMaxTcChunks];  // per band parity: around each chunk's tensor-core count kernel
   DevBuf out2[2], total;
   void *pin2[2] = {nullptr, nullptr};
   size_t pin2_n[2] = {0, 0};
@@ -1865,6 +1867,8 @@ int tn93g_create(tn93g_ctx **out, int device, size_t hbm_budget)
         rc = TN93G_ECUDA;
       for (auto &e : ctx->evk[q])
         if (cudaEventCreate(&e) != cudaSuccess) rc = TN93G_ECUDA;
+      for (auto &e : ctx->evcnt[q])
+        if (cudaEventCreate(&e) != cudaSuccess) rc = TN93G_ECUDA;
     }
     if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) rc = TN93G_ECUDA;
     if (const char *e = getenv("TN93G_COUNT")) ctx->count_path = strcmp(e, "popc") == 0 ? 0 : 1;
@@ -1914,6 +1918,8 @@ void tn93g_destroy(tn93g_ctx *ctx)
     for (cudaEvent_t e : {ctx->evw0[q], ctx->evw1[q], ctx->evc0[q], ctx->evc1[q]})
       if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->evk[q])
+      if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->evcnt[q])
       if (e) cudaEventDestroy(e);
   }
   if (ctx->total.p) cudaFree(ctx->total.p);
@@ -2257,7 +2263,28 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   const size_t dslots = (size_t)band * ncols;
   TRY(ensure(ctx, ctx->dist, 2 * dslots * sizeof(double)));
   const int tc16 = 2 * Lc < 65536;
-  if (use_tc) TRY(ensure(ctx, ctx->tcagg, dslots * (tc16 ? 16 : 32)));
+  // the tensor-core path's row chunks per band (boundaries on the count kernel's 32-row tiles)
+  std::vector<std::vector<std::pair<long, long>>> band_chunks(bands.size());
+  size_t chunk_slots = 1;
+  int nchunks[2] = {0, 0};
+  if (use_tc) {
+    for (size_t b = 0; b < bands.size(); b++) {
+      const long r0 = bands[b].first, r1 = bands[b].second;
+      long bp = 0;
+      for (long r = r0; r < r1; r++) bp += rc.cross ? ncols : (N - r - 1);
+      const long target = std::max(kTcChunkPairs, (bp + kMaxTcChunks - 2) / (kMaxTcChunks - 1));
+      for (long c0 = r0; c0 < r1;) {
+        long c1 = c0, pairs = 0;
+        while (c1 < r1 && (c1 == c0 || pairs < target)) pairs += rc.cross ? ncols : (N - c1++ - 1);
+        c1 = std::min(r1, (c1 + kTcRows - 1) / kTcRows * kTcRows);
+        if ((int)band_chunks[b].size() == kMaxTcChunks - 1) c1 = r1;  // never more chunks than events
+        band_chunks[b].push_back({c0, c1});
+        chunk_slots = std::max(chunk_slots, (size_t)(c1 - c0) * ncols);
+        c0 = c1;
+      }
+    }
+    TRY(ensure(ctx, ctx->tcagg, chunk_slots * (tc16 ? 16 : 32)));
+  }
   TRY(ensure(ctx, ctx->rq, dslots * sizeof(unsigned long long)));
   TRY(ensure(ctx, ctx->rqn, sizeof(unsigned)));
   TRY(ensure(ctx, ctx->counters, 4 * sizeof(unsigned long long)));
@@ -2414,38 +2441,58 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     const long cblk0 = (cstart - colbase) / 32;
     const long cblks = (ncols + 31) / 32 - cblk0;
     if (use_tc && cblks > 0) {
-      // clean-site aggregates of the band's pairs on the tensor cores
-      TcArgs T;
-      T.onehot = (const uint8_t *)ctx->ohimg.p;
-      T.NB = tc_NB;
-      T.KS = tc_KS;
-      T.N = N;
-      T.n1 = n1;
-      T.cross = rc.cross;
-      T.r0 = r0;
-      T.r1 = r1;
-      T.ncols = ncols;
-      T.colbase = colbase;
-      T.cstart = cstart / kTcCols * kTcCols;
-      T.cend = N;
-      T.agg = ctx->tcagg.p;
-      T.agg16 = tc16;
-      T.err = (unsigned long long *)ctx->tcerr.p;
-      T.wait_ns = ctx->wait_ns;
-      T.skip_fill_block = fault == TN93G_FAULT_SKIP_FILL && bi == 0 ? 0 : -1;
-      const long rt0 = r0 / kTcRows * kTcRows;
-      const dim3 g((unsigned)((N - T.cstart + kTcCols - 1) / kTcCols), (unsigned)((r1 - rt0 + kTcRows - 1) / kTcRows));
-      count_tc_kernel<<<g, 128, kTcSmem, st>>>(T);
-      CU(cudaGetLastError());
-      ctx->launches++;
-      A.tcagg = ctx->tcagg.p;
-      A.tc16 = tc16;
-    }
-    CU(cudaEventRecord(K[5], st));
-    if (cblks > 0) {
+      // Clean-site aggregates on the tensor cores, then the pair kernel, chunk by chunk of rows: a chunk's records
+      // (about kTcChunkPairs pairs, 32 MB) are still in L2 when the pair kernel reads them.
+      const std::vector<std::pair<long, long>> &chunks = band_chunks[bi];
+      for (size_t q = 0; q < chunks.size(); q++) {
+        const long c0 = chunks[q].first, c1 = chunks[q].second;
+        const long ccs = rc.cross ? n1 : c0 + 1;
+        TcArgs T;
+        T.onehot = (const uint8_t *)ctx->ohimg.p;
+        T.NB = tc_NB;
+        T.KS = tc_KS;
+        T.N = N;
+        T.n1 = n1;
+        T.cross = rc.cross;
+        T.r0 = c0;
+        T.r1 = c1;
+        T.ncols = ncols;
+        T.colbase = colbase;
+        T.cstart = ccs / kTcCols * kTcCols;
+        T.cend = N;
+        T.agg = ctx->tcagg.p;
+        T.agg16 = tc16;
+        T.err = (unsigned long long *)ctx->tcerr.p;
+        T.wait_ns = ctx->wait_ns;
+        T.skip_fill_block = fault == TN93G_FAULT_SKIP_FILL && bi == 0 && q == 0 ? 0 : -1;
+        const long rt0 = c0 / kTcRows * kTcRows;
+        const dim3 g((unsigned)((N - T.cstart + kTcCols - 1) / kTcCols), (unsigned)((c1 - rt0 + kTcRows - 1) / kTcRows));
+        CU(cudaEventRecord(ctx->evcnt[par][2 * q], st));
+        count_tc_kernel<<<g, 128, kTcSmem, st>>>(T);
+        CU(cudaGetLastError());
+        CU(cudaEventRecord(ctx->evcnt[par][2 * q + 1], st));
+        ctx->launches++;
+        PairArgs AC = A;
+        AC.r0 = c0;
+        AC.r1 = c1;
+        AC.dist = A.dist + (size_t)(c0 - r0) * ncols;
+        AC.tcagg = ctx->tcagg.p;
+        AC.tc16 = tc16;
+        const long cb0 = (ccs - colbase) / 32, cbs = (ncols + 31) / 32 - cb0;
+        if (cbs > 0) {
+          AC.cstart = colbase + cb0 * 32;
+          CU(launch_pair(AC, cbs, c1 - c0, st));
+          ctx->launches++;
+        }
+      }
+      nchunks[par] = (int)chunks.size();
+    } else if (cblks > 0) {
       A.cstart = colbase + cblk0 * 32;
       CU(launch_pair(A, cblks, nr, st));
       ctx->launches++;
+      nchunks[par] = 0;
+    } else {
+      nchunks[par] = 0;
     }
     CU(cudaEventRecord(K[1], st));
     ReplayArgs R;
@@ -2495,8 +2542,10 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     CU(cudaEventSynchronize(K[4]));
     CU(cudaEventElapsedTime(&ms, K[0], K[1]));
     ctx->timings[1] += ms;
-    CU(cudaEventElapsedTime(&ms, K[0], K[5]));
-    ctx->timings[7] += ms;
+    for (int q = 0; q < nchunks[par]; q++) {
+      CU(cudaEventElapsedTime(&ms, ctx->evcnt[par][2 * q], ctx->evcnt[par][2 * q + 1]));
+      ctx->timings[7] += ms;
+    }
     CU(cudaEventElapsedTime(&ms, K[1], K[2]));
     ctx->timings[2] += ms;
     CU(cudaEventElapsedTime(&ms, K[2], K[3]));
@@ -3162,7 +3211,8 @@ struct tn93g_server {
 };
 
 namespace {
-constexpr long kServerTcChunk = 1024;  // query columns per tensor-core count launch (a multiple of 64)
+constexpr long kServerTcChunk = 128;  // query columns per tensor-core count launch (a multiple of 64): the
+                                      // records of a 30,000-sequence reference x 128 columns (61 MB) stay in L2
 
 // opt-in to the count kernel's dynamic shared memory on the current device
 int tc_attr(tn93g_ctx *ctx)
