@@ -27,6 +27,53 @@ const char kUsage[] =
     "usage: tn93 [-h] [-v] [-o OUTPUT] [-t THRESHOLD] [-w MIN_THRESHOLD] [-a AMBIGS] [-g FRACTION] [-l OVERLAP] "
     "[-d COUNTS_IN_NAME] [-f FORMAT] [-s SECOND_FASTA] [-b] [-r] [-c] [-n] [-0] [-q] [-H] [-S] [-D DELIMITER][FASTA]\n";
 
+// tn93's help text after the usage line (argparse.cpp:41-100), printed by -h and --help; kept byte for byte, since
+// callers compare the command line's output with tn93's
+const char kHelp[] =
+    "compute Tamura Nei 93 distances between aligned sequences (version v1.1.0)\n"
+    "\n"
+    "optional arguments:\n"
+    "  -h, --help               show this help message and exit\n"
+    "  -v, --version            show tn93 version (v1.1.0)\n"
+    "  -o OUTPUT                direct the output to a file named OUTPUT (default=stdout)\n"
+    "  -t THRESHOLD             only report (count) distances below this threshold (>=0, default=0.015)\n"
+    "  -w MINIMUM THRESHOLD     report distances above minimum threshold \n"
+    "  -a AMBIGS                handle ambigous nucleotides using one of the following strategies (default=resolve)\n"
+    "                           resolve: resolve ambiguities to minimize distance (e.g.R matches A);\n"
+    "                           average: average ambiguities (e.g.R-A is 0.5 A-A and 0.5 G-A);\n"
+    "                           skip: do not include sites with ambiguous nucleotides in distance calculations;\n"
+    "                           gapmm: a gap ('-') matched to anything other than another gap is like matching an N (4-fold ambig) to it;\n"
+    "                           a string (e.g. RY): any ambiguity in the list is RESOLVED; any ambiguitiy NOT in the list is averaged (LIST-NOT LIST will also be averaged);\n"
+    "  -g FRACTION              in combination with AMBIGS, works to limit (for resolve and string options to AMBIG)\n"
+    "                           the maximum tolerated FRACTION of ambiguous characters; sequences whose pairwise comparisons\n"
+    "                           include no more than FRACTION [0,1] of sites with resolvable ambiguities will be resolved\n"
+    "                           while all others will be AVERAGED (default = 1.0)\n"
+    "  -f FORMAT                controls the format of the output unless -c is set (default=csv)\n"
+    "                           csv: seqname1, seqname2, distance;\n"
+    "                           csvn: 1, 2, distance;\n"
+    "                           hyphy: {{d11,d12,..,d1n}...{dn1,dn2,...,dnn}}, where distances above THRESHOLD are set to 100;\n"
+    "  -l OVERLAP               only process pairs of sequences that overlap over at least OVERLAP nucleotides (an integer >0, default=100):\n"
+    "  -d COUNTS_IN_NAME        if sequence name is of the form 'somethingCOUNTS_IN_NAMEinteger' then treat the integer as a copy number\n"
+    "                           when computing distance histograms (a character, default=':'):\n"
+    "  -s SECOND_FASTA          if specified, read another FASTA file from SECOND_FASTA and perform pairwise comparison BETWEEN the files (default=NULL)\n"
+    "  -b                       bootstrap alignment columns before computing distances (default = false)\n"
+    "                           when -s is supplied, permutes the assigment of sequences to files\n"
+    "                           interacts with -r option\n"
+    "  -r                       if -b is specified AND -s is supplied, using -r will bootstrap across sites\n"
+    "                           instead of allocating sequences to 'compartments' randomly\n"
+    "  -c                       only count the pairs below a threshold, do not write out all the pairs \n"
+    "  -n                       if set, do NOT write out headers for delimited files (default is to write) \n"
+    "  -m                       compute inter- and intra-population means suitable for FST caclulations\n"
+    "                           only applied when -s is used to provide a second file\n"
+    "  -u PROBABILITY           subsample sequences with specified probability (a value between 0 and 1, default = 1.0)\n"
+    "  -D DELIMITER             use this character as a delimiter in the output column-file (a character, default = ',')\n"
+    "  -0                       report distances between each sequence and itself (as 0); this is useful to ensure every sequence\n"
+    "                           in the input file appears in the output, e.g. for network construction to contrast clustered/unclustered\n"
+    "  -q                       do not report progress updates and other diagnostics to stderr \n"
+    "  -H                       use Hamming distance early exit to speed up distance calculations \n"
+    "  -S, --subquadratic       perform subquadratic pairwise distance calculations (default = false)\n"
+    "  FASTA                    read sequences to compare from this file (default=stdin)\n";
+
 struct Options {
   FILE *out = stdout, *in1 = stdin, *in2 = nullptr;
   double distance = 0.015, min_distance = -1.e-10, resolve_fraction = 1.0, include_prob = 1.0;
@@ -68,7 +115,7 @@ Options parse(int argc, char **argv)
     if (a[0] == '-' && a[1] == '-') {
       const char *l = a + 2;
       if (!strcmp(l, "help")) {
-        fprintf(stderr, "%s\n", kUsage);
+        fprintf(stderr, "%s\n%s", kUsage, kHelp);
         exit(1);
       } else if (!strcmp(l, "version")) {
         fprintf(stderr, "v1.1.0\n");
@@ -89,7 +136,7 @@ Options parse(int argc, char **argv)
     switch (a[1]) {
       case 'h':
         if (a[2]) fail("unknown argument: %s", a);
-        fprintf(stderr, "%s\n", kUsage);
+        fprintf(stderr, "%s\n%s", kUsage, kHelp);
         exit(1);
       case 'v': fprintf(stderr, "v1.1.0\n"); exit(0);
       case 'o':

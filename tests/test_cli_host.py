@@ -32,6 +32,14 @@ def test_version_matches_reference(ref_bin, cli, tmp_path):
     assert _run(cli, ["-v"], tmp_path) == _run(ref_bin, ["-v"], tmp_path)
 
 
+@pytest.mark.parametrize("flag", ["-h", "--help"])
+def test_help_matches_reference(ref_bin, cli, tmp_path, flag):
+    """tn93's usage line and help text (argparse.cpp:41-107) on stderr, exit status 1."""
+    want = _run(ref_bin, [flag], tmp_path)
+    assert want[0] == 1 and len(want[2]) > 4000
+    assert _run(cli, [flag], tmp_path) == want
+
+
 @pytest.mark.parametrize("args", BAD_ARGS, ids=[" ".join(a) for a in BAD_ARGS])
 def test_option_errors_match_reference(ref_bin, cli, tmp_path, args):
     fa = tmp_path / "ok.fa"
