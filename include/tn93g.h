@@ -216,6 +216,7 @@ int tn93g_server_create(tn93g_ctx *ctx, tn93g_server **out, const uint8_t *codes
  * n; engine counters are reported in sums[0]). */
 int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries, tn93g_query_sink sink, void *user,
                        tn93g_summary *sums);
+/* Frees the server's device buffers; call it before tn93g_destroy of the server's context. */
 void tn93g_server_destroy(tn93g_server *srv);
 
 /* The JSON summary tn93 prints for one run (swifttn93.cpp:2914-2958), byte for byte; n2 = 0 and second_file = 0

@@ -12,6 +12,7 @@ the built library and a CUDA device, and raises otherwise.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from dataclasses import dataclass, field
 from pathlib import Path
 
@@ -269,6 +270,7 @@ class Engine:
     def __init__(self, device: int = 0, hbm_budget: int = 0):
         self.lib = load_library()
         self.ctx = C.c_void_p()
+        self._servers = weakref.WeakSet()  # servers on this context: destroyed before it
         self._check(self.lib.tn93g_create(C.byref(self.ctx), device, hbm_budget))
 
     def _check(self, rc):
@@ -441,6 +443,8 @@ class Engine:
         return summ
 
     def close(self):
+        for srv in list(getattr(self, "_servers", ())):
+            srv.close()
         if self.ctx:
             self.lib.tn93g_destroy(self.ctx)
             self.ctx = C.c_void_p()
@@ -479,6 +483,7 @@ class ResidentReference:
             engine.ctx, C.byref(self.srv), C.cast(a.codes, C.c_void_p), a.n, a.L, C.cast(a.copy_counts, C.c_void_p),
             C.cast(a.names, C.c_void_p), C.cast(a.name_off, C.c_void_p), C.cast(a.name_len, C.c_void_p),
             C.byref(o), int(max_batch_sequences), int(max_batch_queries)))
+        engine._servers.add(self)
 
     def batch(self, queries: list) -> list:
         """Runs the queries (Fasta objects of the reference's length) in one batch: [(body bytes, Summary)]."""
@@ -510,9 +515,10 @@ class ResidentReference:
         return {Engine.STAGES[q]: t[q] for q in range(k)}
 
     def close(self):
-        if self.srv:
+        # a server lives inside its engine's context: it is destroyed first (Engine.close does so as well)
+        if self.srv and self.engine.ctx:
             self.lib.tn93g_server_destroy(self.srv)
-            self.srv = C.c_void_p()
+        self.srv = C.c_void_p()
 
     def __del__(self):
         try:

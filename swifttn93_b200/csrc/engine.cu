@@ -48,12 +48,16 @@ __device__ __forceinline__ unsigned lanemask_lt() { return (1u << (threadIdx.x &
 __device__ __forceinline__ bool sparse_code(int c, bool wplane) { return c >= 4 && c < 17 && !(wplane && c == 15); }
 
 //------------------------------------------------------------------------------------------------ pack
-// per column: the set of codes seen (bit c), per launch the number of N codes
-__global__ void colscan_kernel(const uint8_t *__restrict__ codes, long N, long L, uint32_t *seen,
-                               unsigned long long *nN)
+// Each packing kernel's body takes its block coordinates as arguments, so that a batch of alignments can run one
+// launch for all of them (the *_batch_kernel forms below map each block to its alignment and local block).
+
+// per column: the set of codes seen (bit c), per launch the number of N codes; block (bx, by) covers 256 columns
+// of 64 sequences
+__device__ __forceinline__ void colscan_body(const uint8_t *__restrict__ codes, long N, long L, uint32_t *seen,
+                                             unsigned long long *nN, long bx, long by)
 {
-  const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const long i0 = blockIdx.y * 64l, i1 = min(N, i0 + 64);
+  const long p = bx * 256l + threadIdx.x;
+  const long i0 = by * 64l, i1 = min(N, i0 + 64);
   uint32_t m = 0;
   unsigned cn = 0;
   if (p < L)
@@ -67,13 +71,20 @@ __global__ void colscan_kernel(const uint8_t *__restrict__ codes, long N, long L
   if ((threadIdx.x & 31) == 0 && cn) atomicAdd(nN, (unsigned long long)cn);
 }
 
-// one warp per (sequence, 64-column word): bit planes, compressed codes, sparse event counts
-__global__ void pack_kernel(PackArgs a)
+__global__ void colscan_kernel(const uint8_t *__restrict__ codes, long N, long L, uint32_t *seen,
+                               unsigned long long *nN)
+{
+  colscan_body(codes, N, L, seen, nN, blockIdx.x, blockIdx.y);
+}
+
+// one warp per (sequence, 64-column word): bit planes, compressed codes, sparse event counts; block bx covers 8
+// sequences, and the words w0, w0 + wstep, ...
+__device__ __forceinline__ void pack_body(const PackArgs &a, long bx, long w0, long wstep)
 {
   const int lane = threadIdx.x & 31;
-  const long i = blockIdx.x * (long)kWarps + (threadIdx.x >> 5);
+  const long i = bx * (long)kWarps + (threadIdx.x >> 5);
   if (i >= a.N) return;
-  for (long w = blockIdx.y; w < a.W; w += gridDim.y) {
+  for (long w = w0; w < a.W; w += wstep) {
   const long k0 = w * 64 + lane, k1 = k0 + 32;
   const int c0 = k0 < a.Lc ? a.codes[i * a.L + a.varcol[k0]] : 17;
   const int c1 = k1 < a.Lc ? a.codes[i * a.L + a.varcol[k1]] : 17;
@@ -101,11 +112,13 @@ __global__ void pack_kernel(PackArgs a)
   }
 }
 
-// one warp per sequence: its sparse events in site order
-__global__ void events_kernel(PackArgs a)
+__global__ void pack_kernel(PackArgs a) { pack_body(a, blockIdx.x, blockIdx.y, gridDim.y); }
+
+// one warp per sequence: its sparse events in site order (block bx: 8 sequences)
+__device__ __forceinline__ void events_body(const PackArgs &a, long bx)
 {
   const int lane = threadIdx.x & 31;
-  const long i = blockIdx.x * (long)kWarps + (threadIdx.x >> 5);
+  const long i = bx * (long)kWarps + (threadIdx.x >> 5);
   if (i >= a.N) return;
   uint32_t off = a.ev_off[i];
   const uint8_t *row = a.cc + i * a.Lc;
@@ -120,11 +133,14 @@ __global__ void events_kernel(PackArgs a)
   }
 }
 
-// ccT[k][i] = cc[i][k] (padding sequences read as gaps)
-__global__ void transpose_kernel(const uint8_t *__restrict__ cc, uint8_t *ccT, long N, long Lc, long Npad)
+__global__ void events_kernel(PackArgs a) { events_body(a, blockIdx.x); }
+
+// ccT[k][i] = cc[i][k] (padding sequences read as gaps); block (bx, by) of 32 x 8 threads: 32 columns x 32 sequences
+__device__ __forceinline__ void transpose_body(const uint8_t *__restrict__ cc, uint8_t *ccT, long N, long Lc, long Npad,
+                                               long bx, long by)
 {
   __shared__ uint8_t tile[32][33];
-  const long k0 = blockIdx.x * 32l, i0 = blockIdx.y * 32l;
+  const long k0 = bx * 32l, i0 = by * 32l;
   const int tx = threadIdx.x, ty = threadIdx.y;
   for (int r = ty; r < 32; r += 8) {
     const long i = i0 + r, k = k0 + tx;
@@ -135,6 +151,11 @@ __global__ void transpose_kernel(const uint8_t *__restrict__ cc, uint8_t *ccT, l
     const long k = k0 + r, i = i0 + tx;
     if (k < Lc && i < Npad) ccT[k * Npad + i] = tile[tx][r];
   }
+}
+
+__global__ void transpose_kernel(const uint8_t *__restrict__ cc, uint8_t *ccT, long N, long Lc, long Npad)
+{
+  transpose_body(cc, ccT, N, Lc, Npad, blockIdx.x, blockIdx.y);
 }
 
 //------------------------------------------------------------------------------------------------ pair
@@ -493,11 +514,14 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const unsigned char
         c.T2 += popc(b & hj & lj);
       }
       if (WPLANE) {
+        // The N plane and the clean plane of one sequence are disjoint, so each pair of cross terms (this row's N
+        // sites against the column's clean bases, and the other way round) covers disjoint sites: one popcount
+        // of their union counts both.
         const uint64_t ni = __ldg(P + 3 * Np + i), nj = __ldg(P + 3 * Np + jj);
-        c.nWc += popc(ni & cj) + popc(nj & ci);
-        c.nWh += popc(ni & hj) + popc(nj & hi);
-        c.nWl += popc(ni & lj) + popc(nj & lo);
-        c.nWt += popc(ni & hj & lj) + popc(nj & hi & lo);
+        c.nWc += popc((ni & cj) | (nj & ci));
+        c.nWh += popc((ni & hj) | (nj & hi));
+        c.nWl += popc((ni & lj) | (nj & lo));
+        c.nWt += popc((ni & hj & lj) | (nj & hi & lo));
         c.nWW += popc(ni & nj);
         if (GAPMM) c.nGG += popc(__ldg(P + 4 * Np + i) & __ldg(P + 4 * Np + jj));
       }
@@ -970,6 +994,17 @@ __device__ __forceinline__ PairView view_pair(const RowArgs &a, long i, long j, 
   return v;
 }
 
+// what the text writers need of a pair: whether it is reported, and its printed distance (tn93's "<= 0 -> 0")
+__device__ __forceinline__ bool linked_pair(const RowArgs &a, long i, long j, double &thisD)
+{
+  const RunConsts &rc = a.rc;
+  if (j >= rc.N) return false;
+  const double raw = a.dist[(size_t)(i - a.r0) * a.ncols + (j - a.colbase)];
+  if ((uint64_t)__double_as_longlong(raw) == kSkipBits) return false;
+  thisD = raw <= 0. ? 0. : raw;
+  return thisD >= rc.min_distance && thisD <= rc.threshold;
+}
+
 __device__ __forceinline__ int self_len(const RowArgs &a, long i)
 {
   if (!a.rc.report_self || a.rc.cross) return 0;
@@ -1261,7 +1296,6 @@ __device__ __forceinline__ void write_rows(const RowArgs &a, long bx, int sg)
   const long lb = rc.cross ? rc.n1 : i + 1;
   const long c0 = lb + (long)sg * kSeg, c1 = min(rc.N, c0 + kSeg);
   if (a.seg_bytes[slot] == 0) return;
-  const long cnt_i = a.counts[i];
   const int nli = a.name_len[i];
   const char *ni = a.names + a.name_off[i];
   Stager S;
@@ -1306,12 +1340,12 @@ __device__ __forceinline__ void write_rows(const RowArgs &a, long bx, int sg)
   const int dli = rc.format == 1 ? digits_of(i) : 0;
   for (long j0 = c0; j0 < c1; j0 += 32) {
     const long j = j0 + lane;
-    const PairView v = view_pair(a, i, j, cnt_i);
-    const bool put = j < c1 && v.valid && v.linked;
+    double thisD = 0.;
+    const bool put = j < c1 && linked_pair(a, i, j, thisD);
     char g[24];
     int gl = 0, len = 0;
     if (put) {
-      gl = fmt_g(v.thisD, g);
+      gl = fmt_g(thisD, g);
       len = rc.format == 0 ? nli + a.name_len[j] + gl + 3 : dli + digits_of(j) + gl + 3;
     }
     int pre = len;
@@ -1560,12 +1594,56 @@ cudaError_t launch_pair(const PairArgs &A, long ncolblocks, long nrows, cudaStre
   return minb == 3 ? launch_pair_t<3>(A, g, st) : launch_pair_t<2>(A, g, st);
 }
 
-// the tensor-core count kernel's opt-in to its dynamic shared memory, once per device
+// the tensor-core count kernels' opt-in to their dynamic shared memory, once per device
 cudaError_t tc_attr_once()
 {
   static PerDevice attr;
-  return attr.once(
-      [] { return cudaFuncSetAttribute(count_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem); });
+  return attr.once([] {
+    cudaError_t e = cudaFuncSetAttribute(count_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(count_tc_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(count_tc_persist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPSmem);
+  });
+}
+
+// TN93G_TC_KERNEL=tile selects the one-tile-per-CTA count kernel instead of the persistent one (same records)
+bool tc_tile_kernel()
+{
+  static const bool tile = [] {
+    const char *e = getenv("TN93G_TC_KERNEL");
+    return e && strcmp(e, "tile") == 0;
+  }();
+  return tile;
+}
+
+// Tensor-core counts over the count_tc_kernel grid (gx column tiles x gy row tiles) of T: the persistent kernel on
+// min(tiles, SMs) CTAs, or one CTA per tile.
+cudaError_t launch_count_grid(const TcArgs &T, long gx, long gy, int sms, cudaStream_t st)
+{
+  cudaError_t e = tc_attr_once();
+  if (e != cudaSuccess) return e;
+  if (tc_tile_kernel()) {
+    count_tc_kernel<<<dim3((unsigned)gx, (unsigned)gy), 128, kTcSmem, st>>>(T);
+  } else {
+    const long nt = gx * gy;
+    count_tc_persist_kernel<<<(unsigned)std::min<long>(nt, sms), 192, kPSmem, st>>>(T, nullptr, nullptr, 0);
+  }
+  return cudaGetLastError();
+}
+
+// the same over a list of (descriptor, first row, first column) tiles; G carries the wait limit, the error word
+// and the test hook for the persistent kernel
+cudaError_t launch_count_list(const TcArgs &G, const TcArgs *descs, const int4 *tiles, int ntiles, int sms,
+                              cudaStream_t st)
+{
+  cudaError_t e = tc_attr_once();
+  if (e != cudaSuccess) return e;
+  if (tc_tile_kernel())
+    count_tc_batch_kernel<<<(unsigned)ntiles, 128, kTcSmem, st>>>(descs, tiles);
+  else
+    count_tc_persist_kernel<<<(unsigned)std::min(ntiles, sms), 192, kPSmem, st>>>(G, descs, tiles, ntiles);
+  return cudaGetLastError();
 }
 
 }  // namespace
@@ -1757,6 +1835,13 @@ int resolve_listed(tn93g_ctx *ctx, const ReplayArgs *d_descs, const unsigned lon
   CU(cudaGetLastError());
   ctx->launches += 2;
   return TN93G_OK;
+}
+
+// a tn93g_sink that appends to the std::string at user
+int append_sink(void *user, const char *bytes, size_t n)
+{
+  static_cast<std::string *>(user)->append(bytes, n);
+  return 0;
 }
 
 // the pair stage's tables for a run: the x16 event table (with the N-plane entries) and its packed form
@@ -2086,8 +2171,8 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   rc.log_band = ctx->log_band;
   rc.log_spread = ctx->log_spread;
   rc.resolve_all = (flags & kRunResolveAll) != 0 || ctx->exact_sums;
-  const int fault = ctx->fault;
-  ctx->fault = TN93G_FAULT_NONE;  // a fault is injected into one run only
+  bool fault_pending = ctx->fault == TN93G_FAULT_SKIP_FILL;  // injected into the first count launch only
+  ctx->fault = TN93G_FAULT_NONE;
   const bool hyphy = rc.emit && opts->format == TN93G_HYPHY;
   cudaEvent_t *E = ctx->evs;
   CU(cudaEventRecord(E[0], st));
@@ -2275,7 +2360,10 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
       const long target = std::max(kTcChunkPairs, (bp + kMaxTcChunks - 2) / (kMaxTcChunks - 1));
       for (long c0 = r0; c0 < r1;) {
         long c1 = c0, pairs = 0;
-        while (c1 < r1 && (c1 == c0 || pairs < target)) pairs += rc.cross ? ncols : (N - c1++ - 1);
+        while (c1 < r1 && (c1 == c0 || pairs < target)) {
+          pairs += rc.cross ? ncols : (N - c1 - 1);
+          c1++;
+        }
         c1 = std::min(r1, (c1 + kTcRows - 1) / kTcRows * kTcRows);
         if ((int)band_chunks[b].size() == kMaxTcChunks - 1) c1 = r1;  // never more chunks than events
         band_chunks[b].push_back({c0, c1});
@@ -2301,6 +2389,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   const unsigned und_cap = (unsigned)std::min<size_t>(rc.resolve_all ? dslots : std::max<size_t>(4096, dslots / 64),
                                                       0xFFFFFFF0u);
   for (int q = 0; q < 2; q++) TRY(ensure(ctx, ctx->und[q], (size_t)und_cap * 2 * sizeof(unsigned long long)));
+  unsigned und_cap_par[2] = {und_cap, und_cap};  // grown per parity when a band lists more
   TRY(ensure(ctx, ctx->undn, 2 * sizeof(unsigned long long)));
   TRY(ensure(ctx, ctx->amb, 3 * 4 * sizeof(unsigned long long)));
   TRY(ensure(ctx, ctx->rdesc, 2 * sizeof(ReplayArgs)));
@@ -2412,7 +2501,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     ExactSink ex;
     ex.und_list = (unsigned long long *)ctx->und[par].p;
     ex.und_n = (unsigned *)((unsigned long long *)ctx->undn.p + par);
-    ex.und_cap = und_cap;
+    ex.und_cap = und_cap_par[par];
     ex.und_k = 0;
     ex.amb = (unsigned long long *)ctx->amb.p;
     ex.counts = set->d_counts;
@@ -2464,12 +2553,12 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
         T.agg16 = tc16;
         T.err = (unsigned long long *)ctx->tcerr.p;
         T.wait_ns = ctx->wait_ns;
-        T.skip_fill_block = fault == TN93G_FAULT_SKIP_FILL && bi == 0 && q == 0 ? 0 : -1;
+        T.skip_fill_block = fault_pending ? 0 : -1;
+        fault_pending = false;
         const long rt0 = c0 / kTcRows * kTcRows;
         const dim3 g((unsigned)((N - T.cstart + kTcCols - 1) / kTcCols), (unsigned)((c1 - rt0 + kTcRows - 1) / kTcRows));
         CU(cudaEventRecord(ctx->evcnt[par][2 * q], st));
-        count_tc_kernel<<<g, 128, kTcSmem, st>>>(T);
-        CU(cudaGetLastError());
+        CU(launch_count_grid(T, g.x, g.y, ctx->sms, st));
         CU(cudaEventRecord(ctx->evcnt[par][2 * q + 1], st));
         ctx->launches++;
         PairArgs AC = A;
@@ -2560,10 +2649,21 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     if (*h.und) {
       // pairs whose bytes or decisions depend on the C library's rounding of a logarithm: finish them with its
       // logarithms, then run the band's row stage again
-      if (*h.und > und_cap) {
-        cudaStreamSynchronize(st);
-        ctx->err = "more undecided pairs in a band than its list holds";
-        return TN93G_EUNDECIDED;
+      if (*h.und > und_cap_par[par]) {
+        // more than the list holds: grow this parity's list and run the band's pair stage again (the same pairs
+        // are listed; the summary bounds only widen, which keeps them valid)
+        const unsigned long long lim = std::min<unsigned long long>(dslots, 0xFFFFFFF0ull);
+        const unsigned need = (unsigned)std::min<unsigned long long>(
+            std::max<unsigned long long>(*h.und + *h.und / 4 + 1024, 2ull * und_cap_par[par]), lim);
+        CU(cudaStreamSynchronize(st));
+        TRY(ensure(ctx, ctx->und[par], (size_t)need * 2 * sizeof(unsigned long long)));
+        und_cap_par[par] = need;
+        TRY(enqueue_compute(bi));
+        CU(cudaEventSynchronize(K[4]));
+        if (*h.und > und_cap_par[par]) {
+          ctx->err = "more undecided pairs in a band than its list holds";
+          return TN93G_EUNDECIDED;
+        }
       }
       ReplayArgs *dd = (ReplayArgs *)ctx->rdesc.p + par;
       CU(cudaMemcpyAsync(dd, &rdesc_h[par], sizeof(ReplayArgs), cudaMemcpyHostToDevice, st));
@@ -2697,7 +2797,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   sum->skipped = skipped;
   sum->logs_ambiguous = (long)counters[0];
   sum->logs_resolved = resolved;
-  sum->undecided = (long)counters[1] - resolved;
+  sum->undecided = 0;  // every listed pair was finished with the C library's logarithms
   sum->pairs_replayed = (long)counters[2];
   ctx->dev_out_n = dev_off;
   if (use_tc) {
@@ -2711,10 +2811,6 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   if (counters[3]) {
     ctx->err = "internal error: a row's text did not match its counted length";
     return TN93G_ECUDA;
-  }
-  if (sum->undecided) {
-    ctx->err = "a pair's distance could not be decided exactly";
-    return TN93G_EUNDECIDED;
   }
   // The JSON numbers (maximum, means): certain for every rounding of the C library's log, or taken from a second
   // pass that finishes every pair with an ambiguous logarithm with the C library's own (rows in the same order).
@@ -3098,16 +3194,15 @@ __global__ void __launch_bounds__(256) qwrite_kernel(RowArgs a)
   const unsigned long long nb = a.seg_bytes[slot];
   if (nb == 0) return;
   const long c0 = a.seg_cols[q], c1 = a.seg_cols[q + 1], jshift = c0 - rc.n1;
-  const long cnt_i = a.counts[i];
   const int nli = a.name_len[i];
   const char *ni = a.names + a.name_off[i];
   const int dli = rc.format == 1 ? digits_of(i) : 0;
   char *o = a.out + a.seg_off[slot], *const end = o + nb;
   for (long j = c0; j < c1; j++) {
-    const PairView v = view_pair(a, i, j, cnt_i);
-    if (!(v.valid && v.linked)) continue;
+    double thisD = 0.;
+    if (!linked_pair(a, i, j, thisD)) continue;
     char g[24];
-    const int gl = fmt_g(v.thisD, g);
+    const int gl = fmt_g(thisD, g);
     const int len = rc.format == 0 ? nli + a.name_len[j] + gl + 3 : dli + digits_of(j - jshift) + gl + 3;
     if (o + len > end) {
       atomicAdd(a.err, 1ull);
@@ -3650,8 +3745,7 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
         T.wait_ns = ctx->wait_ns;
         T.skip_fill_block = -1;
         const dim3 g((unsigned)((c1 - T.cstart + kTcCols - 1) / kTcCols), (unsigned)((Nref + kTcRows - 1) / kTcRows));
-        count_tc_kernel<<<g, 128, kTcSmem, st>>>(T);
-        CU(cudaGetLastError());
+        CU(launch_count_grid(T, g.x, g.y, ctx->sms, st));
         PairArgs AC = A;
         AC.tcagg = srv->tcagg.p;
         AC.tc16 = srv->tc16;
@@ -3766,7 +3860,18 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
       return TN93G_ETIMEOUT;
     }
   }
-  const long undecided0 = (long)counters[1], ambiguous0 = (long)counters[0];
+  const long ambiguous0 = (long)counters[0];
+  // more undecided pairs than the list holds: grow it and run the batch's pair stage again (the same pairs are
+  // listed; the per-query bounds only widen)
+  auto grow_and_rerun = [&](bool resolve_all) -> int {
+    const unsigned cap = (unsigned)std::min<unsigned long long>(
+        std::max<unsigned long long>(und + und / 4 + 1024, 2ull * srv->und_cap), std::min<size_t>(dslots, 0xFFFFFFF0u));
+    TRY(ensure(ctx, srv->und, (size_t)cap * 2 * sizeof(unsigned long long)));
+    srv->und_cap = cap;
+    TRY(enqueue_pairs(resolve_all));
+    return rows_and_read();
+  };
+  if (und > srv->und_cap) TRY(grow_and_rerun(false));
   if (und) TRY(resolve_and_reread());
   // per query: the JSON numbers certain for every rounding of the C library's log, or an exact-sums pass
   CU(cudaMemcpy(ambw.data(), srv->amb.p, ambw.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
@@ -3801,6 +3906,7 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
     }
     TRY(enqueue_pairs(true));
     TRY(rows_and_read());
+    if (und > srv->und_cap) TRY(grow_and_rerun(true));
     if (und) TRY(resolve_and_reread());
     fill_summaries();
   }
@@ -3860,7 +3966,7 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
       X.pairs_replayed = (long)counters[2];
       X.logs_ambiguous = ambiguous0;
       X.logs_resolved = resolved;
-      X.undecided = undecided0 - std::min<long>(undecided0, resolved);
+      X.undecided = 0;  // every listed pair was finished with the C library's logarithms
       X.sums_repass = repass ? 1 : 0;
     }
     if (rc.emit && sink && sink(user, q, (const char *)srv->pin + qoff[q], (size_t)(qoff[q + 1] - qoff[q])))
@@ -3883,9 +3989,100 @@ enum BatchBuf {
   BB_NAMES, BB_NAMEOFF, BB_NAMELEN, BB_COUNTS, BB_DIST, BB_RQ, BB_RQN, BB_COUNTERS, BB_PDESC, BB_RDESC, BB_ROWDESC,
   BB_TILES, BB_NEXT, BB_BLOCKS, BB_SBYTES, BB_SOFF, BB_SLINKS, BB_SSKIP, BB_SMAX, BB_RSUM, BB_RW, BB_HIST, BB_TOTAL,
   BB_SCANTMP, BB_RED, BB_REDC, BB_FIRST, BB_FIRSTIDX, BB_OUT, BB_OH, BB_TCAGG, BB_TCDESC, BB_TCTILES, BB_TCERR,
-  BB_UND, BB_UNDN, BB_AMB, BB_COUNT
+  BB_UND, BB_UNDN, BB_AMB, BB_SCANDESC, BB_PACKDESC, BB_TRDESC, BB_OHDESC, BB_BOFF, BB_COUNT
 };
 static_assert(BB_COUNT <= kBatchBufs, "batch buffer table");
+
+// Packing of a batch, one launch per step over all alignments: block b belongs to the alignment k with
+// off[k] <= b < off[k + 1] (off[] is the prefix sum of the alignments' block counts) and is its block b - off[k].
+__device__ __forceinline__ int batch_owner(const int *off, int K, int b)
+{
+  int lo = 0, hi = K - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= b)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+struct ScanDesc {
+  const uint8_t *codes;
+  long N, L;
+  uint32_t *seen;
+  unsigned long long *nN;
+};
+struct TransDesc {
+  const uint8_t *cc;
+  uint8_t *ccT;
+  long N, Lc, Npad;
+};
+struct OneHotDesc {
+  const uint8_t *cc;
+  long N, Lc, NB, KS;
+  uint8_t *img;
+};
+
+__global__ void __launch_bounds__(256) colscan_batch_kernel(const ScanDesc *d, const int *off, int K)
+{
+  const int k = batch_owner(off, K, blockIdx.x);
+  const long lb = (long)blockIdx.x - off[k];
+  const ScanDesc &a = d[k];
+  const long gx = (a.L + 255) / 256;
+  colscan_body(a.codes, a.N, a.L, a.seen, a.nN, lb % gx, lb / gx);
+}
+
+// one block per (8 sequences, one 64-column word)
+__global__ void __launch_bounds__(256) pack_batch_kernel(const PackArgs *d, const int *off, int K)
+{
+  const int k = batch_owner(off, K, blockIdx.x);
+  const long lb = (long)blockIdx.x - off[k];
+  const PackArgs &a = d[k];
+  const long gx = (a.N + kWarps - 1) / kWarps;
+  pack_body(a, lb % gx, lb / gx, a.W);
+}
+
+__global__ void __launch_bounds__(256) events_batch_kernel(const PackArgs *d, const int *off, int K)
+{
+  const int k = batch_owner(off, K, blockIdx.x);
+  events_body(d[k], (long)blockIdx.x - off[k]);
+}
+
+__global__ void __launch_bounds__(256) transpose_batch_kernel(const TransDesc *d, const int *off, int K)
+{
+  const int k = batch_owner(off, K, blockIdx.x);
+  const long lb = (long)blockIdx.x - off[k];
+  const TransDesc &a = d[k];
+  const long gx = (a.Lc + 31) / 32;
+  transpose_body(a.cc, a.ccT, a.N, a.Lc, a.Npad, lb % gx, lb / gx);
+}
+
+__global__ void __launch_bounds__(256) onehot_batch_kernel(const OneHotDesc *d, const int *off, int K)
+{
+  const int k = batch_owner(off, K, blockIdx.x);
+  const OneHotDesc &a = d[k];
+  onehot_body(a.cc, a.N, a.Lc, a.NB, a.KS, a.img, 0, a.NB * 32, (long)blockIdx.x - off[k]);
+}
+
+// the prefix sum of per-alignment block counts, uploaded to slot q of the offsets buffer; returns the total
+int upload_offsets(tn93g_ctx *ctx, DevBuf &buf, int q, int K, const std::vector<long> &blocks, cudaStream_t st,
+                   int *total)
+{
+  std::vector<int> off(K + 1);
+  long t = 0;
+  for (int k = 0; k < K; k++) {
+    off[k] = (int)t;
+    t += blocks[k];
+  }
+  off[K] = (int)t;
+  if (t >= (1l << 31)) return TN93G_ETOOBIG;
+  CU(cudaMemcpyAsync((int *)buf.p + (size_t)q * (K + 1), off.data(), (K + 1) * sizeof(int), cudaMemcpyHostToDevice,
+                     st));
+  *total = (int)t;
+  return TN93G_OK;
+}
 
 __global__ void gather_u64_kernel(const unsigned long long *src, const long *idx, unsigned long long *dst, int n)
 {
@@ -3986,13 +4183,29 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
   TRY(ensure(ctx, bb[BB_NN], K * sizeof(unsigned long long)));
   CU(cudaMemsetAsync(bb[BB_SEEN].p, 0, seen_off[K] * sizeof(uint32_t), st));
   CU(cudaMemsetAsync(bb[BB_NN].p, 0, K * sizeof(unsigned long long), st));
-  for (int k = 0; k < K; k++) {
-    const long N = alns[k].n, L = alns[k].L;
-    colscan_kernel<<<dim3((unsigned)((L + 255) / 256), (unsigned)((N + 63) / 64)), 256, 0, st>>>(
-        (const uint8_t *)bb[BB_CODES].p + code_off[k], N, L, (uint32_t *)bb[BB_SEEN].p + seen_off[k],
-        (unsigned long long *)bb[BB_NN].p + k);
-    CU(cudaGetLastError());
-    ctx->launches++;
+  TRY(ensure(ctx, bb[BB_BOFF], 5 * (size_t)(K + 1) * sizeof(int)));
+  TRY(ensure(ctx, bb[BB_SCANDESC], K * sizeof(ScanDesc)));
+  TRY(ensure(ctx, bb[BB_PACKDESC], K * sizeof(PackArgs)));
+  TRY(ensure(ctx, bb[BB_TRDESC], K * sizeof(TransDesc)));
+  TRY(ensure(ctx, bb[BB_OHDESC], K * sizeof(OneHotDesc)));
+  const int *boff = (const int *)bb[BB_BOFF].p;
+  {
+    std::vector<ScanDesc> sd(K);
+    std::vector<long> nb(K);
+    for (int k = 0; k < K; k++) {
+      const long N = alns[k].n, L = alns[k].L;
+      sd[k] = ScanDesc{(const uint8_t *)bb[BB_CODES].p + code_off[k], N, L, (uint32_t *)bb[BB_SEEN].p + seen_off[k],
+                       (unsigned long long *)bb[BB_NN].p + k};
+      nb[k] = ((L + 255) / 256) * ((N + 63) / 64);
+    }
+    CU(cudaMemcpyAsync(bb[BB_SCANDESC].p, sd.data(), K * sizeof(ScanDesc), cudaMemcpyHostToDevice, st));
+    int total = 0;
+    TRY(upload_offsets(ctx, bb[BB_BOFF], 0, K, nb, st, &total));
+    if (total) {
+      colscan_batch_kernel<<<(unsigned)total, 256, 0, st>>>((const ScanDesc *)bb[BB_SCANDESC].p, boff, K);
+      CU(cudaGetLastError());
+      ctx->launches++;
+    }
   }
   std::vector<uint32_t> seen(seen_off[K]);
   std::vector<unsigned long long> nN(K);
@@ -4073,14 +4286,33 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
     pa.cc = (uint8_t *)bb[BB_CC].p + cc_off[k];
     pa.evcount = (uint32_t *)bb[BB_EVCOUNT].p + row_base[k];
     pa.ev_off = (const uint32_t *)bb[BB_EVOFF].p + evo_off[k];
-    if (rc.W) {
-      pack_kernel<<<dim3((unsigned)((rc.N + kWarps - 1) / kWarps), (unsigned)std::min<long>(rc.W, 65535)), 256, 0,
-                    st>>>(pa);
+    pa.ev = nullptr;
+  }
+  {
+    // bit planes and codes (one block per 8 sequences and word), and the transposed codes, of every alignment
+    std::vector<long> nbp(K), nbt(K);
+    std::vector<TransDesc> td(K);
+    for (int k = 0; k < K; k++) {
+      const RunConsts &rc = RC[k];
+      nbp[k] = rc.W ? ((rc.N + kWarps - 1) / kWarps) * rc.W : 0;
+      nbt[k] = rc.W ? ((rc.Lc + 31) / 32) * (rc.Npad / 32) : 0;
+      td[k] = TransDesc{PA[k].cc, (uint8_t *)bb[BB_CCT].p + cct_off[k], rc.N, rc.Lc, rc.Npad};
+    }
+    CU(cudaMemcpyAsync(bb[BB_PACKDESC].p, PA.data(), K * sizeof(PackArgs), cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(bb[BB_TRDESC].p, td.data(), K * sizeof(TransDesc), cudaMemcpyHostToDevice, st));
+    int tp = 0, tt = 0;
+    TRY(upload_offsets(ctx, bb[BB_BOFF], 1, K, nbp, st, &tp));
+    TRY(upload_offsets(ctx, bb[BB_BOFF], 2, K, nbt, st, &tt));
+    if (tp) {
+      pack_batch_kernel<<<(unsigned)tp, 256, 0, st>>>((const PackArgs *)bb[BB_PACKDESC].p, boff + (K + 1), K);
       CU(cudaGetLastError());
-      transpose_kernel<<<dim3((unsigned)((rc.Lc + 31) / 32), (unsigned)(rc.Npad / 32)), dim3(32, 8), 0, st>>>(
-          pa.cc, (uint8_t *)bb[BB_CCT].p + cct_off[k], rc.N, rc.Lc, rc.Npad);
+      ctx->launches++;
+    }
+    if (tt) {
+      transpose_batch_kernel<<<(unsigned)tt, dim3(32, 8), 0, st>>>((const TransDesc *)bb[BB_TRDESC].p,
+                                                                  boff + 2 * (K + 1), K);
       CU(cudaGetLastError());
-      ctx->launches += 2;
+      ctx->launches++;
     }
   }
   std::vector<uint32_t> evc(NR), evo(evo_off[K]);
@@ -4100,10 +4332,18 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
   if (nev >= (1ull << 32)) return TN93G_ETOOBIG;
   TRY(ensure(ctx, bb[BB_EV], std::max<size_t>(nev, 1) * sizeof(uint32_t)));
   CU(cudaMemcpyAsync(bb[BB_EVOFF].p, evo.data(), evo_off[K] * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-  for (int k = 0; k < K; k++) {
-    PA[k].ev = (uint32_t *)bb[BB_EV].p;
-    if (RC[k].W && evo[evo_off[k] + alns[k].n] > evo[evo_off[k]]) {
-      events_kernel<<<(unsigned)((RC[k].N + kWarps - 1) / kWarps), 256, 0, st>>>(PA[k]);
+  {
+    // every alignment's sparse events (one block per 8 sequences)
+    std::vector<long> nbe(K);
+    for (int k = 0; k < K; k++) {
+      PA[k].ev = (uint32_t *)bb[BB_EV].p;
+      nbe[k] = (RC[k].W && evo[evo_off[k] + alns[k].n] > evo[evo_off[k]]) ? (RC[k].N + kWarps - 1) / kWarps : 0;
+    }
+    CU(cudaMemcpyAsync(bb[BB_PACKDESC].p, PA.data(), K * sizeof(PackArgs), cudaMemcpyHostToDevice, st));
+    int te = 0;
+    TRY(upload_offsets(ctx, bb[BB_BOFF], 3, K, nbe, st, &te));
+    if (te) {
+      events_batch_kernel<<<(unsigned)te, 256, 0, st>>>((const PackArgs *)bb[BB_PACKDESC].p, boff + 3 * (K + 1), K);
       CU(cudaGetLastError());
       ctx->launches++;
     }
@@ -4251,6 +4491,8 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
     TRY(ensure(ctx, bb[BB_TCAGG], std::max<size_t>(ag_off[K], 16)));
     TRY(ensure(ctx, bb[BB_TCERR], sizeof(unsigned long long)));
     CU(cudaMemsetAsync(bb[BB_TCERR].p, 0, sizeof(unsigned long long), st));
+    std::vector<OneHotDesc> ohd(K);
+    std::vector<long> nbo(K, 0);
     for (int k : order) {
       if (oh_off[k + 1] == oh_off[k]) continue;
       TcArgs &T = TD[k];
@@ -4260,28 +4502,36 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
       T.err = (unsigned long long *)bb[BB_TCERR].p;
       T.wait_ns = ctx->wait_ns;
       T.skip_fill_block = -1;
-      const long nthr = T.NB * 32 * T.KS * (kTcStageK / 16);
-      onehot_kernel<<<(unsigned)((nthr + 255) / 256), 256, 0, st>>>(PA[k].cc, T.N, RC[k].Lc, T.NB, T.KS,
-                                                                    (uint8_t *)bb[BB_OH].p + oh_off[k], 0, T.NB * 32);
-      CU(cudaGetLastError());
-      ctx->launches++;
+      ohd[k] = OneHotDesc{PA[k].cc, T.N, RC[k].Lc, T.NB, T.KS, (uint8_t *)bb[BB_OH].p + oh_off[k]};
+      nbo[k] = (T.NB * 32 * T.KS * (kTcStageK / 16) + 255) / 256;
       for (long i0 = 0; i0 < T.N - 1; i0 += kTcRows)
         for (long j0 = (i0 + 1) / kTcCols * kTcCols; j0 < T.N; j0 += kTcCols) tct.push_back(make_int4(k, (int)i0, (int)j0, 0));
       PD[k].tcagg = T.agg;
       PD[k].tc16 = T.agg16;
+    }
+    {
+      // every alignment's one-hot operand image in one launch
+      int to = 0;
+      TRY(upload_offsets(ctx, bb[BB_BOFF], 4, K, nbo, st, &to));
+      CU(cudaMemcpyAsync(bb[BB_OHDESC].p, ohd.data(), K * sizeof(OneHotDesc), cudaMemcpyHostToDevice, st));
+      if (to) {
+        onehot_batch_kernel<<<(unsigned)to, 256, 0, st>>>((const OneHotDesc *)bb[BB_OHDESC].p, boff + 4 * (K + 1), K);
+        CU(cudaGetLastError());
+        ctx->launches++;
+      }
     }
     if (!tct.empty()) {
       TRY(ensure(ctx, bb[BB_TCDESC], K * sizeof(TcArgs)));
       TRY(ensure(ctx, bb[BB_TCTILES], tct.size() * sizeof(int4)));
       CU(cudaMemcpyAsync(bb[BB_TCDESC].p, TD.data(), K * sizeof(TcArgs), cudaMemcpyHostToDevice, st));
       CU(cudaMemcpyAsync(bb[BB_TCTILES].p, tct.data(), tct.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
-      static PerDevice attr;
-      CU(attr.once([] {
-        return cudaFuncSetAttribute(count_tc_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem);
-      }));
-      count_tc_batch_kernel<<<(unsigned)tct.size(), 128, kTcSmem, st>>>((const TcArgs *)bb[BB_TCDESC].p,
-                                                                      (const int4 *)bb[BB_TCTILES].p);
-      CU(cudaGetLastError());
+      TcArgs G;
+      memset(&G, 0, sizeof G);
+      G.err = (unsigned long long *)bb[BB_TCERR].p;
+      G.wait_ns = ctx->wait_ns;
+      G.skip_fill_block = -1;
+      CU(launch_count_list(G, (const TcArgs *)bb[BB_TCDESC].p, (const int4 *)bb[BB_TCTILES].p, (int)tct.size(),
+                           ctx->sms, st));
       ctx->launches++;
     }
   }
@@ -4423,13 +4673,11 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
   };
   TRY(rows_and_read());
   long resolved = 0;
-  if (und) {
+  // more undecided pairs than the list holds: the alignments that listed any run again alone below
+  const bool overflow = und > und_cap;
+  if (und && !overflow) {
     // pairs whose bytes or decisions depend on the C library's rounding of a logarithm: finished with its
     // logarithms, then the row stage runs again
-    if (und > und_cap) {
-      ctx->err = "more undecided pairs in a batch than its list holds";
-      return TN93G_EUNDECIDED;
-    }
     TRY(resolve_listed(ctx, (const ReplayArgs *)bb[BB_RDESC].p, (const unsigned long long *)bb[BB_UND].p,
                        (unsigned)und, st));
     resolved = (long)und;
@@ -4491,6 +4739,24 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
     S.output_bytes = RC[k].emit ? first[k + 1] - first[k] : 0;
   }
   (void)resolved;
+  // After an overflow of the undecided list, every alignment that listed a pair runs again alone through
+  // tn93g_run's path (which grows its list as needed): its text and summary replace the batch's.
+  std::vector<std::string> redo_text(K);
+  std::vector<char> redone(K, 0);
+  if (overflow) {
+    for (int k = 0; k < K; k++) {
+      if (!counters[4 * k + 1]) continue;
+      const tn93g_alignment &A = alns[k];
+      tn93g_set *set = nullptr;
+      TRY(tn93g_upload(ctx, &set, A.codes, A.n, A.L, A.copy_counts, A.names, A.name_off, A.name_len));
+      tn93g_summary S2;
+      const int r = run_impl(ctx, set, A.n, &opts[k], append_sink, &redo_text[k], &S2, false);
+      tn93g_free_set(ctx, set);
+      TRY(r);
+      sums[k] = S2;
+      redone[k] = 1;
+    }
+  }
   // Per alignment: the JSON numbers certain for every rounding of the C library's log, or the alignment runs
   // again alone through tn93g_run's path, whose exact-sums pass gives its maximum and mean (its text and counts
   // are certified pair by pair already).
@@ -4498,6 +4764,7 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
     std::vector<unsigned long long> ambw((size_t)K * 4);
     CU(cudaMemcpy(ambw.data(), bb[BB_AMB].p, ambw.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
     for (int k = 0; k < K; k++) {
+      if (redone[k]) continue;
       tn93g_summary &S = sums[k];
       amb_bounds(&ambw[(size_t)k * 4], S.amb_bounds[0]);
       if (summary_certified(&S, S.amb_bounds, 2 * alns[k].n + 2, 0)) continue;
@@ -4518,8 +4785,11 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
     }
   }
   if (any_emit && sink)
-    for (int k = 0; k < K; k++)
-      if (RC[k].emit && sink(user, k, (const char *)ctx->pinned + first[k], (size_t)(first[k + 1] - first[k])))
-        return TN93G_ESINK;
+    for (int k = 0; k < K; k++) {
+      if (!RC[k].emit) continue;
+      const int r = redone[k] ? sink(user, k, redo_text[k].data(), redo_text[k].size())
+                              : sink(user, k, (const char *)ctx->pinned + first[k], (size_t)(first[k + 1] - first[k]));
+      if (r) return TN93G_ESINK;
+    }
   return TN93G_OK;
 }

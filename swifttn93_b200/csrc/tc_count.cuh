@@ -148,10 +148,10 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16])
 
 // one thread per (sequence, 16 columns): the four class rows' 16 bytes of the operand image, for the sequences
 // [seq0, seq0 + nseq) (seq0 and nseq multiples of 32; sequences at or past N get zero rows)
-__global__ void onehot_kernel(const uint8_t *__restrict__ cc, long N, long Lc, long NB, long KS, uint8_t *img,
-                              long seq0, long nseq)
+__device__ __forceinline__ void onehot_body(const uint8_t *__restrict__ cc, long N, long Lc, long NB, long KS,
+                                            uint8_t *img, long seq0, long nseq, long bx)
 {
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long t = bx * 256l + threadIdx.x;
   const long nchunk = KS * (kTcStageK / 16);
   if (t >= nseq * nchunk) return;
   const long seq = seq0 + t / nchunk, ch = t % nchunk;
@@ -171,6 +171,83 @@ __global__ void onehot_kernel(const uint8_t *__restrict__ cc, long N, long Lc, l
       w[q] = (uint32_t)(code[4 * q] == cls) | ((uint32_t)(code[4 * q + 1] == cls) << 8) |
              ((uint32_t)(code[4 * q + 2] == cls) << 16) | ((uint32_t)(code[4 * q + 3] == cls) << 24);
     *reinterpret_cast<uint4 *>(blk + (r / 8) * 1024 + c * 128 + (r % 8) * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+__global__ void onehot_kernel(const uint8_t *__restrict__ cc, long N, long Lc, long NB, long KS, uint8_t *img,
+                              long seq0, long nseq)
+{
+  onehot_body(cc, N, Lc, NB, KS, img, seq0, nseq, blockIdx.x);
+}
+
+// Reads the accumulator of tile (i0, j0) (tensor memory from tacc, lane quarter q = 32 rows: sequences
+// i0 + 8q .. i0 + 8q + 7, four class rows each) and stores each pair's record. All 32 lanes of the warp call it.
+__device__ __forceinline__ void tc_tile_epilogue(const TcArgs &a, long i0, long j0, uint32_t tacc, int q, int lane)
+{
+  const int il = q * 8 + lane / 4, cls = lane & 3;
+  const long i = i0 + il;
+  for (int c16 = 0; c16 < 256 / 16; c16++) {
+    uint32_t v[16];
+    tmem_ld16(tacc + ((uint32_t)(q * 32) << 16) + (uint32_t)(c16 * 16), v);
+    // v[4 * jj + b] = N_{cls, b}(i, j = 4 * c16 + jj)
+    int T[4], dg[4], ag[4], ct[4], col[4][4], rowm[4];
+#pragma unroll
+    for (int jj = 0; jj < 4; jj++) {
+      const int n0 = (int)v[4 * jj], n1 = (int)v[4 * jj + 1], n2 = (int)v[4 * jj + 2], n3 = (int)v[4 * jj + 3];
+      rowm[jj] = n0 + n1 + n2 + n3;
+      T[jj] = rowm[jj];
+      dg[jj] = cls == 0 ? n0 : cls == 1 ? n1 : cls == 2 ? n2 : n3;
+      ag[jj] = cls == 0 ? n2 : cls == 2 ? n0 : 0;
+      ct[jj] = cls == 1 ? n3 : cls == 3 ? n1 : 0;
+      col[jj][0] = n0;
+      col[jj][1] = n1;
+      col[jj][2] = n2;
+      col[jj][3] = n3;
+    }
+    // totals over the four class rows of sequence i (lanes 4m..4m+3)
+#pragma unroll
+    for (int o = 1; o < 4; o <<= 1)
+#pragma unroll
+      for (int jj = 0; jj < 4; jj++) {
+        T[jj] += __shfl_xor_sync(0xffffffffu, T[jj], o);
+        dg[jj] += __shfl_xor_sync(0xffffffffu, dg[jj], o);
+        ag[jj] += __shfl_xor_sync(0xffffffffu, ag[jj], o);
+        ct[jj] += __shfl_xor_sync(0xffffffffu, ct[jj], o);
+#pragma unroll
+        for (int b = 0; b < 3; b++) col[jj][b] += __shfl_xor_sync(0xffffffffu, col[jj][b], o);
+      }
+    // this lane finishes column jj = cls: base counts of A, C, G over both sequences
+    const int base = lane & ~3;
+    int out[7] = {0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int jj = 0; jj < 4; jj++) {
+      const int rA = __shfl_sync(0xffffffffu, rowm[jj], base + 0);
+      const int rC = __shfl_sync(0xffffffffu, rowm[jj], base + 1);
+      const int rG = __shfl_sync(0xffffffffu, rowm[jj], base + 2);
+      if (jj == cls) {
+        out[0] = T[jj];
+        out[1] = dg[jj];
+        out[2] = ag[jj];
+        out[3] = ct[jj];
+        out[4] = rA + col[jj][0];
+        out[5] = rC + col[jj][1];
+        out[6] = rG + col[jj][2];
+      }
+    }
+    const long j = j0 + 4 * c16 + cls;
+    const long lb = a.cross ? a.n1 : i + 1;
+    if (i >= a.r0 && i < a.r1 && j >= lb && j >= a.colbase && j < a.N && j < a.cend) {
+      const size_t at = (size_t)(i - a.r0) * a.ncols + (j - a.colbase);
+      if (a.agg16) {
+        reinterpret_cast<uint4 *>(a.agg)[at] =
+            make_uint4((uint32_t)out[0] | (uint32_t)out[1] << 16, (uint32_t)out[2] | (uint32_t)out[3] << 16,
+                       (uint32_t)out[4] | (uint32_t)out[5] << 16, (uint32_t)out[6]);
+      } else {
+        uint4 *dst = reinterpret_cast<uint4 *>(a.agg) + 2 * at;
+        dst[0] = make_uint4((uint32_t)out[0], (uint32_t)out[1], (uint32_t)out[2], (uint32_t)out[3]);
+        dst[1] = make_uint4((uint32_t)out[4], (uint32_t)out[5], (uint32_t)out[6], 0u);
+      }
+    }
   }
 }
 
@@ -253,73 +330,7 @@ __device__ __forceinline__ void count_tc_tile(const TcArgs &a, long i0, long j0)
   const bool ok = __all_sync(0xffffffffu, mbar_wait(&done, 0, lim));
   tc_fence_after();
   const bool go = __all_sync(0xffffffffu, ok && !*(volatile int *)&abort_flag);
-  if (go) {
-    const int il = warp * 8 + lane / 4, cls = lane & 3;
-    const long i = i0 + il;
-    for (int c16 = 0; c16 < 256 / 16; c16++) {
-      uint32_t v[16];
-      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c16 * 16), v);
-      // v[4 * jj + b] = N_{cls, b}(i, j = 4 * c16 + jj)
-      int T[4], dg[4], ag[4], ct[4], col[4][4], rowm[4];
-#pragma unroll
-      for (int jj = 0; jj < 4; jj++) {
-        const int n0 = (int)v[4 * jj], n1 = (int)v[4 * jj + 1], n2 = (int)v[4 * jj + 2], n3 = (int)v[4 * jj + 3];
-        rowm[jj] = n0 + n1 + n2 + n3;
-        T[jj] = rowm[jj];
-        dg[jj] = cls == 0 ? n0 : cls == 1 ? n1 : cls == 2 ? n2 : n3;
-        ag[jj] = cls == 0 ? n2 : cls == 2 ? n0 : 0;
-        ct[jj] = cls == 1 ? n3 : cls == 3 ? n1 : 0;
-        col[jj][0] = n0;
-        col[jj][1] = n1;
-        col[jj][2] = n2;
-        col[jj][3] = n3;
-      }
-      // totals over the four class rows of sequence i (lanes 4m..4m+3)
-#pragma unroll
-      for (int o = 1; o < 4; o <<= 1)
-#pragma unroll
-        for (int jj = 0; jj < 4; jj++) {
-          T[jj] += __shfl_xor_sync(0xffffffffu, T[jj], o);
-          dg[jj] += __shfl_xor_sync(0xffffffffu, dg[jj], o);
-          ag[jj] += __shfl_xor_sync(0xffffffffu, ag[jj], o);
-          ct[jj] += __shfl_xor_sync(0xffffffffu, ct[jj], o);
-#pragma unroll
-          for (int b = 0; b < 3; b++) col[jj][b] += __shfl_xor_sync(0xffffffffu, col[jj][b], o);
-        }
-      // this lane finishes column jj = cls: base counts of A, C, G over both sequences
-      const int base = lane & ~3;
-      int out[7] = {0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-      for (int jj = 0; jj < 4; jj++) {
-        const int rA = __shfl_sync(0xffffffffu, rowm[jj], base + 0);
-        const int rC = __shfl_sync(0xffffffffu, rowm[jj], base + 1);
-        const int rG = __shfl_sync(0xffffffffu, rowm[jj], base + 2);
-        if (jj == cls) {
-          out[0] = T[jj];
-          out[1] = dg[jj];
-          out[2] = ag[jj];
-          out[3] = ct[jj];
-          out[4] = rA + col[jj][0];
-          out[5] = rC + col[jj][1];
-          out[6] = rG + col[jj][2];
-        }
-      }
-      const long j = j0 + 4 * c16 + cls;
-      const long lb = a.cross ? a.n1 : i + 1;
-      if (i >= a.r0 && i < a.r1 && j >= lb && j >= a.colbase && j < a.N && j < a.cend) {
-        const size_t at = (size_t)(i - a.r0) * a.ncols + (j - a.colbase);
-        if (a.agg16) {
-          reinterpret_cast<uint4 *>(a.agg)[at] =
-              make_uint4((uint32_t)out[0] | (uint32_t)out[1] << 16, (uint32_t)out[2] | (uint32_t)out[3] << 16,
-                         (uint32_t)out[4] | (uint32_t)out[5] << 16, (uint32_t)out[6]);
-        } else {
-          uint4 *dst = reinterpret_cast<uint4 *>(a.agg) + 2 * at;
-          dst[0] = make_uint4((uint32_t)out[0], (uint32_t)out[1], (uint32_t)out[2], (uint32_t)out[3]);
-          dst[1] = make_uint4((uint32_t)out[4], (uint32_t)out[5], (uint32_t)out[6], 0u);
-        }
-      }
-    }
-  }
+  if (go) tc_tile_epilogue(a, i0, j0, tmem, warp, lane);
   // On a timeout: report it, let the last fill of each stage land before the ring is released (a stage is
   // refilled only after its previous fill was consumed, so only the last fill can still be in flight), and make
   // sure every MMA this CTA issued has completed before its tensor memory is freed: the issuer commits `done`
@@ -347,6 +358,189 @@ __global__ void __launch_bounds__(128) count_tc_batch_kernel(const TcArgs *descs
 {
   const int4 t = tiles[blockIdx.x];
   count_tc_tile(descs[t.x], t.y, t.z);
+}
+
+// ---- persistent form ----------------------------------------------------------------------------------------
+// One CTA per SM loops over the tiles (t = blockIdx.x, + gridDim.x, ...), with its roles in separate warps:
+//   warp 0 (one lane)  producer: the A' and B' blocks of every stage into a 4-stage ring (cp.async.bulk, mbarrier
+//                      transaction counts);
+//   warp 1 (one lane)  MMA issuer: 4 tcgen05.mma per stage into one of two accumulators (2 x 256 tensor-memory
+//                      columns), each stage committed back to the producer, each finished tile to the epilogue;
+//   warps 2-5          epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. +31 of a finished accumulator,
+//                      stores the records and hands the accumulator back to the MMA issuer.
+// So tile t's epilogue overlaps tile t+1's copies and MMAs. Every wait is bounded (TcArgs::wait_ns); a wait that
+// gives up stops every role, and the CTA lets its copies land and its MMAs complete (bounded) before it frees its
+// tensor memory. Tiles come from a grid over one band (tiles == nullptr: the count_tc_kernel grid of `ga`) or
+// from a list of (descriptor, first row, first column) (a batch of alignments).
+constexpr int kPStages = 4;
+constexpr size_t kPSmem = (size_t)kPStages * kTcStageBytes + 1024;
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool tc_tile_valid(const TcArgs &a, long i0, long j0)
+{
+  if (i0 >= a.r1 || j0 >= a.N || j0 >= a.cend) return false;
+  if (!a.cross && j0 + kTcCols - 1 <= i0) return false;
+  if (a.cross && j0 + kTcCols <= a.n1) return false;
+  return true;
+}
+
+__global__ void __launch_bounds__(192, 1)
+    count_tc_persist_kernel(TcArgs ga, const TcArgs *descs, const int4 *tiles, int ntiles)
+{
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  __shared__ __align__(8) uint64_t full[kPStages], empty[kPStages], accf[2], acce[2], done;
+  __shared__ uint32_t tmem_base;
+  __shared__ int abort_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool listed = tiles != nullptr;
+  const long rt0 = listed ? 0 : ga.r0 / kTcRows * kTcRows;
+  const long ntx = listed ? 1 : (ga.N - ga.cstart + kTcCols - 1) / kTcCols;
+  const long ntot = listed ? (long)ntiles : ntx * ((ga.r1 - rt0 + kTcRows - 1) / kTcRows);
+  const uint64_t lim = ga.wait_ns;
+  auto tile = [&](long t, const TcArgs *&A, long &i0, long &j0) -> bool {
+    if (listed) {
+      const int4 x = tiles[t];
+      A = &descs[x.x];
+      i0 = x.y;
+      j0 = x.z;
+    } else {
+      A = &ga;
+      i0 = rt0 + (t / ntx) * kTcRows;
+      j0 = ga.cstart + (t % ntx) * kTcCols;
+    }
+    return tc_tile_valid(*A, i0, j0);
+  };
+  unsigned char *ring = (unsigned char *)(((uintptr_t)tsm + 1023) & ~(uintptr_t)1023);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kPStages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 4);
+    }
+    mbar_init(&done, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(512u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base;
+  // producer state kept for the drain: the phase of each stage's last fill (-1: never filled)
+  long last_phase[kPStages] = {-1, -1, -1, -1};
+  if (warp == 0 && lane == 0) {
+    bool skip = ga.skip_fill_block >= 0 && (long)blockIdx.x == ga.skip_fill_block;
+    uint32_t g = 0;
+    for (long t = blockIdx.x; t < ntot && !*(volatile int *)&abort_flag; t += gridDim.x) {
+      const TcArgs *A;
+      long i0, j0;
+      if (!tile(t, A, i0, j0)) continue;
+      const long ab = i0 / 32, bb = j0 / 32;
+      for (long k = 0; k < A->KS; k++, g++) {
+        const int s = (int)(g % kPStages);
+        if (g >= kPStages && !mbar_wait(&empty[s], ((g / kPStages) - 1) & 1, lim)) {
+          atomicExch(&abort_flag, 1);
+          break;
+        }
+        if (*(volatile int *)&abort_flag) break;
+        if (skip) {  // test hook: this stage never fills, so the MMA issuer's wait runs out
+          skip = false;
+          continue;
+        }
+        unsigned char *dst = ring + (size_t)s * kTcStageBytes;
+        mbar_arrive_expect_tx(&full[s], (uint32_t)kTcStageBytes);
+        bulk_g2s(dst, A->onehot + ((size_t)k * A->NB + ab) * kTcBlockBytes, kTcBlockBytes, &full[s]);
+        bulk_g2s(dst + kTcBlockBytes, A->onehot + ((size_t)k * A->NB + bb) * kTcBlockBytes, 2 * kTcBlockBytes,
+                 &full[s]);
+        last_phase[s] = (long)(g / kPStages);
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    uint32_t g = 0, u = 0;
+    for (long t = blockIdx.x; t < ntot && !*(volatile int *)&abort_flag; t += gridDim.x) {
+      const TcArgs *A;
+      long i0, j0;
+      if (!tile(t, A, i0, j0)) continue;
+      const uint32_t b = u & 1;
+      if (u >= 2 && !mbar_wait(&acce[b], ((u / 2) - 1) & 1, lim)) {
+        atomicExch(&abort_flag, 1);
+        break;
+      }
+      tc_fence_after();
+      const uint32_t acc = tmem + b * 256;
+      bool ok = true;
+      for (long k = 0; k < A->KS; k++, g++) {
+        const int s = (int)(g % kPStages);
+        if (!mbar_wait(&full[s], (g / kPStages) & 1, lim)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sa = smem_u32(ring + (size_t)s * kTcStageBytes), sb = sa + kTcBlockBytes;
+#pragma unroll
+        for (int kk = 0; kk < kTcStageK / 32; kk++)
+          umma_i8(acc, umma_desc(sa + kk * 256, 128, 1024), umma_desc(sb + kk * 256, 128, 1024),
+                  (k > 0 || kk > 0) ? 1u : 0u);
+        umma_commit(&empty[s]);
+      }
+      if (!ok) {
+        atomicExch(&abort_flag, 1);
+        break;
+      }
+      umma_commit(&accf[b]);
+      u++;
+    }
+    umma_commit(&done);  // arrives when every MMA issued above has completed
+  } else if (warp >= 2) {
+    const int q = warp & 3;  // tensor-memory lane quarter this warp may read
+    uint32_t u = 0;
+    for (long t = blockIdx.x; t < ntot; t += gridDim.x) {
+      const int stop = __shfl_sync(0xffffffffu, lane == 0 ? *(volatile int *)&abort_flag : 0, 0);
+      if (stop) break;
+      const TcArgs *A;
+      long i0, j0;
+      if (!tile(t, A, i0, j0)) continue;
+      const uint32_t b = u & 1;
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&accf[b], (u / 2) & 1, lim));
+      if (!ok) {
+        if (lane == 0) atomicExch(&abort_flag, 1);
+        break;
+      }
+      tc_fence_after();
+      tc_tile_epilogue(*A, i0, j0, tmem + b * 256, q, lane);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce[b]);
+      u++;
+    }
+  }
+  __syncwarp();
+  __syncthreads();
+  // Every MMA this CTA issued has completed once `done` arrives (the issuer commits it on every path); after a
+  // timeout, the last fill of each stage also lands before the ring is released.
+  if (threadIdx.x == 0) {
+    if (*(volatile int *)&abort_flag) {
+      atomicAdd(ga.err, 1ull);
+      for (int s = 0; s < kPStages; s++)
+        if (last_phase[s] >= 0) mbar_wait(&full[s], (uint32_t)(last_phase[s] & 1), lim);
+    }
+    mbar_wait(&done, 0, lim);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u));
 }
 
 }  // namespace tn93

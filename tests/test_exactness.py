@@ -79,18 +79,21 @@ def test_default_band_summary_reports_no_undecided(engine_cli):
 
 
 @pytest.mark.gpu
-def test_widened_band_server_and_batch_match_default(oracle_bin, tmp_path):
+@pytest.mark.parametrize("spread", [2.0 ** 30, 2.0 ** 34], ids=["spread30", "spread34"])
+def test_widened_band_server_and_batch_match_default(oracle_bin, tmp_path, spread):
     """The resident-reference server and the batched form finish their undecided pairs the same way: with a
-    widened band every response equals the oracle's -s run and every batched alignment its default-band run."""
+    widened band every response equals the oracle's -s run and every batched alignment its default-band run. At
+    the wider spread more pairs are undecided than the first lists hold (the server grows its list and runs the
+    batch again; the batched form runs those alignments again alone)."""
     from swifttn93_b200 import Engine, Fasta, HostAlignment, Options, ResidentReference, synth
 
     rng = np.random.default_rng(5)
     rnames, rcodes = synth.serve_reference(seed=9, n=800, L=1200)
     ref = synth.to_fasta(rnames, rcodes)
     (tmp_path / "ref.fa").write_bytes(ref)
-    opts = Options(threshold=0.015, mode="resolve", min_overlap=500)
+    opts = Options(threshold=0.03, mode="resolve", min_overlap=500)
     eng = Engine()
-    eng.set_log_band(0.5, 2.0 ** 30)
+    eng.set_log_band(0.5, spread)
     R = Fasta(ref)
     srv = ResidentReference(eng, R, opts, max_batch_sequences=256, max_batch_queries=8)
     qfa = []
@@ -99,16 +102,20 @@ def test_widened_band_server_and_batch_match_default(oracle_bin, tmp_path):
         qfa.append(synth.to_fasta(names, codes))
     out = srv.batch([Fasta(q, expect_len=R.L) for q in qfa])
     resolved = out[0][1].logs_resolved
+    links = 0
     for k, (body, summ) in enumerate(out):
         qp = tmp_path / f"q{k}.fa"
         qp.write_bytes(qfa[k])
-        rc, fo, so, _ = run_tn93(oracle_bin, ["-t", "0.015", "-a", "resolve", "-l", "500", "-s", str(tmp_path / "ref.fa")],
-                                 qp, tmp_path)
+        # tn93 -s QUERY.fa REF.fa: the reference is the positional file (rows), the query the second
+        rc, fo, so, _ = run_tn93(oracle_bin, ["-t", "0.03", "-a", "resolve", "-l", "500", "-s", str(qp)],
+                                 tmp_path / "ref.fa", tmp_path)
         assert rc == 0
         assert b"ID1,ID2,Distance\n" + body == fo, k
         js = summ.json(R.n, Fasta(qfa[k]).n, second_file=True)
         assert js == so, k
-    assert resolved > 0
+        links += summ.links
+    srv.close()
+    assert resolved > 0 and links > 0
     # batch: widened band against the default band (itself checked against the oracle in test_batch); small
     # alignments of the batched workload's shape
     ha, ops = [], []
