@@ -232,7 +232,8 @@ def serving_variant(rates=(20.0, 200.0), seconds=4.0, saturate=1200, ref_sample=
            "unit": "pairs/s", "hbm_budget_bytes": 8 << 30}
     sample_responses = None
     for w in worker_counts:
-        with Service(ref, opts, hbm_budget=8 << 30, workers=w) as svc:
+        # the budget is split over the workers: at 4 workers a batch holds up to 128 queries
+        with Service(ref, opts, hbm_budget=8 << 30, workers=w, max_batch_queries=256 if w <= 2 else 128) as svc:
             run_load(svc, qs[:50], 1e7, seed=1)  # warm-up: buffers reach their working sizes
             if w == worker_counts[0]:
                 out["workers"] = w

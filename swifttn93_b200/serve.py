@@ -88,9 +88,9 @@ class Service:
         # the reference's codes (3 copies), planes and worst-case events; per query sequence of capacity: its pairs'
         # distance and replay slots, codes (3 copies), planes and events
         resident = N * L * 3 + W * 5 * (N + 64) * 8 + N * L * 4 + len(ref_fasta)
-        # tensor-core counts: the one-hot image (4 bytes per sequence and column) and one 1,024-column chunk of
-        # 16-bit aggregates
-        resident += 4 * L * N + 14 * N * 1024
+        # tensor-core counts: the one-hot image (4 bytes per sequence and column) and the 16-byte records of one
+        # 128-column chunk of query columns
+        resident += 4 * L * N + 16 * N * 128
         fixed = max_batch_queries * N * SEGMENT_BYTES
         cap = (share - resident - fixed - TEXT_RESERVE) // (N * PAIR_BYTES + L * 11 + W * 5 * 8)
         if max_batch_sequences is not None:
