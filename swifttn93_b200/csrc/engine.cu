@@ -1100,75 +1100,121 @@ __device__ __forceinline__ void stats_rows(const RowArgs &a, long bx, int sg)
 __global__ void __launch_bounds__(256) stats_kernel(RowArgs a) { stats_rows(a, blockIdx.x, blockIdx.y); }
 
 
-// tn93's row sums with one lane per row: a warp takes 32 consecutive rows and walks their columns 32 at a time.
-// Each 32 x 32 tile is loaded row by row (coalesced) into shared memory and read back transposed, so that every
-// lane adds its own row's terms in column order, as tn93 does (swifttn93.cpp:2594-2602): the self-pair weights
-// first, then per column the distance times the copy weight (bins by file under -m). Columns before a row's first
-// pair and skipped pairs add +0.0 to the distance sums, which leaves a non-negative sum unchanged, and nothing to
-// the weights. The weights are added as doubles in the same order, which is tn93's own arithmetic (and exact while
-// the total stays below 2^53). 4 warps per block.
-constexpr int kSumWarps = 4;
-__device__ __forceinline__ void sum_lane_rows(const RowArgs &a, long bx)
+// one warp per row: tn93's row sums in column order (swifttn93.cpp:2594-2602); lane 0 adds each chunk's terms in
+// order. The self-pair weights come first, as tn93 adds them when the row starts (swifttn93.cpp:2405-2415).
+__device__ __forceinline__ void sum_rows(const RowArgs &a, long bx)
 {
-  __shared__ double tile[kSumWarps][32][33];
-  __shared__ long wt[kSumWarps][32];
+  __shared__ double sterm[kWarps][32], sw[kWarps][32];
+  __shared__ unsigned char sbin[kWarps][32];
   const RunConsts &rc = a.rc;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const long i0 = a.r0 + (bx * kSumWarps + warp) * 32l;
-  if (i0 >= a.r1) return;  // warp-uniform; the kernel synchronises warps only
-  const long i = i0 + lane;
-  const bool row = i < a.r1;
-  const long nrow = min(32l, a.r1 - i0);
-  const long cnt_i = a.counts[row ? i : i0];
+  const long i = a.r0 + bx * kWarps + warp;
+  if (i >= a.r1) return;
+  const long cnt_i = a.counts[i];
   double s0 = 0., s1 = 0., s2 = 0., w0 = 0., w1 = 0., w2 = 0.;
-  if (row && !rc.cross && cnt_i > 1) {
-    const double svs = (double)((unsigned long long)(cnt_i * (cnt_i - 1l)) >> 1);
+  const long lb = rc.cross ? rc.n1 : i + 1, cend = rc.N, out_row = i - a.r0;
+  if (!rc.cross && cnt_i > 1) {
+    const unsigned long long svs = (unsigned long long)(cnt_i * (cnt_i - 1l)) >> 1;
     if (i < rc.n1)
-      w0 = svs;
+      w0 += (double)svs;
     else
-      w1 = svs;
+      w1 += (double)svs;
   }
-  const long first = rc.cross ? rc.n1 : i0 + 1;  // the warp's first column with a pair
-  const double *base = a.dist + (size_t)(i0 - a.r0) * a.ncols - a.colbase;
-  const double skip = __longlong_as_double((long long)kSkipBits);
-  for (long c0 = first; c0 < rc.N; c0 += 32) {
-    const long j = c0 + lane;
-#pragma unroll 4
-    for (int q = 0; q < 32; q++) {
-      double v = skip;
-      if (q < nrow) {
-        const long lbq = rc.cross ? rc.n1 : i0 + q + 1;
-        if (j >= lbq && j < rc.N) v = base[(size_t)q * a.ncols + j];
+  const double *drow = a.dist + (size_t)(i - a.r0) * a.ncols - a.colbase;
+  if (!rc.fst) {
+    // Single bin: every lane adds the chunk's 32 terms in column order (the same chain in every lane, so no lane
+    // waits for another); skipped pairs and columns past the end add +0.0, which leaves a non-negative sum
+    // unchanged. The weights are integers: their double sum is exact, in any order, while the total stays below
+    // 2^53, so they are added as integers (and re-added one by one in the rare case the total is larger).
+    unsigned long long wsum = 0;
+    for (long j0 = lb; j0 < cend; j0 += 32) {
+      const long j = j0 + lane;
+      double term = 0.;
+      if (j < cend) {
+        const double raw = drow[j];
+        if ((uint64_t)__double_as_longlong(raw) != kSkipBits) {
+          const double t = raw <= 0. ? 0. : raw;
+          const long w = cnt_i * a.counts[j];
+          term = __dmul_rn(t, (double)w);
+          wsum += (unsigned long long)w;
+        }
       }
-      tile[warp][q][lane] = v;
+#pragma unroll
+      for (int l = 0; l < 32; l++) s0 = __dadd_rn(s0, __shfl_sync(0xffffffffu, term, l));
     }
-    wt[warp][lane] = j < rc.N ? a.counts[j] : 0;
-    __syncwarp();
-    if (row) {
-      const int nc = (int)min(32l, rc.N - c0);
-      for (int c = 0; c < nc; c++) {
-        const double raw = tile[warp][lane][c];
-        if ((uint64_t)__double_as_longlong(raw) == kSkipBits) continue;
+    for (int o = 16; o; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+    const unsigned long long svs = (!rc.cross && cnt_i > 1) ? (unsigned long long)(cnt_i * (cnt_i - 1l)) >> 1 : 0;
+    if (wsum + svs < (1ull << 53)) {
+      w0 = (double)(wsum + svs);
+    } else {
+      w0 = (double)svs;
+      for (long j0 = lb; j0 < cend; j0 += 32) {
+        const long j = j0 + lane;
+        double wl = 0.;
+        if (j < cend && (uint64_t)__double_as_longlong(drow[j]) != kSkipBits) wl = (double)(cnt_i * a.counts[j]);
+#pragma unroll
+        for (int l = 0; l < 32; l++) w0 = __dadd_rn(w0, __shfl_sync(0xffffffffu, wl, l));
+      }
+    }
+    if (lane == 0) {
+      const long r = out_row;
+      a.row_sum[r * 3] = s0;
+      a.row_sum[r * 3 + 1] = 0.;
+      a.row_sum[r * 3 + 2] = 0.;
+      a.row_w[r * 3] = w0;
+      a.row_w[r * 3 + 1] = 0.;
+      a.row_w[r * 3 + 2] = 0.;
+    }
+    return;
+  }
+  for (long j0 = lb; j0 < cend; j0 += 32) {
+    const long j = j0 + lane;
+    bool inc = false;
+    double term = 0., wl = 0.;
+    int bin = 0;
+    if (j < cend) {
+      const double raw = drow[j];
+      if ((uint64_t)__double_as_longlong(raw) != kSkipBits) {
         const double t = raw <= 0. ? 0. : raw;
-        const double wl = (double)(cnt_i * wt[warp][c]);
-        const double term = __dmul_rn(t, wl);
-        const int bin = rc.fst ? (i < rc.n1 ? (c0 + c >= rc.n1 ? 2 : 0) : 1) : 0;
-        if (bin == 0) {
-          s0 = __dadd_rn(s0, term);
-          w0 = __dadd_rn(w0, wl);
-        } else if (bin == 1) {
-          s1 = __dadd_rn(s1, term);
-          w1 = __dadd_rn(w1, wl);
-        } else {
-          s2 = __dadd_rn(s2, term);
-          w2 = __dadd_rn(w2, wl);
+        const long w = cnt_i * a.counts[j];
+        if (rc.fst) bin = i < rc.n1 ? (j >= rc.n1 ? 2 : 0) : 1;
+        inc = true;
+        term = __dmul_rn(t, (double)w);
+        wl = (double)w;
+      }
+    }
+    sterm[warp][lane] = term;
+    sw[warp][lane] = wl;
+    sbin[warp][lane] = inc ? (unsigned char)bin : (unsigned char)255;
+    __syncwarp();
+    if (lane == 0) {
+      const int n = (int)min(32l, cend - j0);
+      if (!rc.fst) {
+        for (int l = 0; l < n; l++)
+          if (sbin[warp][l] == 0) {
+            s0 = __dadd_rn(s0, sterm[warp][l]);
+            w0 = __dadd_rn(w0, sw[warp][l]);
+          }
+      } else {
+        for (int l = 0; l < n; l++) {
+          const int bl = sbin[warp][l];
+          if (bl == 0) {
+            s0 = __dadd_rn(s0, sterm[warp][l]);
+            w0 = __dadd_rn(w0, sw[warp][l]);
+          } else if (bl == 1) {
+            s1 = __dadd_rn(s1, sterm[warp][l]);
+            w1 = __dadd_rn(w1, sw[warp][l]);
+          } else if (bl == 2) {
+            s2 = __dadd_rn(s2, sterm[warp][l]);
+            w2 = __dadd_rn(w2, sw[warp][l]);
+          }
         }
       }
     }
     __syncwarp();
   }
-  if (row) {
-    const long r = i - a.r0;
+  if (lane == 0) {
+    const long r = out_row;
     a.row_sum[r * 3] = s0;
     a.row_sum[r * 3 + 1] = s1;
     a.row_sum[r * 3 + 2] = s2;
@@ -1178,7 +1224,7 @@ __device__ __forceinline__ void sum_lane_rows(const RowArgs &a, long bx)
   }
 }
 
-__global__ void __launch_bounds__(128) sum_lane_kernel(RowArgs a) { sum_lane_rows(a, blockIdx.x); }
+__global__ void __launch_bounds__(256) sum_kernel(RowArgs a) { sum_rows(a, blockIdx.x); }
 
 __device__ __forceinline__ char *put_bytes(char *o, const char *s, int n)
 {
@@ -1343,11 +1389,10 @@ __global__ void __launch_bounds__(256) stats_batch_kernel(const RowArgs *descs, 
   stats_rows(a, B.y, blockIdx.y);
 }
 
-// block b: 128 rows (4 warps of 32) of alignment blocks[b].x, from row 128 blocks[b].y
-__global__ void __launch_bounds__(128) sum_batch_kernel(const RowArgs *descs, const int2 *blocks)
+__global__ void __launch_bounds__(256) sum_batch_kernel(const RowArgs *descs, const int2 *blocks)
 {
   const int2 B = blocks[blockIdx.x];
-  sum_lane_rows(descs[B.x], B.y);
+  sum_rows(descs[B.x], B.y);
 }
 
 __global__ void __launch_bounds__(256) write_batch_kernel(const RowArgs *descs, const int2 *blocks)
@@ -1583,7 +1628,7 @@ cudaError_t launch_count_grid(const TcArgs &T, long gx, long gy, int sms, cudaSt
     count_tc_kernel<<<dim3((unsigned)gx, (unsigned)gy), 128, kTcSmem, st>>>(T);
   } else {
     const long nt = gx * gy;
-    count_tc_persist_kernel<<<(unsigned)std::min<long>(nt, sms), 192, kPSmem, st>>>(T, nullptr, nullptr, 0);
+    count_tc_persist_kernel<<<(unsigned)std::min<long>(nt, sms), kPThreads, kPSmem, st>>>(T, nullptr, nullptr, 0);
   }
   return cudaGetLastError();
 }
@@ -1598,7 +1643,7 @@ cudaError_t launch_count_list(const TcArgs &G, const TcArgs *descs, const int4 *
   if (tc_tile_kernel())
     count_tc_batch_kernel<<<(unsigned)ntiles, 128, kTcSmem, st>>>(descs, tiles);
   else
-    count_tc_persist_kernel<<<(unsigned)std::min(ntiles, sms), 192, kPSmem, st>>>(G, descs, tiles, ntiles);
+    count_tc_persist_kernel<<<(unsigned)std::min(ntiles, sms), kPThreads, kPSmem, st>>>(G, descs, tiles, ntiles);
   return cudaGetLastError();
 }
 
@@ -2421,7 +2466,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     stats_kernel<<<dim3((unsigned)((nr + kWarps - 1) / kWarps), (unsigned)maxseg), 256, 0, st>>>(RA);
     CU(cudaGetLastError());
     ctx->launches++;
-    sum_lane_kernel<<<(unsigned)((nr + 32 * kSumWarps - 1) / (32 * kSumWarps)), 32 * kSumWarps, 0, st>>>(RA);
+    sum_kernel<<<(unsigned)((nr + kWarps - 1) / kWarps), 256, 0, st>>>(RA);
     CU(cudaGetLastError());
     ctx->launches++;
     unsigned long long *dtot = (unsigned long long *)ctx->total.p + par;
@@ -4557,7 +4602,7 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
   TRY(ensure(ctx, bb[BB_ROWDESC], K * sizeof(RowArgs)));
   CU(cudaMemsetAsync(bb[BB_HIST].p, 0, (size_t)K * 3 * kHistBins * sizeof(unsigned long long), st));
   std::vector<RowArgs> RA(K);
-  std::vector<int2> blocks, sblocks;  // row blocks of 8 rows (statistics, text) and of 128 rows (sums)
+  std::vector<int2> blocks;
   long segmax = 1;
   std::vector<long> first_idx(K);
   for (int k = 0; k < K; k++) {
@@ -4589,15 +4634,11 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
     a.err = (unsigned long long *)bb[BB_COUNTERS].p + 4 * k + 3;
     segmax = std::max(segmax, maxseg[k]);
     for (long bx = 0; bx < (alns[k].n + kWarps - 1) / kWarps; bx++) blocks.push_back(make_int2(k, (int)bx));
-    for (long bx = 0; bx < (alns[k].n + 32 * kSumWarps - 1) / (32 * kSumWarps); bx++)
-      sblocks.push_back(make_int2(k, (int)bx));
     first_idx[k] = (long)seg_base[k];
   }
-  TRY(ensure(ctx, bb[BB_BLOCKS], (blocks.size() + sblocks.size()) * sizeof(int2)));
+  TRY(ensure(ctx, bb[BB_BLOCKS], blocks.size() * sizeof(int2)));
   CU(cudaMemcpyAsync(bb[BB_ROWDESC].p, RA.data(), K * sizeof(RowArgs), cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync(bb[BB_BLOCKS].p, blocks.data(), blocks.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
-  CU(cudaMemcpyAsync((int2 *)bb[BB_BLOCKS].p + blocks.size(), sblocks.data(), sblocks.size() * sizeof(int2),
-                     cudaMemcpyHostToDevice, st));
   CU(cudaMemcpyAsync(bb[BB_FIRSTIDX].p, first_idx.data(), K * sizeof(long), cudaMemcpyHostToDevice, st));
   const RowArgs *rd = (const RowArgs *)bb[BB_ROWDESC].p;
   const int2 *bp = (const int2 *)bb[BB_BLOCKS].p;
@@ -4609,7 +4650,7 @@ extern "C" int tn93g_batch_run(tn93g_ctx *ctx, int K, const tn93g_alignment *aln
     CU(cudaMemsetAsync(bb[BB_HIST].p, 0, (size_t)K * 3 * kHistBins * sizeof(unsigned long long), st));
     stats_batch_kernel<<<dim3((unsigned)blocks.size(), (unsigned)segmax), 256, 0, st>>>(rd, bp);
     CU(cudaGetLastError());
-    sum_batch_kernel<<<(unsigned)sblocks.size(), 32 * kSumWarps, 0, st>>>(rd, bp + blocks.size());
+    sum_batch_kernel<<<(unsigned)blocks.size(), 256, 0, st>>>(rd, bp);
     CU(cudaGetLastError());
     CU(launch_scan((const unsigned long long *)bb[BB_SBYTES].p, (unsigned long long *)bb[BB_SOFF].p, (long)NS,
                    (unsigned long long *)bb[BB_TOTAL].p, (unsigned long long *)bb[BB_SCANTMP].p, st));

@@ -181,12 +181,14 @@ __global__ void onehot_kernel(const uint8_t *__restrict__ cc, long N, long Lc, l
 }
 
 // Reads the accumulator of tile (i0, j0) (tensor memory from tacc, lane quarter q = 32 rows: sequences
-// i0 + 8q .. i0 + 8q + 7, four class rows each) and stores each pair's record. All 32 lanes of the warp call it.
-__device__ __forceinline__ void tc_tile_epilogue(const TcArgs &a, long i0, long j0, uint32_t tacc, int q, int lane)
+// i0 + 8q .. i0 + 8q + 7, four class rows each; the 16-column chunks c16_0 .. c16_0 + c16_n - 1, 4 column sequences
+// each) and stores each pair's record. All 32 lanes of the warp call it.
+__device__ __forceinline__ void tc_tile_epilogue(const TcArgs &a, long i0, long j0, uint32_t tacc, int q, int lane,
+                                                 int c16_0 = 0, int c16_n = 256 / 16)
 {
   const int il = q * 8 + lane / 4, cls = lane & 3;
   const long i = i0 + il;
-  for (int c16 = 0; c16 < 256 / 16; c16++) {
+  for (int c16 = c16_0; c16 < c16_0 + c16_n; c16++) {
     uint32_t v[16];
     tmem_ld16(tacc + ((uint32_t)(q * 32) << 16) + (uint32_t)(c16 * 16), v);
     // v[4 * jj + b] = N_{cls, b}(i, j = 4 * c16 + jj)
@@ -366,8 +368,9 @@ __global__ void __launch_bounds__(128) count_tc_batch_kernel(const TcArgs *descs
 //                      transaction counts);
 //   warp 1 (one lane)  MMA issuer: 4 tcgen05.mma per stage into one of two accumulators (2 x 256 tensor-memory
 //                      columns), each stage committed back to the producer, each finished tile to the epilogue;
-//   warps 2-5          epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. +31 of a finished accumulator,
-//                      stores the records and hands the accumulator back to the MMA issuer.
+//   warps 2-9          epilogue: warp w reads tensor-memory lanes 32 (w % 4) .. +31 of a finished accumulator,
+//                      columns 128 ((w - 2) / 4) .. +127, stores the records and hands the accumulator back to the
+//                      MMA issuer (eight warps, so that the epilogue keeps up with the MMAs).
 // So tile t's epilogue overlaps tile t+1's copies and MMAs. Every wait is bounded (TcArgs::wait_ns); a wait that
 // gives up stops every role, and the CTA lets its copies land and its MMAs complete (bounded) before it frees its
 // tensor memory. Tiles come from a grid over one band (tiles == nullptr: the count_tc_kernel grid of `ga`) or
@@ -388,7 +391,10 @@ __device__ __forceinline__ bool tc_tile_valid(const TcArgs &a, long i0, long j0)
   return true;
 }
 
-__global__ void __launch_bounds__(192, 1)
+constexpr int kPEpiWarps = 8;
+constexpr int kPThreads = 32 * (2 + kPEpiWarps);
+
+__global__ void __launch_bounds__(kPThreads, 1)
     count_tc_persist_kernel(TcArgs ga, const TcArgs *descs, const int4 *tiles, int ntiles)
 {
   extern __shared__ __align__(1024) unsigned char tsm[];
@@ -422,7 +428,7 @@ __global__ void __launch_bounds__(192, 1)
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(&accf[b], 1);
-      mbar_init(&acce[b], 4);
+      mbar_init(&acce[b], kPEpiWarps);
     }
     mbar_init(&done, 1);
     abort_flag = 0;
@@ -503,7 +509,8 @@ __global__ void __launch_bounds__(192, 1)
     }
     umma_commit(&done);  // arrives when every MMA issued above has completed
   } else if (warp >= 2) {
-    const int q = warp & 3;  // tensor-memory lane quarter this warp may read
+    const int q = warp & 3;                // tensor-memory lane quarter this warp may read
+    const int half = (warp - 2) >> 2;      // which half of the accumulator's columns it reads
     uint32_t u = 0;
     for (long t = blockIdx.x; t < ntot; t += gridDim.x) {
       const int stop = __shfl_sync(0xffffffffu, lane == 0 ? *(volatile int *)&abort_flag : 0, 0);
@@ -518,7 +525,7 @@ __global__ void __launch_bounds__(192, 1)
         break;
       }
       tc_fence_after();
-      tc_tile_epilogue(*A, i0, j0, tmem + b * 256, q, lane);
+      tc_tile_epilogue(*A, i0, j0, tmem + b * 256, q, lane, half * 8, 8);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&acce[b]);
