@@ -245,6 +245,13 @@ int tn93g_set_exact_sums(tn93g_ctx *ctx, int on);
 int tn93g_set_wait_limit(tn93g_ctx *ctx, double seconds);
 int tn93g_inject_fault(tn93g_ctx *ctx, int fault);
 
+/* Self-test of the device formula's division scheme (tests). n random pairs of counts go through the formula up
+ * to its logarithms on the device and on the host (IEEE division), and n random quotients x / b through the
+ * device's reciprocal-sharing division against its own correctly rounded division. mismatches[0] receives the
+ * formula inputs whose results differ in any bit, mismatches[1] the quotients. Replaces: nothing in the
+ * reference. */
+int tn93g_selftest_division(tn93g_ctx *ctx, long n, unsigned long long seed, long mismatches[2]);
+
 /* Allocation-free pair distances. This entry point has no counterpart in the reference; it exists for callers
  * that cannot allocate device memory: plugin hosts whose own allocator owns the whole device (a second
  * allocator would fail or fragment it), and latency-critical loops that must not enter the driver's allocator.

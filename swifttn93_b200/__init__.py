@@ -33,7 +33,7 @@ EXPORTS = ("tn93g_create", "tn93g_destroy", "tn93g_strerror", "tn93g_last_cuda_e
            "tn93g_alignment_free", "tn93g_server_create", "tn93g_server_batch", "tn93g_server_destroy",
            "tn93g_summary_json", "tn93g_run_rows", "tn93g_batch_run", "tn93g_set_count_path",
            "tn93g_summary_certified", "tn93g_set_log_band", "tn93g_set_exact_sums", "tn93g_set_wait_limit",
-           "tn93g_inject_fault")
+           "tn93g_inject_fault", "tn93g_selftest_division")
 
 # error codes of include/tn93g.h used by the binding
 EUNDECIDED = -10
@@ -117,6 +117,7 @@ def load_library(path: Path | str = LIB_PATH):
     lib.tn93g_set_exact_sums.argtypes = [C.c_void_p, C.c_int]
     lib.tn93g_set_wait_limit.argtypes = [C.c_void_p, C.c_double]
     lib.tn93g_inject_fault.argtypes = [C.c_void_p, C.c_int]
+    lib.tn93g_selftest_division.argtypes = [C.c_void_p, C.c_long, C.c_ulonglong, C.POINTER(C.c_long)]
     _lib = lib
     return lib
 
@@ -401,6 +402,13 @@ class Engine:
     def set_wait_limit(self, seconds: float):
         """Limit of each bounded device wait (tn93g_set_wait_limit)."""
         self._check(self.lib.tn93g_set_wait_limit(self.ctx, float(seconds)))
+
+    def selftest_division(self, n: int, seed: int) -> tuple:
+        """(formula inputs, quotients) whose device results differ from the host's IEEE division or the device's own
+        correctly rounded division (tn93g_selftest_division)."""
+        m = (C.c_long * 2)()
+        self._check(self.lib.tn93g_selftest_division(self.ctx, int(n), int(seed), m))
+        return m[0], m[1]
 
     def inject_fault(self, fault: int):
         """A TN93G_FAULT_* for the next run only (tn93g_inject_fault)."""

@@ -76,7 +76,7 @@ def build_cli(force=False) -> Path:
         return CLI
     CLI.parent.mkdir(parents=True, exist_ok=True)
     tmp = CLI.with_name("tn93g.tmp")
-    _run([HOSTCXX, "-O2", "-std=c++17", f"-I{REPO / 'include'}", str(CSRC / "cli.cpp"), "-o", str(tmp),
+    _run([HOSTCXX, "-O2", "-std=c++17", "-pthread", f"-I{REPO / 'include'}", str(CSRC / "cli.cpp"), "-o", str(tmp),
           f"-L{lib.parent}", "-ltn93g", "-Wl,-rpath,$ORIGIN/../lib"])
     tmp.replace(CLI)
     return CLI

@@ -12,9 +12,11 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <iomanip>
 #include <iostream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "tn93g.h"
@@ -267,16 +269,31 @@ bool read_fasta(FILE *F, Alignment &A, long &first_len, char sep)
   return true;
 }
 
+double now_s()
+{
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// the distance file's sink: the text of each band, in order, with the time spent writing it
+struct OutFile {
+  FILE *f;
+  double seconds = 0;
+};
+
 int write_sink(void *user, const char *bytes, size_t n)
 {
-  FILE *f = (FILE *)user;
-  return fwrite(bytes, 1, n, f) == n ? 0 : 1;
+  OutFile *o = (OutFile *)user;
+  const double t0 = now_s();
+  const bool ok = fwrite(bytes, 1, n, o->f) == n;
+  o->seconds += now_s() - t0;
+  return ok ? 0 : 1;
 }
 
 }  // namespace
 
 int main(int argc, char **argv)
 {
+  const double t_start = now_s();
   Options o = parse(argc, argv);
   if (o.bootstrap || o.bootstrap2 || o.include_prob < 1.) {
     std::cerr << "swifttn93: -b, -r and -u (random resampling) are not supported" << std::endl;
@@ -291,6 +308,23 @@ int main(int argc, char **argv)
     const char *f = strchr(kValid, toupper(ch));
     if (f && toupper(ch) && f - kValid > 3) subset[f - kValid] = 1;
   }
+  // the device context is set up on a second thread while the input is parsed
+  tn93g_ctx *ctx = nullptr;
+  int rc = TN93G_OK;
+  double t_ctx = 0;
+  std::thread init([&] {
+    const double t0 = now_s();
+    rc = tn93g_create(&ctx, 0, 0);
+    t_ctx = now_s() - t0;
+  });
+  struct Joiner {
+    std::thread &t;
+    ~Joiner()
+    {
+      if (t.joinable()) t.join();
+    }
+  } joiner{init};
+  const double t_read0 = now_s();
   Alignment A;
   long L = 0;
   if (!read_fasta(o.in1, A, L, o.counts_sep)) return 1;
@@ -300,6 +334,7 @@ int main(int argc, char **argv)
     if (!read_fasta(o.in2, A, L, o.counts_sep)) return 1;
     n2 = (unsigned long)A.N - n1;
   }
+  const double t_read = now_s() - t_read0;
   const bool fst = o.in2 && o.fst;
   const bool report_self = !o.in2 && o.report_self && !o.count;
   const unsigned long N = (unsigned long)A.N;
@@ -321,8 +356,9 @@ int main(int argc, char **argv)
     else
       fprintf(o.out, "Seq1%cSeq2%cDistance\n", o.delimiter, o.delimiter);
   }
-  tn93g_ctx *ctx = nullptr;
-  int rc = tn93g_create(&ctx, 0, 0);
+  const double t_wait0 = now_s();
+  init.join();
+  const double t_wait = now_s() - t_wait0;
   if (rc != TN93G_OK) {
     std::cerr << "tn93g: " << tn93g_strerror(rc) << std::endl;
     return 2;
@@ -349,20 +385,30 @@ int main(int argc, char **argv)
   op.do_fst = fst;
   memcpy(op.subset, subset, sizeof subset);
   tn93g_summary S;
-  rc = tn93g_run(ctx, set, (long)n1, &op, write_sink, o.out, &S);
+  OutFile of{o.out};
+  const double t_run0 = now_s();
+  rc = tn93g_run(ctx, set, (long)n1, &op, write_sink, &of, &S);
+  const double t_run = now_s() - t_run0;
   if (rc != TN93G_OK) {
     // a run that could not make every printed byte exact fails loudly (exit 3), like any engine error (exit 2)
     std::cerr << "tn93g: " << tn93g_strerror(rc) << " " << tn93g_last_cuda_error(ctx) << std::endl;
     return rc == TN93G_EUNDECIDED ? 3 : 2;
   }
-  if (getenv("TN93G_STATS"))
+  const double t_free0 = now_s();
+  tn93g_free_set(ctx, set);
+  tn93g_destroy(ctx);
+  fflush(o.out);
+  const double t_free = now_s() - t_free0;
+  if (getenv("TN93G_STATS")) {
     fprintf(stderr,
             "tn93g: replayed %ld, ambiguous-log pairs %ld, finished with the C library's log %ld, undecided %ld, "
             "exact-sums pass %d\n",
             S.pairs_replayed, S.logs_ambiguous, S.logs_resolved, S.undecided, S.sums_repass);
-  tn93g_free_set(ctx, set);
-  tn93g_destroy(ctx);
-  fflush(o.out);
+    fprintf(stderr,
+            "tn93g: seconds: read %.3f, context %.3f (waited %.3f), run %.3f (writing %.3f), release %.3f, "
+            "to here %.3f\n",
+            t_read, t_ctx, t_wait, t_run, of.seconds, t_free, now_s() - t_start);
+  }
   if (!o.quiet)
     std::cerr << std::endl << "Progress:" << std::setw(8) << 100. << "% (" << std::setw(8) << S.links
               << " links found, " << std::setw(12) << std::setprecision(3) << (double)pairwise << " evals)";

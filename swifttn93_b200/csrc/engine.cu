@@ -22,6 +22,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <chrono>
 #include <atomic>
 #include <mutex>
 #include <string>
@@ -182,6 +183,18 @@ __device__ __forceinline__ int same_g_fast(double lo, double hi)
   return -1;
 }
 
+// Do lo and hi print the same text? The certificate's exact test when the fast one cannot decide; out of line, so
+// that the big-number scratch of the decimal conversion lives in its own stack frame, not in its callers'.
+__device__ __noinline__ bool same_g_text(double lo, double hi)
+{
+  char x[24], y[24];
+  const int nx = fmt_g(lo, x), ny = fmt_g(hi, y);
+  if (nx != ny) return false;
+  for (int k = 0; k < nx; k++)
+    if (x[k] != y[k]) return false;
+  return true;
+}
+
 // decision-stability certificate: do the histogram bin, the link decision and the printed text agree for
 // every distance the C library's log may lead to?
 __device__ bool certified(const Dist &D, const RunConsts &rc)
@@ -195,11 +208,7 @@ __device__ bool certified(const Dist &D, const RunConsts &rc)
   if (llo && rc.emit && tlo != thi) {
     const int f = same_g_fast(tlo, thi);
     if (f >= 0) return f == 1;
-    char x[24], y[24];
-    const int nx = fmt_g(tlo, x), ny = fmt_g(thi, y);
-    if (nx != ny) return false;
-    for (int k = 0; k < nx; k++)
-      if (x[k] != y[k]) return false;
+    return same_g_text(tlo, thi);
   }
   return true;
 }
@@ -267,9 +276,9 @@ __device__ __forceinline__ int fst_bin(const RunConsts &rc, long i, long j)
 // logarithms). A pair whose printed bytes or decisions depend on the C library's rounding (or, in resolve-all
 // mode, any pair with an ambiguous logarithm) is appended to the undecided list, to be finished with the C
 // library's own logarithms; every pair with an ambiguous logarithm widens its summary unit's bounds.
-__device__ double finish_exact(const LogTable &T, const RunConsts &rc, const ExactSink &ex, const double nf[4],
-                               double diag, double ag, double ct, long i, long j, long colbase, int &namb, int &nund,
-                               AmbLane &al)
+__device__ __forceinline__ double finish_exact(const LogTable &T, const RunConsts &rc, const ExactSink &ex,
+                                               const double nf[4], double diag, double ag, double ct, long i, long j,
+                                               long colbase, int &namb, int &nund, AmbLane &al)
 {
   const Dist D = tn93_distance(T, nf, diag, ag, ct, rc.log_band, rc.log_spread);
   if (D.amb) {
@@ -354,12 +363,30 @@ struct Counts {
   int nWc, nWh, nWl, nWt, nWW, nGG;
 };
 
-// the per-pair epilogue: exact x16 aggregates, tn93's -l / -g / order decisions, formula, certificate
-template <bool WPLANE>
+// The final aggregates of a pair for formula_kernel, written over its tensor-core record at: ag[0..6] and a state
+// lane (0: the formula kernel finishes the pair; 1: finished here, skipped or queued for the site-order replay)
+__device__ __forceinline__ void store_final(const PairArgs &a, size_t at, const int ag[7], bool formula)
+{
+  const uint32_t st = formula ? 0u : 1u;
+  if (a.tc16) {
+    reinterpret_cast<uint4 *>(a.tcagg)[at] =
+        make_uint4((uint32_t)ag[0] | (uint32_t)ag[1] << 16, (uint32_t)ag[2] | (uint32_t)ag[3] << 16,
+                   (uint32_t)ag[4] | (uint32_t)ag[5] << 16, (uint32_t)ag[6] | st << 16);
+  } else {
+    uint4 *d = reinterpret_cast<uint4 *>(a.tcagg) + 2 * at;
+    d[0] = make_uint4((uint32_t)ag[0], (uint32_t)ag[1], (uint32_t)ag[2], (uint32_t)ag[3]);
+    d[1] = make_uint4((uint32_t)ag[4], (uint32_t)ag[5], (uint32_t)ag[6], st);
+  }
+}
+
+// the per-pair epilogue: exact x16 aggregates, tn93's -l / -g / order decisions, formula, certificate (SPLIT: the
+// aggregates go back into the pair's tensor-core record at, and formula_kernel runs the formula)
+template <bool WPLANE, bool SPLIT>
 // cl: the clean-site aggregates of the pair (jointly clean sites, matches, A<->G and C<->T transitions, A, C and G
 // base counts over both sequences), from the popcount loop or the tensor-core count kernel; c: N-plane counts
 __device__ __forceinline__ void pair_epilogue(const PairArgs &a, const AggEntry *EW, const Counts &c, const int cl[7],
-                                              const int acc[9], long i, long j, int &namb, int &nund, AmbLane &al)
+                                              const int acc[9], long i, long j, size_t at, int &namb, int &nund,
+                                              AmbLane &al)
 {
   const RunConsts &rc = a.rc;
   const int base[7] = {16 * (cl[0] + (int)rc.constT), 16 * (cl[1] + (int)rc.constT), 16 * cl[2], 16 * cl[3],
@@ -384,7 +411,7 @@ __device__ __forceinline__ void pair_epilogue(const PairArgs &a, const AggEntry 
   if (WPLANE) amb += wb[0] * EW[0].v[7] + wb[1] * EW[1].v[7] + wb[2] * EW[2].v[7] + wb[3] * EW[3].v[7] + nww * EW[4].v[7];
   double *slot = a.dist + (size_t)(i - a.r0) * a.ncols + (j - a.colbase);
   unsigned long long qentry = 0;
-  bool to_replay = false;
+  bool to_replay = false, formula = false;
   if (acc[8] & 1) {
     to_replay = true;  // order-dependent float sums in the main mode
   } else {
@@ -395,6 +422,8 @@ __device__ __forceinline__ void pair_epilogue(const PairArgs &a, const AggEntry 
       // tn93 recomputes the pair with -a average (refkernel.cpp:742-750): the site-order path does that exactly
       to_replay = true;
       qentry = 1ull << 63;
+    } else if (SPLIT) {
+      formula = true;
     } else {
       const double nf[4] = {(double)ag[4] / 16.0, (double)ag[5] / 16.0, (double)ag[6] / 16.0,
                             (double)(2 * ag[0] - ag[4] - ag[5] - ag[6]) / 16.0};
@@ -402,6 +431,7 @@ __device__ __forceinline__ void pair_epilogue(const PairArgs &a, const AggEntry 
                            j, a.colbase, namb, nund, al);
     }
   }
+  if (SPLIT) store_final(a, at, ag, formula);
   if (to_replay) {
     const unsigned idx = atomicAdd(a.replay_n, 1u);
     if (idx < a.replay_cap) a.replay_q[idx] = qentry | ((unsigned long long)i << 31) | (unsigned long long)j;
@@ -425,7 +455,7 @@ __device__ __forceinline__ void add_packed(PackedAcc &p, const uint32_t (*tab)[4
 
 // One tile of pairs: rows [i0, i0 + 8 * rpw) (rpw = rows per warp, 1..4) x columns [j0, j0 + 32). The block's
 // tables must be in smem (load_pair_tables). All threads of the block call it with the same arguments.
-template <bool WPLANE, bool GAPMM>
+template <bool WPLANE, bool GAPMM, bool SPLIT>
 __device__ __forceinline__ void pair_tile(const PairArgs &a, const unsigned char *smem, int *colacc, long i0, long j0,
                                           int rpw)
 {
@@ -555,12 +585,14 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const unsigned char
       }
     }
     int cl[7];
+    size_t at = 0;
     if (tc) {
-      // the pair's record from the tensor-core kernel (8 lanes, 7 used)
+      // the pair's record from the tensor-core kernel (8 lanes, 7 used); plain loads when SPLIT writes it back
       const long tn = a.tcncols ? a.tcncols : a.ncols, tb = a.tcncols ? a.tccolbase : a.colbase;
-      const size_t at = (size_t)(i - a.r0) * tn + (jj - tb);
+      at = (size_t)(i - a.r0) * tn + (jj - tb);
       if (a.tc16) {
-        const uint4 g = valid ? __ldg(reinterpret_cast<const uint4 *>(a.tcagg) + at) : make_uint4(0, 0, 0, 0);
+        const uint4 *gp = reinterpret_cast<const uint4 *>(a.tcagg) + at;
+        const uint4 g = valid ? (SPLIT ? *gp : __ldg(gp)) : make_uint4(0, 0, 0, 0);
         cl[0] = (int)(g.x & 0xFFFFu);
         cl[1] = (int)(g.x >> 16);
         cl[2] = (int)(g.y & 0xFFFFu);
@@ -570,7 +602,8 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const unsigned char
         cl[6] = (int)(g.w & 0xFFFFu);
       } else {
         const uint4 *g = reinterpret_cast<const uint4 *>(a.tcagg) + 2 * at;
-        const uint4 g0 = valid ? __ldg(g) : make_uint4(0, 0, 0, 0), g1 = valid ? __ldg(g + 1) : make_uint4(0, 0, 0, 0);
+        const uint4 g0 = valid ? (SPLIT ? g[0] : __ldg(g)) : make_uint4(0, 0, 0, 0);
+        const uint4 g1 = valid ? (SPLIT ? g[1] : __ldg(g + 1)) : make_uint4(0, 0, 0, 0);
         cl[0] = (int)g0.x;
         cl[1] = (int)g0.y;
         cl[2] = (int)g0.z;
@@ -589,13 +622,15 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const unsigned char
       cl[5] = nfC;
       cl[6] = nfG;
     }
-    if (valid) pair_epilogue<WPLANE>(a, EW, c, cl, acc, i, j, namb, nund, al);
+    if (valid) pair_epilogue<WPLANE, SPLIT>(a, EW, c, cl, acc, i, j, at, namb, nund, al);
   }
-  count_flags(a.counters, namb, nund);
-  if (a.ex.amb) amb_warp_flush(a.ex.amb, al);
+  if (!SPLIT) {
+    count_flags(a.counters, namb, nund);
+    if (a.ex.amb) amb_warp_flush(a.ex.amb, al);
+  }
 }
 
-template <bool WPLANE, bool GAPMM, int MINB>
+template <bool WPLANE, bool GAPMM, int MINB, bool SPLIT>
 __global__ void __launch_bounds__(256, MINB) pair_kernel(PairArgs a)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -605,7 +640,59 @@ __global__ void __launch_bounds__(256, MINB) pair_kernel(PairArgs a)
   if (i0 >= a.r1 || j0 >= a.rc.N || (!a.rc.cross && j0 + kTile - 1 <= i0)) return;
   load_pair_tables(a.tab, smem_raw, a.rc.packed);
   __syncthreads();
-  pair_tile<WPLANE, GAPMM>(a, smem_raw, colacc, i0, j0, kRowsPerWarp);
+  pair_tile<WPLANE, GAPMM, SPLIT>(a, smem_raw, colacc, i0, j0, kRowsPerWarp);
+}
+
+// The formula for the pairs of one split pair-kernel launch (rows [r0, r1), columns [cstart, cstart + ncol)): one
+// thread per pair slot, lanes along a row's columns, reading the final aggregates the pair kernel left in the
+// pair's tensor-core record (state 0) and writing the distance. No shared memory; the registers of the formula
+// alone decide the occupancy (MINB resident blocks per SM).
+template <bool REC16, int MINB>
+__global__ void __launch_bounds__(256, MINB) formula_kernel(PairArgs a, long ncol)
+{
+  const RunConsts &rc = a.rc;
+  const long tn = a.tcncols ? a.tcncols : a.ncols, tb = a.tcncols ? a.tccolbase : a.colbase;
+  const long j = a.cstart + blockIdx.x * 256l + threadIdx.x;
+  int namb = 0, nund = 0;
+  AmbLane al;
+  al.unit = -1;
+  for (long i = a.r0 + blockIdx.y; i < a.r1; i += gridDim.y) {
+    const long lb = rc.cross ? rc.n1 : i + 1;
+    if (j < lb || j >= rc.N || j >= a.cstart + ncol) continue;
+    const size_t at = (size_t)(i - a.r0) * tn + (j - tb);
+    int ag[7];
+    uint32_t st;
+    if (REC16) {
+      const uint4 g = reinterpret_cast<const uint4 *>(a.tcagg)[at];
+      ag[0] = (int)(g.x & 0xFFFFu);
+      ag[1] = (int)(g.x >> 16);
+      ag[2] = (int)(g.y & 0xFFFFu);
+      ag[3] = (int)(g.y >> 16);
+      ag[4] = (int)(g.z & 0xFFFFu);
+      ag[5] = (int)(g.z >> 16);
+      ag[6] = (int)(g.w & 0xFFFFu);
+      st = g.w >> 16;
+    } else {
+      const uint4 *g = reinterpret_cast<const uint4 *>(a.tcagg) + 2 * at;
+      const uint4 g0 = g[0], g1 = g[1];
+      ag[0] = (int)g0.x;
+      ag[1] = (int)g0.y;
+      ag[2] = (int)g0.z;
+      ag[3] = (int)g0.w;
+      ag[4] = (int)g1.x;
+      ag[5] = (int)g1.y;
+      ag[6] = (int)g1.z;
+      st = g1.w;
+    }
+    if (st) continue;
+    const double nf[4] = {(double)ag[4] / 16.0, (double)ag[5] / 16.0, (double)ag[6] / 16.0,
+                          (double)(2 * ag[0] - ag[4] - ag[5] - ag[6]) / 16.0};
+    a.dist[(size_t)(i - a.r0) * a.ncols + (j - a.colbase)] =
+        finish_exact(*a.logt, rc, a.ex, nf, (double)ag[1] / 16.0, (double)ag[2] / 16.0, (double)ag[3] / 16.0, i, j,
+                     a.colbase, namb, nund, al);
+  }
+  count_flags(a.counters, namb, nund);
+  if (a.ex.amb) amb_warp_flush(a.ex.amb, al);
 }
 
 static_assert(sizeof(PairArgs) % 4 == 0, "PairArgs is copied as 32-bit words");
@@ -643,7 +730,7 @@ __global__ void __launch_bounds__(256, MINB)
       cur = T.k;
     }
     __syncthreads();
-    pair_tile<WPLANE, GAPMM>(sd, smem_raw, colacc, T.i0, T.j0, T.rpw);
+    pair_tile<WPLANE, GAPMM, false>(sd, smem_raw, colacc, T.i0, T.j0, T.rpw);
     __syncthreads();
   }
 }
@@ -1554,45 +1641,84 @@ struct PerDevice {
 };
 
 // pair kernel launch (dynamic shared memory above the 48 KB default needs the opt-in attribute once per device).
-// Two register budgets are built: 2 blocks per SM (128 registers, no spills) and 3 (80 registers, some spills).
-template <int MINB>
+// Register budgets: 2 blocks per SM (128 registers, no spills) and 3 (80 registers, some spills) for the fused
+// kernel; 4 (64 registers) for the split kernel, which holds no formula state.
+template <int MINB, bool SPLIT>
 cudaError_t launch_pair_t(const PairArgs &A, dim3 g, cudaStream_t st)
 {
   static PerDevice attr;
   cudaError_t e = attr.once([] {
     cudaError_t r;
-    if ((r = cudaFuncSetAttribute(pair_kernel<false, false, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if ((r = cudaFuncSetAttribute(pair_kernel<false, false, MINB, SPLIT>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmem)) != cudaSuccess)
+      return r;
+    if ((r = cudaFuncSetAttribute(pair_kernel<true, false, MINB, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kPairSmem)) != cudaSuccess)
       return r;
-    if ((r = cudaFuncSetAttribute(pair_kernel<true, false, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kPairSmem)) != cudaSuccess)
-      return r;
-    return cudaFuncSetAttribute(pair_kernel<true, true, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(pair_kernel<true, true, MINB, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)kPairSmem);
   });
   if (e != cudaSuccess) return e;
   if (A.rc.wplane) {
     if (A.rc.gapmm)
-      pair_kernel<true, true, MINB><<<g, 256, kPairSmem, st>>>(A);
+      pair_kernel<true, true, MINB, SPLIT><<<g, 256, kPairSmem, st>>>(A);
     else
-      pair_kernel<true, false, MINB><<<g, 256, kPairSmem, st>>>(A);
+      pair_kernel<true, false, MINB, SPLIT><<<g, 256, kPairSmem, st>>>(A);
   } else
-    pair_kernel<false, false, MINB><<<g, 256, kPairSmem, st>>>(A);
+    pair_kernel<false, false, MINB, SPLIT><<<g, 256, kPairSmem, st>>>(A);
   return cudaGetLastError();
 }
 
 // Resident blocks per SM: 3 (80 registers a thread) when the clean-site counts come from the tensor cores, 2 (128)
 // with the popcount loop, which needs the registers (measured: 3 is 11% faster on the tensor-core path, and slower
 // with the popcount loop). TN93G_PAIR_BLOCKS=2|3 overrides.
+// Whether the tensor-core path splits the pair stage into the event kernel and formula_kernel: when the N plane is
+// in use (gapmm, or many N), whose popcount loop runs faster in the split kernel's 64 registers; otherwise one fused
+// kernel overlaps the formula with the event sums better (measured on the 6,700 x 1,500 HIV benchmark set: split
+// 5.57 ms vs fused 6.15 ms per gapmm pair stage, fused 3.46 ms vs split 3.73 ms under resolve). TN93G_PAIR_SPLIT=0|1
+// forces either; both give the same bytes.
+int pair_split(const RunConsts &rc)
+{
+  static const int v = [] {
+    const char *e = getenv("TN93G_PAIR_SPLIT");
+    return e ? (atoi(e) ? 1 : 0) : -1;
+  }();
+  return v >= 0 ? v : (rc.wplane ? 1 : 0);
+}
+
 cudaError_t launch_pair(const PairArgs &A, long ncolblocks, long nrows, cudaStream_t st)
 {
   static const int forced = [] {
     const char *e = getenv("TN93G_PAIR_BLOCKS");
     return e ? (atoi(e) == 3 ? 3 : 2) : 0;
   }();
-  const int minb = forced ? forced : (A.tcagg ? 3 : 2);
   dim3 g((unsigned)ncolblocks, (unsigned)((nrows + kTile - 1) / kTile));
-  return minb == 3 ? launch_pair_t<3>(A, g, st) : launch_pair_t<2>(A, g, st);
+  if (A.split && A.tcagg) {
+    cudaError_t e = launch_pair_t<4, true>(A, g, st);
+    if (e != cudaSuccess) return e;
+    const long ncol = ncolblocks * kTile;
+    // a few row groups per launch: each thread takes many rows, so that its ambiguity bounds and counters reach the
+    // global atomics once per launch, not once per row
+    const dim3 gf((unsigned)((ncol + 255) / 256), (unsigned)std::min<long>(nrows, 16));
+    static const int fb = [] {
+      const char *v = getenv("TN93G_FORMULA_BLOCKS");  // tuning knob: 2 (128 registers) or 3 (80)
+      return v && atoi(v) == 2 ? 2 : 3;
+    }();
+    if (fb == 2) {
+      if (A.tc16)
+        formula_kernel<true, 2><<<gf, 256, 0, st>>>(A, ncol);
+      else
+        formula_kernel<false, 2><<<gf, 256, 0, st>>>(A, ncol);
+    } else {
+      if (A.tc16)
+        formula_kernel<true, 3><<<gf, 256, 0, st>>>(A, ncol);
+      else
+        formula_kernel<false, 3><<<gf, 256, 0, st>>>(A, ncol);
+    }
+    return cudaGetLastError();
+  }
+  const int minb = forced ? forced : (A.tcagg ? 3 : 2);
+  return minb == 3 ? launch_pair_t<3, false>(A, g, st) : launch_pair_t<2, false>(A, g, st);
 }
 
 // the tensor-core count kernels' opt-in to their dynamic shared memory, once per device
@@ -1924,6 +2050,110 @@ int tn93g_inject_fault(tn93g_ctx *ctx, int fault)
   if (!ctx || fault < TN93G_FAULT_NONE || fault > TN93G_FAULT_SKIP_FILL) return TN93G_EINVAL;
   ctx->fault = fault;
   return TN93G_OK;
+}
+
+//------------------------------------------------------------------------------------------------ self-test
+// one thread per input: the formula up to its logarithms (in: nf[4], diag, ag, ct; out: nlog, k2p, K1..K3, arg[3]),
+// and the quotient xb[0] / xb[1] by div_by against the device's division (bad: differing bits)
+__global__ void selftest_division_kernel(const double *in, double *out, const double *xb, long n,
+                                         unsigned long long *bad)
+{
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double *p = in + 7 * t;
+  const double nf[4] = {p[0], p[1], p[2], p[3]};
+  const Prep P = tn93_prep(nf, p[4], p[5], p[6]);
+  double *o = out + 8 * t;
+  o[0] = P.nlog;
+  o[1] = P.k2p;
+  o[2] = P.K1;
+  o[3] = P.K2;
+  o[4] = P.K3;
+  o[5] = P.arg[0];
+  o[6] = P.arg[1];
+  o[7] = P.arg[2];
+  const double x = xb[2 * t], b = xb[2 * t + 1];
+  const double q = div_by(x, b, __ddiv_rn(1.0, b)), r = __ddiv_rn(x, b);
+  if (__double_as_longlong(q) != __double_as_longlong(r)) atomicAdd(bad, 1ull);
+}
+
+int tn93g_selftest_division(tn93g_ctx *ctx, long n, unsigned long long seed, long mismatches[2])
+{
+  if (!ctx || n <= 0 || !mismatches) return TN93G_EINVAL;
+  cudaSetDevice(ctx->device);
+  uint64_t st = seed * 2654435761ull + 0x9E3779B97F4A7C15ull;
+  auto rnd = [&]() {
+    st ^= st << 13;
+    st ^= st >> 7;
+    st ^= st << 17;
+    return st;
+  };
+  std::vector<double> in(7 * (size_t)n), out(8 * (size_t)n), xb(2 * (size_t)n);
+  for (long t = 0; t < n; t++) {
+    // counts as the pair kernel forms them: T clean-equivalent sites (sixteenths), base totals over both sequences
+    // summing to 2T, matches, and A<->G / C<->T transitions among the mismatches; some inputs have a base absent
+    // (K2P) or more mismatches than the formula takes (no logarithms)
+    const long L = 50 + (long)(rnd() % 30000);
+    const long T16 = 16 * (L / 2) + (long)(rnd() % (16 * (L / 2)));
+    long rest = 2 * T16, nf16[4];
+    for (int k = 0; k < 3; k++) {
+      nf16[k] = (rnd() % 8 == 0) ? 0 : (long)(rnd() % (uint64_t)(rest / 2 + 1));
+      rest -= nf16[k];
+    }
+    nf16[3] = rest;
+    const long mis16 = (long)(rnd() % (uint64_t)(T16 / (rnd() % 4 == 0 ? 1 : 8) + 1));
+    const long ag16 = (long)(rnd() % (uint64_t)(mis16 + 1)), ct16 = (long)(rnd() % (uint64_t)(mis16 - ag16 + 1));
+    double *p = &in[7 * (size_t)t];
+    for (int k = 0; k < 4; k++) p[k] = (double)nf16[k] / 16.0;
+    p[4] = (double)(T16 - mis16) / 16.0;
+    p[5] = (double)ag16 / 16.0;
+    p[6] = (double)ct16 / 16.0;
+    // quotients over 80 binades of divisor, either sign of dividend
+    const double m = 1.0 + (double)(rnd() >> 12) * 0x1p-52, mb = 1.0 + (double)(rnd() >> 12) * 0x1p-52;
+    const int ex = (int)(rnd() % 81) - 40, eb = (int)(rnd() % 81) - 40;
+    xb[2 * (size_t)t] = ldexp(rnd() & 1 ? -m : m, ex);
+    xb[2 * (size_t)t + 1] = ldexp(mb, eb);
+  }
+  DevBuf din, dout, dxb, dbad;
+  const cudaStream_t st2 = ctx->stream;
+  int rc = TN93G_OK;
+  do {
+    if ((rc = ensure(ctx, din, in.size() * 8)) != TN93G_OK || (rc = ensure(ctx, dout, out.size() * 8)) != TN93G_OK ||
+        (rc = ensure(ctx, dxb, xb.size() * 8)) != TN93G_OK || (rc = ensure(ctx, dbad, 8)) != TN93G_OK)
+      break;
+    unsigned long long bad = 0;
+    if (cudaMemcpyAsync(din.p, in.data(), in.size() * 8, cudaMemcpyHostToDevice, st2) != cudaSuccess ||
+        cudaMemcpyAsync(dxb.p, xb.data(), xb.size() * 8, cudaMemcpyHostToDevice, st2) != cudaSuccess ||
+        cudaMemsetAsync(dbad.p, 0, 8, st2) != cudaSuccess) {
+      rc = TN93G_ECUDA;
+      break;
+    }
+    selftest_division_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st2>>>(
+        (const double *)din.p, (double *)dout.p, (const double *)dxb.p, n, (unsigned long long *)dbad.p);
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(out.data(), dout.p, out.size() * 8, cudaMemcpyDeviceToHost, st2) != cudaSuccess ||
+        cudaMemcpyAsync(&bad, dbad.p, 8, cudaMemcpyDeviceToHost, st2) != cudaSuccess ||
+        cudaStreamSynchronize(st2) != cudaSuccess) {
+      rc = TN93G_ECUDA;
+      break;
+    }
+    long diff = 0;
+    for (long t = 0; t < n; t++) {
+      const double *p = &in[7 * (size_t)t];
+      const double nf[4] = {p[0], p[1], p[2], p[3]};
+      const Prep P = tn93_prep(nf, p[4], p[5], p[6]);
+      const double want[8] = {(double)P.nlog, (double)P.k2p, P.K1, P.K2, P.K3, P.arg[0], P.arg[1], P.arg[2]};
+      if (memcmp(want, &out[8 * (size_t)t], sizeof want) != 0) diff++;
+    }
+    mismatches[0] = diff;
+    mismatches[1] = (long)bad;
+  } while (0);
+  for (DevBuf *b : {&din, &dout, &dxb, &dbad})
+    if (b->p) {
+      cudaFree(b->p);
+      ctx->used -= b->n;
+    }
+  return rc;
 }
 
 int tn93g_create(tn93g_ctx **out, int device, size_t hbm_budget)
@@ -2348,7 +2578,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   // per band parity (double-buffered): distances, segment statistics, row sums; the replay queue is per band
   const size_t dslots = (size_t)band * ncols;
   TRY(ensure(ctx, ctx->dist, 2 * dslots * sizeof(double)));
-  const int tc16 = 2 * Lc < 65536;
+  const int tc16 = 32 * L < 65536;  // the final x16 aggregates fit 16-bit lanes
   // the tensor-core path's row chunks per band (boundaries on the count kernel's 32-row tiles)
   std::vector<std::vector<std::pair<long, long>>> band_chunks(bands.size());
   size_t chunk_slots = 1;
@@ -2568,11 +2798,12 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
         AC.dist = A.dist + (size_t)(c0 - r0) * ncols;
         AC.tcagg = ctx->tcagg.p;
         AC.tc16 = tc16;
+        AC.split = pair_split(AC.rc);
         const long cb0 = (ccs - colbase) / 32, cbs = (ncols + 31) / 32 - cb0;
         if (cbs > 0) {
           AC.cstart = colbase + cb0 * 32;
           CU(launch_pair(AC, cbs, c1 - c0, st));
-          ctx->launches++;
+          ctx->launches += AC.split ? 2 : 1;
         }
       }
       nchunks[par] = (int)chunks.size();
@@ -2611,6 +2842,11 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   int pend_par[2] = {0, 0}, pend_n = 0;
   size_t pend_bytes[2] = {0, 0};
   bool par_used[2] = {false, false};
+  // TN93G_TRACE=1: one stderr line per delivered band (device milliseconds from the run's first event: write
+  // start and end, copy start and end; host milliseconds when the copy was seen complete), for pipeline tuning
+  static const bool trace = getenv("TN93G_TRACE") != nullptr;
+  const auto host0 = std::chrono::steady_clock::now();
+  int delivered = 0;
   auto deliver_oldest = [&]() -> int {
     const int q = pend_par[0];
     CU(cudaEventSynchronize(ctx->evc1[q]));
@@ -2618,6 +2854,16 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     ctx->timings[4] += ms;
     CU(cudaEventElapsedTime(&ms, ctx->evc0[q], ctx->evc1[q]));
     ctx->timings[5] += ms;
+    if (trace) {
+      float w0, w1, c0, c1;
+      CU(cudaEventElapsedTime(&w0, E[0], ctx->evw0[q]));
+      CU(cudaEventElapsedTime(&w1, E[0], ctx->evw1[q]));
+      CU(cudaEventElapsedTime(&c0, E[0], ctx->evc0[q]));
+      CU(cudaEventElapsedTime(&c1, E[0], ctx->evc1[q]));
+      const double h = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - host0).count();
+      fprintf(stderr, "tn93g trace: band %d bytes %zu write %.3f-%.3f copy %.3f-%.3f host %.3f\n", delivered++,
+              pend_bytes[q], w0, w1, c0, c1, h);
+    }
     pend_par[0] = pend_par[1];
     pend_n--;
     if (sink && sink(user, (const char *)ctx->pin2[q], pend_bytes[q])) return TN93G_ESINK;
@@ -2713,7 +2959,14 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
       dev_off += tot;
       return TN93G_OK;
     }
-    // this parity's text buffers were last used by an older band, already delivered; wait for its copy
+    // this parity's text buffers were last used by an older band. When the bands between them wrote no text, that
+    // band's text may not have gone to the sink yet: deliver it (and any older one) before the buffers are reused.
+    for (;;) {
+      bool held = false;
+      for (int q = 0; q < pend_n; q++) held |= pend_par[q] == par;
+      if (!held) break;
+      TRY(deliver_oldest());
+    }
     if (par_used[par]) CU(cudaEventSynchronize(ctx->evc1[par]));
     TRY(ensure(ctx, ctx->out2[par], tot));
     TRY(ensure_pinned_at(ctx, ctx->pin2[par], ctx->pin2_n[par], tot));
@@ -2784,6 +3037,12 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   CU(cudaMemcpyAsync(ambw, ctx->amb.p, sizeof ambw, cudaMemcpyDeviceToHost, st));
   CU(cudaEventRecord(E[9], st));
   CU(cudaStreamSynchronize(st));
+  if (trace) {
+    float d9;
+    CU(cudaEventElapsedTime(&d9, E[0], E[9]));
+    fprintf(stderr, "tn93g trace: end device %.3f host %.3f bands %d\n", d9,
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - host0).count(), nb);
+  }
   CU(cudaEventElapsedTime(&ms, E[0], E[1]));
   ctx->timings[0] = ms;
   CU(cudaEventElapsedTime(&ms, E[0], E[9]));
@@ -3527,7 +3786,7 @@ int tn93g_server_create(tn93g_ctx *ctx, tn93g_server **out, const uint8_t *codes
   if (ctx->count_path == 1) {
     srv->tc_NB = (N + max_batch_sequences + 31) / 32 + 1;
     srv->tc_KS = (L + kTcStageK - 1) / kTcStageK;
-    srv->tc16 = 2 * L < 65536;
+    srv->tc16 = 32 * L < 65536;
     const size_t img = (size_t)srv->tc_KS * srv->tc_NB * kTcBlockBytes;
     const size_t agg = (size_t)N * kServerTcChunk * (srv->tc16 ? 16 : 32);
     if (ensure(ctx, srv->ohimg, img) == TN93G_OK && ensure(ctx, srv->tcagg, agg) == TN93G_OK &&
@@ -3750,11 +4009,12 @@ int tn93g_server_batch(tn93g_server *srv, int nq, const tn93g_alignment *queries
         PairArgs AC = A;
         AC.tcagg = srv->tcagg.p;
         AC.tc16 = srv->tc16;
+        AC.split = pair_split(AC.rc);
         AC.tcncols = kServerTcChunk;
         AC.tccolbase = c0;
         AC.cstart = c0;
         CU(launch_pair(AC, (c1 - c0 + 31) / 32, Nref, st));
-        ctx->launches += 2;
+        ctx->launches += AC.split ? 3 : 2;
       }
     } else {
       CU(launch_pair(A, (Q + 31) / 32, Nref, st));

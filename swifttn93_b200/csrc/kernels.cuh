@@ -90,9 +90,12 @@ struct PairArgs {
   unsigned long long *counters;  // [0] pairs with an ambiguous log, [1] undecided pairs
   const LogTable *logt;
   ExactSink ex;
-  const void *tcagg = nullptr;  // clean-site aggregates from the tensor-core kernel: one record per pair slot of
-                                // [band rows][ncols], 8 uint16 (16 bytes) or 8 int32 (32 bytes), 7 used
-  int tc16 = 0;                 // the aggregates are uint16 (every value fits: 2 Lc < 65536), else int32
+  void *tcagg = nullptr;  // clean-site aggregates from the tensor-core kernel: one record per pair slot of
+                          // [band rows][ncols], 8 uint16 (16 bytes) or 8 int32 (32 bytes), 7 used; with split, the
+                          // pair kernel writes the pair's final x16 aggregates back into it
+  int tc16 = 0;           // the records are uint16 (every final aggregate fits: 32 L < 65536), else int32
+  int split = 0;          // tensor-core path only: the pair kernel stops before the formula, which formula_kernel
+                          // finishes from the records
   long tcncols = 0, tccolbase = 0;  // row stride and first column of the aggregates when they hold a chunk of the
                                     // columns (0: the same as ncols and colbase)
 };

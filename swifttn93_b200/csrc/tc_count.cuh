@@ -7,8 +7,9 @@
 // accumulates D = A' B'^T, whose 4x4 blocks are the pairs' tables. The epilogue turns each table into the seven
 // clean-site aggregates the pair kernel needs (jointly clean sites, matches, A<->G and C<->T transitions, and the
 // A, C, G base counts over both sequences) and stores one record per pair slot of [band rows][band columns]: eight
-// uint16 (16 bytes, the eighth unused) when twice the column count fits in 16 bits (the largest aggregate is a base
-// count over both sequences), else eight int32 (32 bytes). The pair kernel reads a record with one vector load.
+// uint16 (16 bytes, the eighth unused) when the caller asks for them (agg16: the engine's runs do when 32 L < 65536,
+// so that the pair kernel can write the final x16 aggregates, at most 32 L, back into the same slot), else eight
+// int32 (32 bytes). The pair kernel reads a record with one vector load.
 //
 // Operand image in HBM (built by onehot_kernel from the compressed codes): per 128-column stage s and 32-sequence
 // block b a 16 KB block at (s * NB + b) * 16 KB, in the canonical K-major layout without swizzle: row r =

@@ -189,8 +189,31 @@ struct Prep {
   double arg[3];
 };
 
+// x / b rounded to nearest, given y = RN(1 / b). On the device the quotient is corrected twice with fused
+// multiply-adds (P. Markstein, "Computation of elementary functions on the IBM RISC System/6000 processor", IBM J.
+// Res. Dev. 34(1), 1990; J.-M. Muller et al., Handbook of Floating-Point Arithmetic, ch. on FMA-based division):
+// q0 = RN(x y) lies within 1.5 ulp of x / b; q1 = RN(q0 + r0 y) with r0 = RN(x - b q0) lies within 1 ulp; then
+// r1 = x - b q1 is exact and RN(q1 + r1 y) = RN(x / b) by Markstein's theorem. It holds while no product or
+// remainder underflows or overflows, which the formula cannot reach: base frequencies are at least 2^-31 (a
+// sixteenth of a count over at most 2^26 sites), so every nonzero operand lies between 2^-200 and 2^200. Several
+// quotients share one divisor, so one true division (the reciprocal) serves all of them. The host build divides.
+TN_HD double div_by(double x, double b, double y)
+{
+#if defined(__CUDA_ARCH__)
+  const double q0 = TMUL(x, y);
+  const double r0 = TFMA(-q0, b, x);
+  const double q1 = TFMA(r0, y, q0);
+  const double r1 = TFMA(-q1, b, x);
+  return TFMA(r1, y, q1);
+#else
+  (void)y;
+  return x / b;
+#endif
+}
+
 // tn93's formula (refkernel.cpp:752-803, swifttn93.cpp:1954-2001) with every IEEE operation in its order, split
-// at the logarithms: tn93_prep computes their arguments, tn93_combine the distance from their values.
+// at the logarithms: tn93_prep computes their arguments, tn93_combine the distance from their values. Every
+// quotient is the correctly rounded one (div_by with the divisor's reciprocal, or a true division).
 TN_HD Prep tn93_prep(const double nf[4], double diag, double ag_in, double ct_in)
 {
   Prep P;
@@ -202,10 +225,14 @@ TN_HD Prep tn93_prep(const double nf[4], double diag, double ag_in, double ct_in
   const double fR = TADD(f0, f2), fY = TADD(f1, f3);
   P.k2p = nf[0] == 0 || nf[1] == 0 || nf[2] == 0 || nf[3] == 0;
   P.K1 = P.K2 = P.K3 = 0;
+  double rR = 0, rY = 0;  // RN(1 / fR), RN(1 / fY)
   if (!P.k2p) {
-    P.K1 = TDIV(TMUL(TMUL(2.0, f0), f2), fR);
-    P.K2 = TDIV(TMUL(TMUL(2.0, f1), f3), fY);
-    P.K3 = TMUL(2.0, TSUB(TSUB(TMUL(fR, fY), TDIV(TMUL(TMUL(f0, f2), fY), fR)), TDIV(TMUL(TMUL(f1, f3), fR), fY)));
+    rR = TDIV(1.0, fR);
+    rY = TDIV(1.0, fY);
+    P.K1 = div_by(TMUL(TMUL(2.0, f0), f2), fR, rR);
+    P.K2 = div_by(TMUL(TMUL(2.0, f1), f3), fY, rY);
+    P.K3 = TMUL(2.0, TSUB(TSUB(TMUL(fR, fY), div_by(TMUL(TMUL(f0, f2), fY), fR, rR)),
+                          div_by(TMUL(TMUL(f1, f3), fR), fY, rY)));
   }
   double AG = TMUL(ag_in, tng), CT = TMUL(ct_in, tng);
   double tv = TSUB(1.0, TADD(TADD(TMUL(diag, tng), AG), CT));
@@ -218,9 +245,10 @@ TN_HD Prep tn93_prep(const double nf[4], double diag, double ag_in, double ct_in
     P.arg[2] = 1.0;
     P.nlog = (AG > 0. && CT > 0.) ? 2 : 0;
   } else {
-    AG = TSUB(TSUB(1.0, TDIV(AG, P.K1)), TDIV(TMUL(0.5, tv), fR));
-    CT = TSUB(TSUB(1.0, TDIV(CT, P.K2)), TDIV(TMUL(0.5, tv), fY));
-    tv = TSUB(1.0, TDIV(TDIV(TMUL(0.5, tv), fY), fR));
+    const double htv = TMUL(0.5, tv), hY = div_by(htv, fY, rY);
+    AG = TSUB(TSUB(1.0, TDIV(AG, P.K1)), div_by(htv, fR, rR));
+    CT = TSUB(TSUB(1.0, TDIV(CT, P.K2)), hY);
+    tv = TSUB(1.0, div_by(hY, fR, rR));
     P.arg[0] = AG;
     P.arg[1] = CT;
     P.arg[2] = tv;

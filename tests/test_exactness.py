@@ -152,6 +152,17 @@ def test_bounded_wait_times_out_and_context_recovers():
     assert got == want and summ.undecided == 0
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_division_scheme_is_exact(seed):
+    """The device formula shares one true division per divisor and finishes each quotient with two fused
+    multiply-add corrections: its outputs up to the logarithms equal the host's IEEE-division evaluation bit for bit,
+    and its quotients over 80 binades equal the device's correctly rounded division."""
+    from swifttn93_b200 import Engine
+
+    assert Engine().selftest_division(2_000_000, seed) == (0, 0)
+
+
 #----------------------------------------------------------------------------------------------- CPU
 def _summary(mean, weighted, mx, bounds):
     from swifttn93_b200 import _Summary
