@@ -453,6 +453,30 @@ __device__ __forceinline__ void add_packed(PackedAcc &p, const uint32_t (*tab)[4
   p.f |= flags[k];
 }
 
+// Adds the packed table entries of the events [e0, e1) of one sequence against the partner at column p of the
+// position-major code matrix. Four events per step: their words and partner codes are loaded before any sum, so
+// that four partner-code loads (mostly from L2) are in flight at once.
+__device__ __forceinline__ void add_events(PackedAcc &p, const uint32_t (*tab)[4], const uint32_t *flags,
+                                           const uint32_t *ev, const uint8_t *ccT, long Np, long partner,
+                                           uint32_t e0, uint32_t e1)
+{
+  uint32_t e = e0;
+  for (; e + 4 <= e1; e += 4) {
+    uint32_t v[4];
+    int pc[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) v[q] = __ldg(ev + e + q);
+#pragma unroll
+    for (int q = 0; q < 4; q++) pc[q] = __ldg(ccT + (size_t)(v[q] >> 5) * Np + partner);
+#pragma unroll
+    for (int q = 0; q < 4; q++) add_packed(p, tab, flags, ((v[q] & 31) - 4) * kCodes + pc[q]);
+  }
+  for (; e < e1; e++) {
+    const uint32_t v = __ldg(ev + e);
+    add_packed(p, tab, flags, ((v & 31) - 4) * kCodes + __ldg(ccT + (size_t)(v >> 5) * Np + partner));
+  }
+}
+
 // One tile of pairs: rows [i0, i0 + 8 * rpw) (rpw = rows per warp, 1..4) x columns [j0, j0 + 32). The block's
 // tables must be in smem (load_pair_tables). All threads of the block call it with the same arguments.
 template <bool WPLANE, bool GAPMM, bool SPLIT>
@@ -479,14 +503,7 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const unsigned char
       int *dst = colacc + lane * kColAccStride + cl * 9;
       if (packed) {
         PackedAcc p = {0u, 0u, 0u, 0u, 0u};
-        if (j < rc.N) {
-          const uint32_t f0 = a.ev_off[j], f1 = a.ev_off[j + 1];
-          for (uint32_t e = f0; e < f1; e++) {
-            const uint32_t v = __ldg(a.ev + e);
-            const int pc = a.ccT[(size_t)(v >> 5) * Np + ib];
-            add_packed(p, PT.col, PT.colf, ((v & 31) - 4) * kCodes + pc);
-          }
-        }
+        if (j < rc.N) add_events(p, PT.col, PT.colf, a.ev, a.ccT, Np, ib, a.ev_off[j], a.ev_off[j + 1]);
         dst[0] = (int)p.w0;
         dst[1] = (int)p.w1;
         dst[2] = (int)p.w2;
@@ -561,11 +578,7 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const unsigned char
     const uint32_t e0 = a.ev_off[i], e1 = a.ev_off[i + 1];
     if (packed) {
       PackedAcc p = {(uint32_t)src[0], (uint32_t)src[1], (uint32_t)src[2], (uint32_t)src[3], (uint32_t)src[4]};
-      for (uint32_t e = e0; e < e1; e++) {
-        const uint32_t v = __ldg(a.ev + e);
-        const int pc = a.ccT[(size_t)(v >> 5) * Np + jj];
-        add_packed(p, PT.row, PT.rowf, ((v & 31) - 4) * kCodes + pc);
-      }
+      add_events(p, PT.row, PT.rowf, a.ev, a.ccT, Np, jj, e0, e1);
       acc[0] = (int)(p.w0 & 0xFFFFu);
       acc[1] = (int)(p.w0 >> 16);
       acc[2] = (int)(p.w1 & 0xFFFFu);
@@ -1081,6 +1094,42 @@ __device__ __forceinline__ PairView view_pair(const RowArgs &a, long i, long j, 
   return v;
 }
 
+// A printed distance handed from the stats kernel to the writer, one 32-bit word per pair slot: 0 = not printed;
+// kind 1 (bits 30-31) = the six digits q (bits 0-19) and the decimal exponent X + 16 (bits 20-25) of a value in
+// [1e-5, 1e5); kind 2 = zero ("0"); kind 3 = any other value (the writer formats the double itself). len receives
+// the length of the text. d is a reported distance: not negative, not NaN.
+__device__ __forceinline__ uint32_t print_code(double d, int &len)
+{
+  if (d == 0.0) {
+    len = 1;
+    return 2u << 30;
+  }
+  if (d >= 1e-5 && d < 1e5) {
+    const Dec D = decimal6(d);
+    len = dec_len(D);
+    return (1u << 30) | ((uint32_t)(D.X + 16) << 20) | D.q;
+  }
+  len = fmt_g_len(d);
+  return 3u << 30;
+}
+
+// the text of a printed-distance code (d: the distance, read only for kind 3); returns the length
+__device__ __forceinline__ int fmt_code(uint32_t code, double d, char *out)
+{
+  const uint32_t kind = code >> 30;
+  if (kind == 1) {
+    Dec D;
+    D.q = code & 0xFFFFFu;
+    D.X = (int)((code >> 20) & 63u) - 16;
+    return fmt_dec(D, out);
+  }
+  if (kind == 2) {
+    out[0] = '0';
+    return 1;
+  }
+  return fmt_g(d, out);
+}
+
 // what the text writers need of a pair: whether it is reported, and its printed distance (tn93's "<= 0 -> 0")
 __device__ __forceinline__ bool linked_pair(const RowArgs &a, long i, long j, double &thisD)
 {
@@ -1143,11 +1192,16 @@ __device__ __forceinline__ void stats_rows(const RowArgs &a, long bx, int sg)
       } else if (v.computed) {
         atomicAdd(&sh[key], (unsigned long long)v.w);
       }
+      uint32_t code = 0;
       if (v.valid && v.linked) {
         links += v.w;
         if (rc.emit) {
           if (rc.format != 2) {
-            const int gl = fmt_g_len(v.thisD);
+            int gl;
+            if (a.dcode)
+              code = print_code(v.thisD, gl);
+            else
+              gl = fmt_g_len(v.thisD);
             bytes += rc.format == 0 ? nli + a.name_len[j] + gl + 3 : dli + digits_of(j) + gl + 3;
           } else {
             a.hy[(size_t)i * rc.N + j] = v.thisD;
@@ -1155,6 +1209,7 @@ __device__ __forceinline__ void stats_rows(const RowArgs &a, long bx, int sg)
           }
         }
       }
+      if (a.dcode && v.valid) a.dcode[(size_t)(i - a.r0) * a.ncols + (j - a.colbase)] = code;
       if (v.valid && !v.counted) skipped++;
       if (v.valid && v.counted) {
         if (v.bin == 0) m0 = v.thisD > m0 ? v.thisD : m0;
@@ -1429,11 +1484,20 @@ __device__ __forceinline__ void write_rows(const RowArgs &a, long bx, int sg)
   for (long j0 = c0; j0 < c1; j0 += 32) {
     const long j = j0 + lane;
     double thisD = 0.;
-    const bool put = j < c1 && linked_pair(a, i, j, thisD);
+    bool put;
+    uint32_t code = 0;
+    if (a.dcode) {
+      // the stats kernel's code of this pair: printed or not, and its digits
+      code = j < c1 ? a.dcode[(size_t)(i - a.r0) * a.ncols + (j - a.colbase)] : 0u;
+      put = code != 0;
+      if (put && (code >> 30) == 3u) linked_pair(a, i, j, thisD);
+    } else {
+      put = j < c1 && linked_pair(a, i, j, thisD);
+    }
     char g[24];
     int gl = 0, len = 0;
     if (put) {
-      gl = fmt_g(thisD, g);
+      gl = a.dcode ? fmt_code(code, thisD, g) : fmt_g(thisD, g);
       len = rc.format == 0 ? nli + a.name_len[j] + gl + 3 : dli + digits_of(j) + gl + 3;
     }
     int pre = len;
@@ -1672,18 +1736,17 @@ cudaError_t launch_pair_t(const PairArgs &A, dim3 g, cudaStream_t st)
 // Resident blocks per SM: 3 (80 registers a thread) when the clean-site counts come from the tensor cores, 2 (128)
 // with the popcount loop, which needs the registers (measured: 3 is 11% faster on the tensor-core path, and slower
 // with the popcount loop). TN93G_PAIR_BLOCKS=2|3 overrides.
-// Whether the tensor-core path splits the pair stage into the event kernel and formula_kernel: when the N plane is
-// in use (gapmm, or many N), whose popcount loop runs faster in the split kernel's 64 registers; otherwise one fused
-// kernel overlaps the formula with the event sums better (measured on the 6,700 x 1,500 HIV benchmark set: split
-// 5.57 ms vs fused 6.15 ms per gapmm pair stage, fused 3.46 ms vs split 3.73 ms under resolve). TN93G_PAIR_SPLIT=0|1
-// forces either; both give the same bytes.
-int pair_split(const RunConsts &rc)
+// Whether the tensor-core path splits the pair stage into the event kernel and formula_kernel. One fused kernel
+// overlaps the formula with the event sums and is the faster form on the 6,700 x 1,500 HIV benchmark set in every
+// mode once the event loads are batched (fused 3.31 / 5.44 ms vs split 3.62 / 6.13 ms per resolve / gapmm pair
+// stage), so it is the default; TN93G_PAIR_SPLIT=1 selects the split form, which gives the same bytes.
+int pair_split(const RunConsts &)
 {
   static const int v = [] {
     const char *e = getenv("TN93G_PAIR_SPLIT");
-    return e ? (atoi(e) ? 1 : 0) : -1;
+    return e && atoi(e) ? 1 : 0;
   }();
-  return v >= 0 ? v : (rc.wplane ? 1 : 0);
+  return v;
 }
 
 cudaError_t launch_pair(const PairArgs &A, long ncolblocks, long nrows, cudaStream_t st)
@@ -1805,12 +1868,13 @@ struct tn93g_ctx {
   LogTable *d_logt = nullptr;
   Tables *h_tab = nullptr;
   PairTables *h_ptab = nullptr;  // host staging of the pair stage's tables
-  DevBuf seen, nN, varcol, planes, cc, ccT, evcount, evoff, ev, agg, site, dist, rq, rqn, counters, rbytes, rsum, rw,
+  DevBuf seen, nN, varcol, planes, cc, ccT, evcount, evoff, ev, agg, site, dist, dcode, rq, rqn, counters, rbytes, rsum, rw,
       rmax, rlinks, rskip, hist, roff, out, hy;
   void *pinned = nullptr;
   size_t pinned_n = 0;
   cudaEvent_t evs[16];
-  cudaStream_t copy_stream = nullptr;  // device->host copies of finished bands
+  cudaStream_t copy_stream = nullptr;   // device->host copies of finished bands
+  cudaStream_t write_stream = nullptr;  // text writers of finished bands (beside the next bands' kernels)
   cudaEvent_t evw0[2], evw1[2], evc0[2], evc1[2];
   cudaEvent_t evk[2][5];  // per band parity: start, after pair, after replay, after stats+sums+scan, stats on host
   cudaEvent_t evcnt[2][2 * kMaxTcChunks];  // per band parity: around each chunk's tensor-core count kernel
@@ -1880,14 +1944,14 @@ int ensure_pinned(tn93g_ctx *ctx, size_t bytes)
   return TN93G_OK;
 }
 
-int ensure_pinned_at(tn93g_ctx *ctx, void *&p, size_t &n, size_t bytes)
+int ensure_pinned_at(tn93g_ctx *ctx, void *&p, size_t &n, size_t bytes, unsigned flags = cudaHostAllocDefault)
 {
   if (bytes <= n && p) return TN93G_OK;
   if (p) cudaFreeHost(p);
   p = nullptr;
   n = 0;
   bytes = std::max<size_t>(bytes + bytes / 4, 1 << 20);
-  CU(cudaHostAlloc(&p, bytes, cudaHostAllocDefault));
+  CU(cudaHostAlloc(&p, bytes, flags));
   n = bytes;
   return TN93G_OK;
 }
@@ -2052,6 +2116,22 @@ int tn93g_inject_fault(tn93g_ctx *ctx, int fault)
   return TN93G_OK;
 }
 
+// Copies up to nine ranges of 8-byte words into pinned host memory that the device maps (a band's statistics), so
+// that they reach the host without a copy-engine transfer, which would queue behind the band texts in flight.
+struct Gather {
+  const unsigned long long *src[9];
+  unsigned long long *dst[9];
+  long n[9];
+  int k;
+};
+
+__global__ void __launch_bounds__(256) gather_kernel(Gather g)
+{
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (int r = 0; r < g.k; r++)
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < g.n[r]; t += stride) g.dst[r][t] = g.src[r][t];
+}
+
 //------------------------------------------------------------------------------------------------ self-test
 // one thread per input: the formula up to its logarithms (in: nf[4], diag, ag, ct; out: nlog, k2p, K1..K3, arg[3]),
 // and the quotient xb[0] / xb[1] by div_by against the device's division (bad: differing bits)
@@ -2187,6 +2267,7 @@ int tn93g_create(tn93g_ctx **out, int device, size_t hbm_budget)
         if (cudaEventCreate(&e) != cudaSuccess) rc = TN93G_ECUDA;
     }
     if (cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) rc = TN93G_ECUDA;
+    if (cudaStreamCreateWithFlags(&ctx->write_stream, cudaStreamNonBlocking) != cudaSuccess) rc = TN93G_ECUDA;
     if (const char *e = getenv("TN93G_COUNT")) ctx->count_path = strcmp(e, "popc") == 0 ? 0 : 1;
     {
       const char *b = getenv("TN93G_LOG_BAND"), *p = getenv("TN93G_LOG_SPREAD");
@@ -2216,7 +2297,7 @@ void tn93g_destroy(tn93g_ctx *ctx)
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   DevBuf *bufs[] = {&ctx->seen, &ctx->nN, &ctx->varcol, &ctx->planes, &ctx->cc, &ctx->ccT, &ctx->evcount,
-                    &ctx->evoff, &ctx->ev, &ctx->agg, &ctx->site, &ctx->dist, &ctx->rq, &ctx->rqn, &ctx->counters,
+                    &ctx->evoff, &ctx->ev, &ctx->agg, &ctx->site, &ctx->dist, &ctx->dcode, &ctx->rq, &ctx->rqn, &ctx->counters,
                     &ctx->rbytes, &ctx->rsum, &ctx->rw, &ctx->rmax, &ctx->rlinks, &ctx->rskip, &ctx->hist,
                     &ctx->roff, &ctx->out, &ctx->hy};
   for (DevBuf *b : bufs)
@@ -2242,6 +2323,7 @@ void tn93g_destroy(tn93g_ctx *ctx)
   for (auto &b : ctx->set_pool) cudaFree(b.first);
   if (ctx->pstats) cudaFreeHost(ctx->pstats);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  if (ctx->write_stream) cudaStreamDestroy(ctx->write_stream);
   for (auto &e : ctx->evs)
     if (e) cudaEventDestroy(e);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -2578,6 +2660,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   // per band parity (double-buffered): distances, segment statistics, row sums; the replay queue is per band
   const size_t dslots = (size_t)band * ncols;
   TRY(ensure(ctx, ctx->dist, 2 * dslots * sizeof(double)));
+  if (rc.emit && !hyphy) TRY(ensure(ctx, ctx->dcode, 2 * dslots * sizeof(uint32_t)));
   const int tc16 = 32 * L < 65536;  // the final x16 aggregates fit 16-bit lanes
   // the tensor-core path's row chunks per band (boundaries on the count kernel's 32-row tiles)
   std::vector<std::vector<std::pair<long, long>>> band_chunks(bands.size());
@@ -2630,7 +2713,9 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   const size_t stat_stride = (size_t)band * 6 * sizeof(double) +
                              (size_t)nseg * (3 * sizeof(double) + 2 * sizeof(long long)) +
                              (3 + 3 * kHistBins) * sizeof(unsigned long long);
-  TRY(ensure_pinned_at(ctx, ctx->pstats, ctx->pstats_n, 2 * stat_stride));
+  TRY(ensure_pinned_at(ctx, ctx->pstats, ctx->pstats_n, 2 * stat_stride, cudaHostAllocMapped));
+  char *d_pstats = nullptr;  // the device's address of the staging
+  CU(cudaHostGetDevicePointer((void **)&d_pstats, ctx->pstats, 0));
   CU(cudaMemsetAsync(ctx->counters.p, 0, 4 * sizeof(unsigned long long), st));
   double max_[3] = {0, 0, 0}, mean[3] = {0, 0, 0}, wc[3] = {0, 0, 0};
   unsigned long long hist_total[3 * kHistBins];
@@ -2684,6 +2769,7 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     RA.out = nullptr;
     RA.hy = (double *)ctx->hy.p;
     RA.err = (unsigned long long *)ctx->counters.p + 3;
+    RA.dcode = (rc.emit && !hyphy) ? (uint32_t *)ctx->dcode.p + par * dslots : nullptr;
     return RA;
   };
   // stats -> sums -> scan of band bi, then its statistics to the host (on the compute stream)
@@ -2704,20 +2790,33 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     CU(cudaGetLastError());
     ctx->launches++;
     CU(cudaEventRecord(K[3], st));
+    // the band's statistics into the mapped staging (device addresses at the same offsets as host_stats')
     const HostStats h = host_stats(par);
-    CU(cudaMemcpyAsync(h.sum, RA.row_sum, nr * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(h.w, RA.row_w, nr * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(h.max, RA.seg_max, nr * maxseg * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(h.links, RA.seg_links, nr * maxseg * sizeof(long long), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(h.skip, RA.seg_skip, nr * maxseg * sizeof(long long), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(h.total, dtot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(h.hist, RA.hist, 3 * kHistBins * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
-    CU(cudaMemcpyAsync(h.und, (unsigned long long *)ctx->undn.p + par, sizeof(unsigned long long),
-                       cudaMemcpyDeviceToHost, st));
+    auto dev = [&](const void *hp) {
+      return (unsigned long long *)(d_pstats + ((const char *)hp - (const char *)ctx->pstats));
+    };
+    Gather g;
+    g.k = 0;
+    auto add = [&](const void *src, const void *hdst, long nwords) {
+      g.src[g.k] = (const unsigned long long *)src;
+      g.dst[g.k] = dev(hdst);
+      g.n[g.k++] = nwords;
+    };
+    add(RA.row_sum, h.sum, nr * 3);
+    add(RA.row_w, h.w, nr * 3);
+    add(RA.seg_max, h.max, nr * maxseg * 3);
+    add(RA.seg_links, h.links, nr * maxseg);
+    add(RA.seg_skip, h.skip, nr * maxseg);
+    add(dtot, h.total, 1);
+    add(RA.hist, h.hist, 3 * kHistBins);
+    add((unsigned long long *)ctx->undn.p + par, h.und, 1);
     if (use_tc)
-      CU(cudaMemcpyAsync(h.tcerr, ctx->tcerr.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+      add(ctx->tcerr.p, h.tcerr, 1);
     else
       *h.tcerr = 0;
+    gather_kernel<<<32, 256, 0, st>>>(g);
+    CU(cudaGetLastError());
+    ctx->launches++;
     CU(cudaEventRecord(K[4], st));
     return TN93G_OK;
   };
@@ -2726,6 +2825,8 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     const int par = bi & 1;
     const long r0 = bands[bi].first, r1 = bands[bi].second, nr = r1 - r0;
     cudaEvent_t *K = ctx->evk[par];
+    // this parity's distances, codes and row arrays are read by band bi - 2's text writer on the write stream
+    if (bi >= 2 && stream_text) CU(cudaStreamWaitEvent(st, ctx->evw1[par], 0));
     CU(cudaEventRecord(K[0], st));
     CU(cudaMemsetAsync(ctx->rqn.p, 0, sizeof(unsigned), st));
     CU(cudaMemsetAsync((unsigned long long *)ctx->undn.p + par, 0, sizeof(unsigned long long), st));
@@ -2959,23 +3060,28 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
       dev_off += tot;
       return TN93G_OK;
     }
-    // this parity's text buffers were last used by an older band. When the bands between them wrote no text, that
-    // band's text may not have gone to the sink yet: deliver it (and any older one) before the buffers are reused.
+    // The band's text is written on the write stream, beside the next band's kernels, once its statistics are final
+    // (K[4]), then copied on the copy stream. The older band of this parity (or, when the bands between them wrote
+    // no text, an even older one) goes to the sink first: its copy has then left the device buffer, the sink has
+    // taken the pinned buffer, and its write and copy events are free to record this band's. Meanwhile the copy
+    // engine works on the band in between.
     for (;;) {
       bool held = false;
       for (int q = 0; q < pend_n; q++) held |= pend_par[q] == par;
       if (!held) break;
       TRY(deliver_oldest());
     }
-    if (par_used[par]) CU(cudaEventSynchronize(ctx->evc1[par]));
+    const cudaStream_t ws = ctx->write_stream;
     TRY(ensure(ctx, ctx->out2[par], tot));
     TRY(ensure_pinned_at(ctx, ctx->pin2[par], ctx->pin2_n[par], tot));
     RA.out = (char *)ctx->out2[par].p;
-    CU(cudaEventRecord(ctx->evw0[par], st));
-    write_kernel<<<wgrid, 256, 0, st>>>(RA);
+    CU(cudaStreamWaitEvent(ws, K[4], 0));
+    if (par_used[par]) CU(cudaStreamWaitEvent(ws, ctx->evc1[par], 0));
+    CU(cudaEventRecord(ctx->evw0[par], ws));
+    write_kernel<<<wgrid, 256, 0, ws>>>(RA);
     CU(cudaGetLastError());
     ctx->launches++;
-    CU(cudaEventRecord(ctx->evw1[par], st));
+    CU(cudaEventRecord(ctx->evw1[par], ws));
     CU(cudaStreamWaitEvent(ctx->copy_stream, ctx->evw1[par], 0));
     CU(cudaEventRecord(ctx->evc0[par], ctx->copy_stream));
     CU(cudaMemcpyAsync(ctx->pin2[par], ctx->out2[par].p, tot, cudaMemcpyDeviceToHost, ctx->copy_stream));
@@ -2985,13 +3091,13 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     pend_par[pend_n++] = par;
     return TN93G_OK;
   };
+  // Band bi + 1's kernels are queued before band bi is finished, so the device computes while the host takes band
+  // bi's statistics; texts reach the sink when their pinned buffer is needed again, or at the end (at most one band
+  // per parity waits).
   const int nb = (int)bands.size();
   for (int bi = 0; bi <= nb; bi++) {
     if (bi < nb) TRY(enqueue_compute(bi));
-    if (bi >= 1) {
-      TRY(finish(bi - 1));
-      while (pend_n >= 2) TRY(deliver_oldest());
-    }
+    if (bi >= 1) TRY(finish(bi - 1));
   }
   while (pend_n) TRY(deliver_oldest());
   if (hyphy) {

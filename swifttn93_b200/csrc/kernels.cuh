@@ -149,6 +149,8 @@ struct RowArgs {
   char *out;
   double *hy;               // hyphy: [N][N] reported distances (NaN = not reported)
   unsigned long long *err;  // set when a segment's text would exceed its counted length
+  uint32_t *dcode = nullptr;  // [band rows][ncols] printed-distance codes (print_code): the stats kernel writes them,
+                              // the writer formats from them; nullptr: the writer converts the distances itself
 };
 
 }  // namespace tn93

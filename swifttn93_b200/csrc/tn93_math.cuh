@@ -461,11 +461,26 @@ TN_HDI inline uint64_t dec_scale_big(uint64_t m, int e2, int s, int &cmp)
   return big_low64(A);
 }
 
-// the same for 1e-5 <= d < 1e5, where m * 10^s < 2^87 and the binary shift is 26..68 bits
+// 10^s for 0 <= s <= 10
+#if defined(__CUDACC__)
+__constant__ uint64_t kPow10u[11] = {1ull, 10ull, 100ull, 1000ull, 10000ull, 100000ull, 1000000ull, 10000000ull,
+                                     100000000ull, 1000000000ull, 10000000000ull};
+#endif
+TN_HD uint64_t pow10u(int s)
+{
+#if defined(__CUDA_ARCH__)
+  return kPow10u[s];
+#else
+  uint64_t p = 1;
+  for (int i = 0; i < s; i++) p *= 10u;
+  return p;
+#endif
+}
+
+// the same for 1e-5 <= d < 1e5, where m * 10^s < 2^87 and the binary shift is 26..68 bits (0 <= s <= 10)
 TN_HD uint64_t dec_scale_fast(uint64_t m, int e2, int s, int &cmp)
 {
-  uint64_t p10 = 1;
-  for (int i = 0; i < s; i++) p10 *= 10u;
+  const uint64_t p10 = pow10u(s);
   uint64_t hi, lo;
   mul64(m, p10, hi, lo);
   const int u = -(e2);  // value = (hi:lo) * 2^e2, e2 < 0 here
@@ -520,10 +535,8 @@ TN_HD Dec decimal6(double d)
   int cmp = 0;
   for (int guard = 0; guard < 4; guard++) {
     const int s = 5 - X;
-    q = fast ? dec_scale_fast(m, e2, s, cmp) : dec_scale_big(m, e2, s, cmp);
-    if (fast && (s < 1 || s > 10)) {  // the estimate left the fast window: use the exact general path
-      q = dec_scale_big(m, e2, s, cmp);
-    }
+    // the fast path covers 1 <= s <= 10; an estimate that left the window takes the exact general path
+    q = (fast && s >= 1 && s <= 10) ? dec_scale_fast(m, e2, s, cmp) : dec_scale_big(m, e2, s, cmp);
     if (q >= 1000000ull)
       X++;
     else if (q < 100000ull)
@@ -542,26 +555,10 @@ TN_HD Dec decimal6(double d)
   return r;
 }
 
-// printf("%g", d) at the default precision 6; out needs 24 bytes; returns the length
-TN_HD int fmt_g(double d, char *out)
+// the text of printf("%g") for a positive value with decimal digits D (after any sign); returns the length
+TN_HD int fmt_dec(const Dec &D, char *out)
 {
   int n = 0;
-  const uint64_t b = TBITS(d);
-  if (b >> 63) out[n++] = '-';
-  const uint64_t a = b & 0x7FFFFFFFFFFFFFFFull;
-  if (a > 0x7FF0000000000000ull) {
-    out[n++] = 'n'; out[n++] = 'a'; out[n++] = 'n';
-    return n;
-  }
-  if (a == 0x7FF0000000000000ull) {
-    out[n++] = 'i'; out[n++] = 'n'; out[n++] = 'f';
-    return n;
-  }
-  if (a == 0) {
-    out[n++] = '0';
-    return n;
-  }
-  const Dec D = decimal6(TDBL(a));
   char dg[6];
   uint32_t q = D.q;
   for (int i = 5; i >= 0; i--) {
@@ -603,6 +600,43 @@ TN_HD int fmt_g(double d, char *out)
   return n;
 }
 
+// printf("%g", d) at the default precision 6; out needs 24 bytes; returns the length
+TN_HD int fmt_g(double d, char *out)
+{
+  int n = 0;
+  const uint64_t b = TBITS(d);
+  if (b >> 63) out[n++] = '-';
+  const uint64_t a = b & 0x7FFFFFFFFFFFFFFFull;
+  if (a > 0x7FF0000000000000ull) {
+    out[n++] = 'n'; out[n++] = 'a'; out[n++] = 'n';
+    return n;
+  }
+  if (a == 0x7FF0000000000000ull) {
+    out[n++] = 'i'; out[n++] = 'n'; out[n++] = 'f';
+    return n;
+  }
+  if (a == 0) {
+    out[n++] = '0';
+    return n;
+  }
+  return n + fmt_dec(decimal6(TDBL(a)), out + n);
+}
+
+// length of fmt_dec's text for digits D
+TN_HD int dec_len(const Dec &D)
+{
+  uint32_t q = D.q;
+  int nd = 6;
+  while (nd > 1 && q % 10u == 0) {
+    q /= 10u;
+    nd--;
+  }
+  const int X = D.X;
+  if (X < -4 || X >= 6) return nd + (nd > 1 ? 1 : 0) + 2 + ((X <= -100 || X >= 100) ? 3 : 2);
+  if (X >= 0) return nd > X + 1 ? nd + 1 : X + 1;
+  return 2 + (-X - 1) + nd;
+}
+
 // length of printf("%g", d) without building the text (the same rules as fmt_g)
 TN_HD int fmt_g_len(double d)
 {
@@ -611,17 +645,7 @@ TN_HD int fmt_g_len(double d)
   const uint64_t a = b & 0x7FFFFFFFFFFFFFFFull;
   if (a >= 0x7FF0000000000000ull) return neg + 3;  // nan, inf
   if (a == 0) return neg + 1;
-  const Dec D = decimal6(TDBL(a));
-  uint32_t q = D.q;
-  int nd = 6;
-  while (nd > 1 && q % 10u == 0) {
-    q /= 10u;
-    nd--;
-  }
-  const int X = D.X;
-  if (X < -4 || X >= 6) return neg + nd + (nd > 1 ? 1 : 0) + 2 + ((X <= -100 || X >= 100) ? 3 : 2);
-  if (X >= 0) return neg + (nd > X + 1 ? nd + 1 : X + 1);
-  return neg + 2 + (-X - 1) + nd;
+  return neg + dec_len(decimal6(TDBL(a)));
 }
 
 // decimal digits of a non-negative integer below 10^18; returns the length

@@ -106,3 +106,21 @@ def test_tc_equals_popc_wide_alignment_int32_aggregates():
         got[path] = [(body, summ.json(n)) for body, summ in eng.batch_run([aln], [o])]
     assert got["tc"] == got["popc"]
     eng.close()
+
+
+@pytest.mark.parametrize("mode", ["resolve", "gapmm", "average"])
+def test_split_pair_stage_matches_oracle(engine_cli, oracle_bin, tmp_path, mode):
+    """The split pair stage (event kernel, then the formula kernel over the pairs' records; TN93G_PAIR_SPLIT=1)
+    prints the oracle's bytes, including an alignment past 2,047 columns, whose records are 32 bytes."""
+    from swifttn93_b200 import synth
+    from tests.conftest import run_tn93
+
+    for n, L in ((300, 1300), (160, 2500)):
+        names, codes = synth.plain_small(seed=3, n=n, L=L)
+        inp = tmp_path / f"s{n}.fa"
+        inp.write_bytes(synth.to_fasta(names, codes))
+        flags = ["-t", "0.5", "-a", mode, "-g", "0.05", "-l", "100"]
+        rg, fg, sg, eg = run_tn93(engine_cli, flags, inp, tmp_path, extra_env={"TN93G_PAIR_SPLIT": "1"})
+        ro, fo, so, _ = run_tn93(oracle_bin, flags, inp, tmp_path)
+        assert ro == 0 and rg == 0, eg[-300:]
+        assert fg == fo and sg == so, (mode, n, L)
