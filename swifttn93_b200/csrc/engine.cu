@@ -115,6 +115,27 @@ __device__ __forceinline__ void pack_body(const PackArgs &a, long bx, long w0, l
 
 __global__ void pack_kernel(PackArgs a) { pack_body(a, blockIdx.x, blockIdx.y, gridDim.y); }
 
+// one thread per sequence: how many of its N-plane words (plane 3 of each word) are nonzero
+__global__ void wcount_kernel(const uint64_t *planes, long N, long W, int NP, long Npad, uint32_t *wcount)
+{
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  uint32_t n = 0;
+  for (long w = 0; w < W; w++) n += planes[((size_t)w * NP + 3) * Npad + i] != 0;
+  wcount[i] = n;
+}
+
+// one thread per sequence: the indices of its nonzero N-plane words, in order, from wl_off[i]
+__global__ void wlist_kernel(const uint64_t *planes, long N, long W, int NP, long Npad, const uint32_t *wl_off,
+                             uint32_t *wl)
+{
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  uint32_t o = wl_off[i];
+  for (long w = 0; w < W; w++)
+    if (planes[((size_t)w * NP + 3) * Npad + i] != 0) wl[o++] = (uint32_t)w;
+}
+
 // one warp per sequence: its sparse events in site order (block bx: 8 sequences)
 __device__ __forceinline__ void events_body(const PackArgs &a, long bx)
 {
@@ -494,6 +515,9 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const unsigned char
   if (i0 >= a.r1 || j0 >= rc.N) return;
   if (!rc.cross && j0 + kTile - 1 <= i0) return;
   const long Np = rc.Npad;
+  // N-plane cross terms from the sequences' nonzero N words (row side and column side), when the clean-site counts
+  // come from the tensor cores and the events are packed (the column accumulator has room); else every word
+  const bool sparse_w = WPLANE && packed && a.tcagg != nullptr && a.wl_off != nullptr;
   // ---- column-side sparse events: lane = tile row, warp-uniform column; skipped where the row is sparse too
   // (packed: the column-side table holds zeros there)
   if (lane < trows) {
@@ -509,6 +533,24 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const unsigned char
         dst[2] = (int)p.w2;
         dst[3] = (int)p.w3;
         dst[4] = (int)p.f;
+        if (sparse_w) {
+          // the column's N sites against the row's clean bases (its share of the N-plane cross terms)
+          int xc = 0, xh = 0, xl = 0, xt = 0;
+          if (j < rc.N)
+            for (uint32_t q = a.wl_off[j]; q < a.wl_off[j + 1]; q++) {
+              const uint64_t *P = a.planes + (size_t)__ldg(a.wl + q) * rc.NP * Np;
+              const uint64_t nj = __ldg(P + 3 * Np + j);
+              const uint64_t hi = __ldg(P + ib), lo = __ldg(P + Np + ib), ci = __ldg(P + 2 * Np + ib);
+              xc += popc(nj & ci);
+              xh += popc(nj & hi);
+              xl += popc(nj & lo);
+              xt += popc(nj & hi & lo);
+            }
+          dst[5] = xc;
+          dst[6] = xh;
+          dst[7] = xl;
+          dst[8] = xt;
+        }
       } else {
         int acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
         if (j < rc.N) {
@@ -542,8 +584,29 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const unsigned char
     if (!__any_sync(0xffffffffu, valid)) continue;
     Counts c = Counts{0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     const bool tc = a.tcagg != nullptr;  // clean-site counts from the tensor-core kernel
+    const int *src = colacc + (int)(i - i0) * kColAccStride + lane * 9;
+    if (sparse_w) {
+      // the row's N sites against the column's clean bases and N sites (warp-uniform word list), then the column's
+      // share from the column phase: each union term of the dense loop below splits into these disjoint parts
+      for (uint32_t q = a.wl_off[i]; q < a.wl_off[i + 1]; q++) {
+        const uint64_t *Pw = a.planes + (size_t)__ldg(a.wl + q) * rc.NP * Np;
+        const uint64_t ni = __ldg(Pw + 3 * Np + i);
+        const uint64_t hj = __ldg(Pw + jj), lj = __ldg(Pw + Np + jj), cj = __ldg(Pw + 2 * Np + jj);
+        const uint64_t nj = __ldg(Pw + 3 * Np + jj);
+        c.nWc += popc(ni & cj);
+        c.nWh += popc(ni & hj);
+        c.nWl += popc(ni & lj);
+        c.nWt += popc(ni & hj & lj);
+        c.nWW += popc(ni & nj);
+        if (GAPMM) c.nGG += popc(__ldg(Pw + 4 * Np + i) & __ldg(Pw + 4 * Np + jj));
+      }
+      c.nWc += src[5];
+      c.nWh += src[6];
+      c.nWl += src[7];
+      c.nWt += src[8];
+    }
     const uint64_t *P = a.planes;
-    for (long w = 0; w < ((tc && !WPLANE) ? 0 : rc.W); w++, P += (size_t)rc.NP * Np) {
+    for (long w = 0; w < ((tc && (!WPLANE || sparse_w)) ? 0 : rc.W); w++, P += (size_t)rc.NP * Np) {
       const uint64_t hj = __ldg(P + jj), lj = __ldg(P + Np + jj), cj = __ldg(P + 2 * Np + jj);
       const uint64_t hi = __ldg(P + i), lo = __ldg(P + Np + i), ci = __ldg(P + 2 * Np + i);
       if (!tc) {
@@ -574,7 +637,6 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const unsigned char
       }
     }
     int acc[9];
-    const int *src = colacc + (int)(i - i0) * kColAccStride + lane * 9;
     const uint32_t e0 = a.ev_off[i], e1 = a.ev_off[i + 1];
     if (packed) {
       PackedAcc p = {(uint32_t)src[0], (uint32_t)src[1], (uint32_t)src[2], (uint32_t)src[3], (uint32_t)src[4]};
@@ -1868,7 +1930,8 @@ struct tn93g_ctx {
   LogTable *d_logt = nullptr;
   Tables *h_tab = nullptr;
   PairTables *h_ptab = nullptr;  // host staging of the pair stage's tables
-  DevBuf seen, nN, varcol, planes, cc, ccT, evcount, evoff, ev, agg, site, dist, dcode, rq, rqn, counters, rbytes, rsum, rw,
+  DevBuf seen, nN, varcol, planes, cc, ccT, evcount, evoff, ev, agg, site, dist, dcode, wcount, wloff, wl, rq, rqn, counters,
+      rbytes, rsum, rw,
       rmax, rlinks, rskip, hist, roff, out, hy;
   void *pinned = nullptr;
   size_t pinned_n = 0;
@@ -2297,7 +2360,7 @@ void tn93g_destroy(tn93g_ctx *ctx)
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   DevBuf *bufs[] = {&ctx->seen, &ctx->nN, &ctx->varcol, &ctx->planes, &ctx->cc, &ctx->ccT, &ctx->evcount,
-                    &ctx->evoff, &ctx->ev, &ctx->agg, &ctx->site, &ctx->dist, &ctx->dcode, &ctx->rq, &ctx->rqn, &ctx->counters,
+                    &ctx->evoff, &ctx->ev, &ctx->agg, &ctx->site, &ctx->dist, &ctx->dcode, &ctx->wcount, &ctx->wloff, &ctx->wl, &ctx->rq, &ctx->rqn, &ctx->counters,
                     &ctx->rbytes, &ctx->rsum, &ctx->rw, &ctx->rmax, &ctx->rlinks, &ctx->rskip, &ctx->hist,
                     &ctx->roff, &ctx->out, &ctx->hy};
   for (DevBuf *b : bufs)
@@ -2561,9 +2624,42 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     CU(cudaGetLastError());
     ctx->launches++;
   }
+  // per sequence, its nonzero N-plane words (the pair kernel's sparse N-plane pass); counted here, listed below
+  bool sparse_w = rc.wplane && W > 0;
+  std::vector<uint32_t> wcnt;
+  if (sparse_w) {
+    TRY(ensure(ctx, ctx->wcount, N * sizeof(uint32_t)));
+    wcount_kernel<<<(unsigned)((N + 255) / 256), 256, 0, st>>>((const uint64_t *)ctx->planes.p, N, W, rc.NP, Npad,
+                                                                (uint32_t *)ctx->wcount.p);
+    CU(cudaGetLastError());
+    ctx->launches++;
+    wcnt.resize(N);
+    CU(cudaMemcpyAsync(wcnt.data(), ctx->wcount.p, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  }
   std::vector<uint32_t> evc(N), evoff(N + 1);
   CU(cudaMemcpyAsync(evc.data(), ctx->evcount.p, N * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
   CU(cudaStreamSynchronize(st));
+  if (sparse_w) {
+    std::vector<uint32_t> woff(N + 1);
+    unsigned long long t = 0;
+    for (long i = 0; i < N; i++) {
+      woff[i] = (uint32_t)t;
+      t += wcnt[i];
+    }
+    sparse_w = t < 0xFFFFFFFFull;  // 32-bit offsets; beyond them every word is visited
+    if (sparse_w) {
+      woff[N] = (uint32_t)t;
+      TRY(ensure(ctx, ctx->wloff, (N + 1) * sizeof(uint32_t)));
+      TRY(ensure(ctx, ctx->wl, std::max<size_t>(t, 1) * sizeof(uint32_t)));
+      CU(cudaMemcpyAsync(ctx->wloff.p, woff.data(), (N + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+      wlist_kernel<<<(unsigned)((N + 255) / 256), 256, 0, st>>>((const uint64_t *)ctx->planes.p, N, W, rc.NP, Npad,
+                                                                 (const uint32_t *)ctx->wloff.p, (uint32_t *)ctx->wl.p);
+      CU(cudaGetLastError());
+      ctx->launches++;
+      // the host copy must outlive the asynchronous upload
+      CU(cudaStreamSynchronize(st));
+    }
+  }
   evoff[0] = 0;
   uint32_t max_ev = 0;
   for (long i = 0; i < N; i++) {
@@ -2624,9 +2720,10 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   }();
   const long target_pairs = (stream_text || rc.resolve_all) ? band_pairs : (1l << 62);
   const long cap_slots = (stream_text || rc.resolve_all) ? (16l << 20) : (64l << 20);
-  // When the text streams to the host, the bands ramp up (1/8, 1/4, 1/2 of the target) and taper at the end
-  // (half of what is left, down to 1/8), so that the first copy starts early and the last one, which nothing
-  // overlaps, is short.
+  // When the text streams to the host, the bands ramp up from 1/16 of the target, 1.4 times larger each (a band's
+  // kernels take about 0.7 of its copy's time, so each band's kernels end before the previous band's copy does and
+  // the copies run back to back), and taper at the end (half of what is left, down to 1/8), so that the first copy
+  // starts early and the last one, which nothing overlaps, is short.
   std::vector<std::pair<long, long>> bands;
   long maxrows = 1;
   long left = 0;
@@ -2634,8 +2731,8 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
   for (long r0 = row_begin; r0 < upper;) {
     long tgt = target_pairs;
     if (stream_text) {
-      const long k = (long)bands.size();
-      if (k < 3) tgt = target_pairs >> (3 - k);
+      const double ramp = std::pow(1.4, (double)bands.size()) / 16.0;
+      if (ramp < 1.0) tgt = std::max<long>(1, (long)((double)target_pairs * ramp));
       if (left < 2 * target_pairs) tgt = std::min(tgt, std::max(target_pairs / 8, left / 2));
     }
     long r = r0, pairs = 0;
@@ -2857,6 +2954,8 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     A.counters = (unsigned long long *)ctx->counters.p;
     A.logt = ctx->d_logt;
     A.ex = ex;
+    A.wl_off = sparse_w ? (const uint32_t *)ctx->wloff.p : nullptr;
+    A.wl = sparse_w ? (const uint32_t *)ctx->wl.p : nullptr;
     // columns: the smallest lower bound of the band's rows onwards
     const long cstart = rc.cross ? n1 : r0 + 1;
     const long cblk0 = (cstart - colbase) / 32;

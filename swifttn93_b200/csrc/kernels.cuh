@@ -96,6 +96,10 @@ struct PairArgs {
   int tc16 = 0;           // the records are uint16 (every final aggregate fits: 32 L < 65536), else int32
   int split = 0;          // tensor-core path only: the pair kernel stops before the formula, which formula_kernel
                           // finishes from the records
+  // The nonzero words of each sequence's N plane (N sites, or N and gap sites under gapmm): sequence s owns
+  // wl[wl_off[s] .. wl_off[s + 1]). With the tensor-core counts and packed events, the pair kernel's N-plane
+  // cross terms visit only these words; nullptr: every word.
+  const uint32_t *wl_off = nullptr, *wl = nullptr;
   long tcncols = 0, tccolbase = 0;  // row stride and first column of the aggregates when they hold a chunk of the
                                     // columns (0: the same as ncols and colbase)
 };
