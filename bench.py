@@ -45,11 +45,16 @@ FLAGS = dict(threshold=1000.0, resolve_fraction=0.05, min_overlap=500, format="c
 WORKLOAD = "hiv_bench 6700x1500, -t 1000 -g 0.05 -l 500 -f csv, -a resolve/average/gapmm (all pairs written)"
 
 
-# ncu figures of the pair stage behind the roofline line (profiles/pair_stage_hiv_bench_n4000.md): one launch
-# of count_tc_kernel and one of pair_kernel over the 7,998,000 pairs of the 4,000-sequence prefix, -a resolve
-PAIR_STAGE_PROFILE = {"file": "profiles/count_tc_kernel_hiv_bench_n4000.md", "pairs": 7998000,
-                      "dram_bytes": 104.5e6 + 167.8e6, "tensor_pipe_active": 0.294,
-                      "pair_kernel_inst_per_pair": 507.1e6 * 32 / 7998000, "pair_kernel_issue_active": 0.524}
+# ncu figures of the pair stage behind the roofline line, 4,000-sequence prefix under -a resolve: DRAM bytes of the
+# four chunks' count_tc_persist_kernel + pair_kernel launches with the caches kept between kernels (7,998,000 pairs;
+# profiles/pair_stage_traffic_hiv_bench_n4000.md), the count kernel's tensor-pipe activity and the pair kernel's
+# instructions and issue activity on one 2,137,824-pair chunk (profiles/count_tc_kernel_hiv_bench_n4000.md,
+# profiles/pair_kernel_hiv_bench_n4000.md)
+PAIR_STAGE_PROFILE = {"file": "profiles/pair_stage_traffic_hiv_bench_n4000.md", "pairs": 7998000,
+                      "dram_bytes": 25.2e6 + 149.7e6, "tensor_pipe_active": 0.393,
+                      "pair_kernel_inst_per_pair": 123711806 * 32 / 2137824, "pair_kernel_issue_active": 0.502,
+                      "files": ["profiles/pair_stage_traffic_hiv_bench_n4000.md",
+                                "profiles/count_tc_kernel_hiv_bench_n4000.md", "profiles/pair_kernel_hiv_bench_n4000.md"]}
 
 
 def peaks():
@@ -597,7 +602,7 @@ def main():
             "pair_kernel": {"ms_per_launch": {m: pair_ms[m] - count_ms[m] for m in MODES}, "bound": "issue",
                             "instructions_per_pair": PAIR_STAGE_PROFILE["pair_kernel_inst_per_pair"],
                             "issue_active": PAIR_STAGE_PROFILE["pair_kernel_issue_active"]},
-            "profile": PAIR_STAGE_PROFILE["file"]}
+            "profile": PAIR_STAGE_PROFILE["files"]}
 
     line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",

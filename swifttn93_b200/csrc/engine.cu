@@ -474,6 +474,19 @@ __device__ __forceinline__ void add_packed(PackedAcc &p, const uint32_t (*tab)[4
   p.f |= flags[k];
 }
 
+// Drops from L2 the tensor-core records of one tile row once every lane of the warp has read its own (all 32 lanes
+// call it): the 128-byte lines wholly inside the tile row's records [rec0, rec0 + nrec) (nrec <= 32: the tile's
+// columns that lie in this row of the record array) are invalidated without being written back
+// (discard.global.L2), so records that the count kernel left in L2 never travel to DRAM. A line that straddles
+// either edge also holds records of another tile or row and is kept. Each record is read once, by this warp.
+__device__ __forceinline__ void discard_records(const void *base, size_t rec0, long nrec, int rec_bytes, int lane)
+{
+  __syncwarp();
+  const uintptr_t lo = (uintptr_t)base + rec0 * (uintptr_t)rec_bytes, hi = lo + (uintptr_t)nrec * rec_bytes;
+  const uintptr_t line = ((lo + 127) & ~(uintptr_t)127) + (uintptr_t)lane * 128;
+  if (line + 128 <= hi) asm volatile("discard.global.L2 [%0], 128;" ::"l"(line) : "memory");
+}
+
 // Adds the packed table entries of the events [e0, e1) of one sequence against the partner at column p of the
 // position-major code matrix. Four events per step: their words and partner codes are loaded before any sum, so
 // that four partner-code loads (mostly from L2) are in flight at once.
@@ -687,6 +700,10 @@ __device__ __forceinline__ void pair_tile(const PairArgs &a, const unsigned char
         cl[5] = (int)g1.y;
         cl[6] = (int)g1.z;
       }
+      // the records are read once; the split form's formula kernel reads them again
+      if (!SPLIT)
+        discard_records(a.tcagg, (size_t)(i - a.r0) * tn + (size_t)(j0 - tb), min((long)kTile, tb + tn - j0),
+                        a.tc16 ? 16 : 32, lane);
     } else {
       const int nfT = c.T1 + c.T2, nfC = c.Y1 + c.Y2 - nfT, nfG = c.L1 + c.L2 - nfT;
       cl[0] = c.T;
