@@ -285,13 +285,17 @@ TN_HD Dist tn93_distance(const LogTable &T, const double nf[4], double diag, dou
   D.lo = D.hi = D.d;
   D.amb = a.amb + c.amb + t.amb;
   if (D.amb) {
-    // every combination of candidates (the distance is monotone in each logarithm, so the corners bound it)
-    for (int m = 1; m < 8; m++) {
-      const double la = (m & 1) ? a.alt : a.y, lc = (m & 2) ? c.alt : c.y, lt = (m & 4) ? t.alt : t.y;
-      const double v = tn93_combine(P, la, lc, lt);
-      D.lo = v < D.lo ? v : D.lo;
-      D.hi = v > D.hi ? v : D.hi;
-    }
+    // The range over every combination of candidates. tn93_combine is monotone in each logarithm (IEEE products and
+    // differences round monotonically): non-increasing in la, lc, lt when K1, K2, K3 >= 0 (always under K2P, whose
+    // coefficients are -1/2 and -1/4), non-decreasing when negative. So the smallest distance is the combination
+    // that takes, per logarithm, the larger candidate where its coefficient is >= 0 and the smaller elsewhere, and
+    // the largest the opposite one: the same two values the eight corners would give.
+    const bool da = P.k2p || P.K1 >= 0, dc = P.k2p || P.K2 >= 0, dt = P.k2p || P.K3 >= 0;
+    const double a_hi = a.alt > a.y ? a.alt : a.y, a_lo = a.alt > a.y ? a.y : a.alt;
+    const double c_hi = c.alt > c.y ? c.alt : c.y, c_lo = c.alt > c.y ? c.y : c.alt;
+    const double t_hi = t.alt > t.y ? t.alt : t.y, t_lo = t.alt > t.y ? t.y : t.alt;
+    D.lo = tn93_combine(P, da ? a_hi : a_lo, dc ? c_hi : c_lo, dt ? t_hi : t_lo);
+    D.hi = tn93_combine(P, da ? a_lo : a_hi, dc ? c_lo : c_hi, dt ? t_lo : t_hi);
   }
   return D;
 }

@@ -133,6 +133,26 @@ int main(int argc, char **argv)
     d_amb += D.amb != 0;
     bool ok = D.amb ? (ref >= D.lo && ref <= D.hi) : (memcmp(&ref, &D.d, 8) == 0);
     ok = ok && memcmp(&ref, &res, 8) == 0;
+    // with every logarithm ambiguous (band 0.5 ulp, candidates 2^20 ulps apart) the distance's range must equal the
+    // smallest and largest of the eight combinations of candidates
+    if (P.nlog) {
+      const Dist W = tn93_distance(T, nf, diag, agv, ctv, 0.5, 1048576.0);
+      const LogR la = tlog(T, P.arg[0], 0.5, 1048576.0), lc = tlog(T, P.arg[1], 0.5, 1048576.0);
+      LogR lt;
+      lt.y = lt.alt = 0.0;
+      lt.amb = 0;
+      if (P.nlog == 3) lt = tlog(T, P.arg[2], 0.5, 1048576.0);
+      double lo = 1e300, hi = -1e300;
+      for (int m = 0; m < 8; m++) {
+        const double v = tn93_combine(P, (m & 1) ? la.alt : la.y, (m & 2) ? lc.alt : lc.y, (m & 4) ? lt.alt : lt.y);
+        lo = v < lo ? v : lo;
+        hi = v > hi ? v : hi;
+      }
+      if (memcmp(&lo, &W.lo, 8) != 0 || memcmp(&hi, &W.hi, 8) != 0) {
+        if (d_bad < 5) fprintf(stderr, "corner mismatch: [%a,%a] want [%a,%a]\n", W.lo, W.hi, lo, hi);
+        ok = false;
+      }
+    }
     if (!ok) {
       if (d_bad < 5) fprintf(stderr, "dist mismatch: got %a [%a,%a] amb %d want %a\n", D.d, D.lo, D.hi, D.amb, ref);
       d_bad++;
