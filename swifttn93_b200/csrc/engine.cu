@@ -1347,21 +1347,33 @@ __device__ __forceinline__ void sum_rows(const RowArgs &a, long bx)
     // waits for another); skipped pairs and columns past the end add +0.0, which leaves a non-negative sum
     // unchanged. The weights are integers: their double sum is exact, in any order, while the total stays below
     // 2^53, so they are added as integers (and re-added one by one in the rare case the total is larger).
+    // The next chunk's distance and count are loaded before this chunk's chain runs, so the loads overlap it.
     unsigned long long wsum = 0;
+    double raw = 0.;
+    long cj = 0;
+    if (lb + lane < cend) {
+      raw = drow[lb + lane];
+      cj = a.counts[lb + lane];
+    }
     for (long j0 = lb; j0 < cend; j0 += 32) {
-      const long j = j0 + lane;
+      const long j = j0 + lane, jn = j + 32;
+      double raw_n = 0.;
+      long cj_n = 0;
+      if (jn < cend) {
+        raw_n = drow[jn];
+        cj_n = a.counts[jn];
+      }
       double term = 0.;
-      if (j < cend) {
-        const double raw = drow[j];
-        if ((uint64_t)__double_as_longlong(raw) != kSkipBits) {
-          const double t = raw <= 0. ? 0. : raw;
-          const long w = cnt_i * a.counts[j];
-          term = __dmul_rn(t, (double)w);
-          wsum += (unsigned long long)w;
-        }
+      if (j < cend && (uint64_t)__double_as_longlong(raw) != kSkipBits) {
+        const double t = raw <= 0. ? 0. : raw;
+        const long w = cnt_i * cj;
+        term = __dmul_rn(t, (double)w);
+        wsum += (unsigned long long)w;
       }
 #pragma unroll
       for (int l = 0; l < 32; l++) s0 = __dadd_rn(s0, __shfl_sync(0xffffffffu, term, l));
+      raw = raw_n;
+      cj = cj_n;
     }
     for (int o = 16; o; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
     const unsigned long long svs = (!rc.cross && cnt_i > 1) ? (unsigned long long)(cnt_i * (cnt_i - 1l)) >> 1 : 0;
