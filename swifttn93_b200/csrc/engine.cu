@@ -1318,7 +1318,10 @@ __device__ __forceinline__ void stats_rows(const RowArgs &a, long bx, int sg)
     if (sh[t]) atomicAdd(&a.hist[t], sh[t]);
 }
 
-__global__ void __launch_bounds__(256) stats_kernel(RowArgs a) { stats_rows(a, blockIdx.x, blockIdx.y); }
+// Resident blocks per SM for the stats kernel 6 (40 registers) and the write kernel 4 (64): more warps hide their load
+// latency better than fewer spills would (same box, per 22.4 M pairs: stats + sums 0.80 ms with 3 blocks, 0.76 with
+// 4, 0.72 with 6; write 0.78 ms with 3, 0.68 with 4, 0.91 with 6; 2 blocks without spills were slower still)
+__global__ void __launch_bounds__(256, 6) stats_kernel(RowArgs a) { stats_rows(a, blockIdx.x, blockIdx.y); }
 
 
 // one warp per row: tn93's row sums in column order (swifttn93.cpp:2594-2602); lane 0 adds each chunk's terms in
@@ -1619,7 +1622,7 @@ __device__ __forceinline__ void write_rows(const RowArgs &a, long bx, int sg)
   if (S.over && lane == 0) atomicAdd(a.err, 1ull);
 }
 
-__global__ void __launch_bounds__(256) write_kernel(RowArgs a) { write_rows(a, blockIdx.x, blockIdx.y); }
+__global__ void __launch_bounds__(256, 4) write_kernel(RowArgs a) { write_rows(a, blockIdx.x, blockIdx.y); }
 
 // Batched row stage: block b of the batch is row block blocks[b].y of alignment blocks[b].x; blockIdx.y is the
 // segment (blocks past an alignment's segment count exit).
@@ -1824,9 +1827,6 @@ cudaError_t launch_pair_t(const PairArgs &A, dim3 g, cudaStream_t st)
   return cudaGetLastError();
 }
 
-// Resident blocks per SM: 3 (80 registers a thread) when the clean-site counts come from the tensor cores, 2 (128)
-// with the popcount loop, which needs the registers (measured: 3 is 11% faster on the tensor-core path, and slower
-// with the popcount loop). TN93G_PAIR_BLOCKS=2|3 overrides.
 // Whether the tensor-core path splits the pair stage into the event kernel and formula_kernel. One fused kernel
 // overlaps the formula with the event sums and is the faster form on the 6,700 x 1,500 HIV benchmark set in every
 // mode once the event loads are batched (fused 3.31 / 5.44 ms vs split 3.62 / 6.13 ms per resolve / gapmm pair
@@ -1840,11 +1840,15 @@ int pair_split(const RunConsts &)
   return v;
 }
 
+// Resident blocks per SM with the tensor-core counts: 4 (64 registers a thread) when the N plane is off, 3 (80) when
+// it is on (6,700 x 1,500 benchmark set, same box: resolve 3.18 ms with 4 vs 3.25 ms with 3 per pair stage, gapmm
+// 3.82 ms with 3 vs 3.89 ms with 4; 2 blocks, 128 registers without spills, 3.60 ms under resolve); 2 with the
+// popcount loop, which needs the registers. TN93G_PAIR_BLOCKS=2|3|4 overrides.
 cudaError_t launch_pair(const PairArgs &A, long ncolblocks, long nrows, cudaStream_t st)
 {
   static const int forced = [] {
     const char *e = getenv("TN93G_PAIR_BLOCKS");
-    return e ? (atoi(e) == 3 ? 3 : 2) : 0;
+    return e ? (atoi(e) == 4 ? 4 : atoi(e) == 3 ? 3 : 2) : 0;
   }();
   dim3 g((unsigned)ncolblocks, (unsigned)((nrows + kTile - 1) / kTile));
   if (A.split && A.tcagg) {
@@ -1871,7 +1875,8 @@ cudaError_t launch_pair(const PairArgs &A, long ncolblocks, long nrows, cudaStre
     }
     return cudaGetLastError();
   }
-  const int minb = forced ? forced : (A.tcagg ? 3 : 2);
+  const int minb = forced ? forced : (A.tcagg ? (A.rc.wplane ? 3 : 4) : 2);
+  if (minb == 4) return launch_pair_t<4, false>(A, g, st);
   return minb == 3 ? launch_pair_t<3, false>(A, g, st) : launch_pair_t<2, false>(A, g, st);
 }
 
