@@ -1943,7 +1943,12 @@ struct DevBuf {
 
 constexpr int kBatchBufs = 56;
 constexpr int kMaxTcChunks = 48;         // row chunks of a band on the tensor-core count path
-constexpr long kTcChunkPairs = 2l << 20;  // pairs per chunk: 32 MB of 16-byte records, L2-resident
+// Pairs per chunk of the tensor-core path (count kernel, then pair kernel): 16 M pairs, 256 MB of 16-byte records.
+// Larger chunks amortise the persistent count kernel's pipeline fill and drain and the pair kernel's last wave
+// (6,700 x 1,500 benchmark set, resolve pair stage per 22.4 M pairs: 3.17 ms with 2 M-pair chunks, 2.94 with 4 M,
+// 2.77 with 8 M, 2.71 with 16 M, 2.67 with one chunk); the records then travel through HBM, which the pair stage
+// leaves almost idle. TN93G_TC_CHUNK_PAIRS overrides.
+constexpr long kTcChunkPairs = 16l << 20;
 
 struct tn93g_set {
   long N = 0, L = 0;
@@ -2802,7 +2807,11 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
       const long r0 = bands[b].first, r1 = bands[b].second;
       long bp = 0;
       for (long r = r0; r < r1; r++) bp += rc.cross ? ncols : (N - r - 1);
-      const long target = std::max(kTcChunkPairs, (bp + kMaxTcChunks - 2) / (kMaxTcChunks - 1));
+      static const long chunk_pairs = [] {
+        const char *e = getenv("TN93G_TC_CHUNK_PAIRS");  // tuning knob: pairs per count/pair chunk
+        return e && atol(e) > 0 ? atol(e) : kTcChunkPairs;
+      }();
+      const long target = std::max(chunk_pairs, (bp + kMaxTcChunks - 2) / (kMaxTcChunks - 1));
       for (long c0 = r0; c0 < r1;) {
         long c1 = c0, pairs = 0;
         while (c1 < r1 && (c1 == c0 || pairs < target)) {
@@ -2995,8 +3004,8 @@ static int run_impl(tn93g_ctx *ctx, const tn93g_set *set, long n1, const tn93g_o
     const long cblk0 = (cstart - colbase) / 32;
     const long cblks = (ncols + 31) / 32 - cblk0;
     if (use_tc && cblks > 0) {
-      // Clean-site aggregates on the tensor cores, then the pair kernel, chunk by chunk of rows: a chunk's records
-      // (about kTcChunkPairs pairs, 32 MB) are still in L2 when the pair kernel reads them.
+      // Clean-site aggregates on the tensor cores, then the pair kernel, chunk by chunk of rows (about kTcChunkPairs
+      // pairs each); the pair kernel reads each record once and drops its cache line.
       const std::vector<std::pair<long, long>> &chunks = band_chunks[bi];
       for (size_t q = 0; q < chunks.size(); q++) {
         const long c0 = chunks[q].first, c1 = chunks[q].second;

@@ -124,3 +124,20 @@ def test_split_pair_stage_matches_oracle(engine_cli, oracle_bin, tmp_path, mode)
         ro, fo, so, _ = run_tn93(oracle_bin, flags, inp, tmp_path)
         assert ro == 0 and rg == 0, eg[-300:]
         assert fg == fo and sg == so, (mode, n, L)
+
+
+@pytest.mark.parametrize("mode", ["resolve", "gapmm"])
+def test_many_row_chunks_match_oracle(engine_cli, oracle_bin, tmp_path, mode):
+    """Bands split into many count/pair chunks (TN93G_TC_CHUNK_PAIRS=40,000; the default chunk holds 16 M pairs,
+    more than most bands): chunk edges on the 32-row grid, records reused chunk after chunk."""
+    from swifttn93_b200 import synth
+    from tests.conftest import run_tn93
+
+    names, codes = synth.plain_small(seed=4, n=900, L=1100)
+    inp = tmp_path / "c.fa"
+    inp.write_bytes(synth.to_fasta(names, codes))
+    flags = ["-t", "0.3", "-a", mode, "-g", "0.05", "-l", "100"]
+    rg, fg, sg, eg = run_tn93(engine_cli, flags, inp, tmp_path, extra_env={"TN93G_TC_CHUNK_PAIRS": "40000"})
+    ro, fo, so, _ = run_tn93(oracle_bin, flags, inp, tmp_path)
+    assert ro == 0 and rg == 0, eg[-300:]
+    assert fg == fo and sg == so
