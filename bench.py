@@ -45,14 +45,13 @@ FLAGS = dict(threshold=1000.0, resolve_fraction=0.05, min_overlap=500, format="c
 WORKLOAD = "hiv_bench 6700x1500, -t 1000 -g 0.05 -l 500 -f csv, -a resolve/average/gapmm (all pairs written)"
 
 
-# ncu figures of the pair stage behind the roofline line, 4,000-sequence prefix under -a resolve: DRAM bytes of the
-# four chunks' count_tc_persist_kernel + pair_kernel launches with the caches kept between kernels (7,998,000 pairs;
-# profiles/pair_stage_traffic_hiv_bench_n4000.md), the count kernel's tensor-pipe activity and the pair kernel's
-# instructions and issue activity on one 2,137,824-pair chunk (profiles/count_tc_kernel_hiv_bench_n4000.md,
-# profiles/pair_kernel_hiv_bench_n4000.md)
-PAIR_STAGE_PROFILE = {"file": "profiles/pair_stage_traffic_hiv_bench_n4000.md", "pairs": 7998000,
-                      "dram_bytes": 25.2e6 + 149.7e6, "tensor_pipe_active": 0.393,
-                      "pair_kernel_inst_per_pair": 123711806 * 32 / 2137824, "pair_kernel_issue_active": 0.502,
+# ncu figures of the pair stage behind the roofline line, 4,000-sequence prefix under -a resolve (one 16 M-pair chunk
+# holds all 7,998,000 pairs): DRAM bytes of its count_tc_persist_kernel + pair_kernel launches with the caches kept
+# between kernels (profiles/pair_stage_traffic_hiv_bench_n4000.md), the count kernel's tensor-pipe activity
+# (profiles/count_tc_kernel_hiv_bench_n4000.md) and the pair kernel's instructions and issue activity
+# (profiles/pair_kernel_hiv_bench_n4000.md)
+PAIR_STAGE_PROFILE = {"pairs": 7998000, "dram_bytes": 400.36e6, "tensor_pipe_active": 0.417,
+                      "pair_kernel_inst_per_pair": 467694944 * 32 / 7998000, "pair_kernel_issue_active": 0.555,
                       "files": ["profiles/pair_stage_traffic_hiv_bench_n4000.md",
                                 "profiles/count_tc_kernel_hiv_bench_n4000.md", "profiles/pair_kernel_hiv_bench_n4000.md"]}
 
