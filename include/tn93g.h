@@ -196,6 +196,16 @@ int tn93g_read_fasta(const char *bytes, size_t nbytes, long expect_len, char cou
                      char *msg, size_t msg_cap);
 void tn93g_alignment_free(tn93g_alignment *a);
 
+/* FASTA ingest on the device: the work of tn93g_read_fasta followed by tn93g_upload, with the per-byte work on the
+ * GPU. The host finds the records (names, and the byte range of each sequence up to the next '>' or '#') with
+ * vectorised byte searches; the file's bytes go to the device once, where one kernel counts each sequence's letters
+ * and another maps and compresses them, in file order, into the new set's codes. The same acceptance rules, checks
+ * and messages as tn93g_read_fasta (TN93G_EFASTA, with the message in msg); expect_len > 0 requires that length.
+ * On success *out is a set as tn93g_upload makes it, of *n_out sequences of *L_out columns.
+ * Replaces: the byte map and compression of the FASTA reader, swifttn93.cpp:259-406 (345-369 in AVX-512). */
+int tn93g_upload_fasta(tn93g_ctx *ctx, tn93g_set **out, const char *bytes, size_t nbytes, long expect_len,
+                       char counts_sep, long *n_out, long *L_out, char *msg, size_t msg_cap);
+
 /* ---- the -s mode as a service: a resident reference and batches of queries ----
  * A server keeps one reference alignment packed on the device and runs batches of query alignments against it.
  * Each query's result is exactly the distance file body and summary of `tn93 -s QUERY.fa REF.fa` with the

@@ -33,7 +33,7 @@ EXPORTS = ("tn93g_create", "tn93g_destroy", "tn93g_strerror", "tn93g_last_cuda_e
            "tn93g_alignment_free", "tn93g_server_create", "tn93g_server_batch", "tn93g_server_destroy",
            "tn93g_summary_json", "tn93g_run_rows", "tn93g_batch_run", "tn93g_set_count_path",
            "tn93g_summary_certified", "tn93g_set_log_band", "tn93g_set_exact_sums", "tn93g_set_wait_limit",
-           "tn93g_inject_fault", "tn93g_selftest_division")
+           "tn93g_inject_fault", "tn93g_selftest_division", "tn93g_upload_fasta")
 
 # error codes of include/tn93g.h used by the binding
 EUNDECIDED = -10
@@ -118,6 +118,8 @@ def load_library(path: Path | str = LIB_PATH):
     lib.tn93g_set_wait_limit.argtypes = [C.c_void_p, C.c_double]
     lib.tn93g_inject_fault.argtypes = [C.c_void_p, C.c_int]
     lib.tn93g_selftest_division.argtypes = [C.c_void_p, C.c_long, C.c_ulonglong, C.POINTER(C.c_long)]
+    lib.tn93g_upload_fasta.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t, C.c_long, C.c_char,
+                                       C.POINTER(C.c_long), C.POINTER(C.c_long), C.c_char_p, C.c_size_t]
     _lib = lib
     return lib
 
@@ -304,6 +306,19 @@ class Engine:
         self._check(self.lib.tn93g_upload(self.ctx, C.byref(s), codes.ctypes.data, N, L, cnt.ctypes.data, blob,
                                           off.ctypes.data, ln.ctypes.data))
         return DeviceSet(s, N, L)
+
+    def upload_fasta(self, data: bytes, expect_len: int = 0, counts_sep: str = ":") -> DeviceSet:
+        """tn93g_upload_fasta: a FASTA file's bytes read into a set on the device (the byte map and compression run
+        on the GPU), with tn93g_read_fasta's rules and messages (FastaError)."""
+        s = C.c_void_p()
+        n, L = C.c_long(), C.c_long()
+        msg = C.create_string_buffer(512)
+        rc = self.lib.tn93g_upload_fasta(self.ctx, C.byref(s), data, len(data), int(expect_len),
+                                         counts_sep.encode()[:1], C.byref(n), C.byref(L), msg, 512)
+        if rc == -9:
+            raise FastaError(msg.value.decode(errors="replace"))
+        self._check(rc)
+        return DeviceSet(s, n.value, L.value)
 
     def free(self, s: DeviceSet):
         self.lib.tn93g_free_set(self.ctx, s.handle)

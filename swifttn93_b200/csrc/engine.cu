@@ -1970,7 +1970,7 @@ struct tn93g_ctx {
   Tables *h_tab = nullptr;
   PairTables *h_ptab = nullptr;  // host staging of the pair stage's tables
   DevBuf seen, nN, varcol, planes, cc, ccT, evcount, evoff, ev, agg, site, dist, dcode, wcount, wloff, wl, rq, rqn, counters,
-      rbytes, rsum, rw,
+      rbytes, rsum, rw, fraw, fspan, flen, fcode,
       rmax, rlinks, rskip, hist, roff, out, hy;
   void *pinned = nullptr;
   size_t pinned_n = 0;
@@ -2399,7 +2399,7 @@ void tn93g_destroy(tn93g_ctx *ctx)
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   DevBuf *bufs[] = {&ctx->seen, &ctx->nN, &ctx->varcol, &ctx->planes, &ctx->cc, &ctx->ccT, &ctx->evcount,
-                    &ctx->evoff, &ctx->ev, &ctx->agg, &ctx->site, &ctx->dist, &ctx->dcode, &ctx->wcount, &ctx->wloff, &ctx->wl, &ctx->rq, &ctx->rqn, &ctx->counters,
+                    &ctx->evoff, &ctx->ev, &ctx->agg, &ctx->site, &ctx->dist, &ctx->dcode, &ctx->wcount, &ctx->wloff, &ctx->wl, &ctx->fraw, &ctx->fspan, &ctx->flen, &ctx->fcode, &ctx->rq, &ctx->rqn, &ctx->counters,
                     &ctx->rbytes, &ctx->rsum, &ctx->rw, &ctx->rmax, &ctx->rlinks, &ctx->rskip, &ctx->hist,
                     &ctx->roff, &ctx->out, &ctx->hy};
   for (DevBuf *b : bufs)
@@ -2434,8 +2434,18 @@ void tn93g_destroy(tn93g_ctx *ctx)
   delete ctx;
 }
 
+// A new set from codes (host memory, or device memory when codes_kind says so), copy numbers and names (host).
+static int upload_set(tn93g_ctx *ctx, tn93g_set **out, const uint8_t *codes, cudaMemcpyKind codes_kind, long N, long L,
+                      const long *copy_counts, const char *names, const size_t *name_off, const long *name_len);
+
 int tn93g_upload(tn93g_ctx *ctx, tn93g_set **out, const uint8_t *codes, long N, long L, const long *copy_counts,
                  const char *names, const size_t *name_off, const long *name_len)
+{
+  return upload_set(ctx, out, codes, cudaMemcpyHostToDevice, N, L, copy_counts, names, name_off, name_len);
+}
+
+static int upload_set(tn93g_ctx *ctx, tn93g_set **out, const uint8_t *codes, cudaMemcpyKind codes_kind, long N, long L,
+                      const long *copy_counts, const char *names, const size_t *name_off, const long *name_len)
 {
   if (!ctx || !out || !codes || N <= 0 || L <= 0 || !copy_counts || !names || !name_off || !name_len)
     return TN93G_EINVAL;
@@ -2478,8 +2488,7 @@ int tn93g_upload(tn93g_ctx *ctx, tn93g_set **out, const uint8_t *codes, long N, 
   if ((e = take((void **)&s->d_names, nbytes + 1, 2)) != cudaSuccess) return fail(e);
   if ((e = take((void **)&s->d_name_off, N * sizeof(uint64_t), 3)) != cudaSuccess) return fail(e);
   if ((e = take((void **)&s->d_name_len, N * sizeof(int32_t), 4)) != cudaSuccess) return fail(e);
-  if ((e = cudaMemcpyAsync(s->d_codes, codes, (size_t)N * L, cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
-    return fail(e);
+  if ((e = cudaMemcpyAsync(s->d_codes, codes, (size_t)N * L, codes_kind, ctx->stream)) != cudaSuccess) return fail(e);
   if ((e = cudaMemcpyAsync(s->d_counts, copy_counts, N * sizeof(long), cudaMemcpyHostToDevice, ctx->stream)) !=
       cudaSuccess)
     return fail(e);
@@ -2493,6 +2502,200 @@ int tn93g_upload(tn93g_ctx *ctx, tn93g_set **out, const uint8_t *codes, long N, 
     return fail(e);
   if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return fail(e);
   *out = s;
+  return TN93G_OK;
+}
+
+//------------------------------------------------------------------------------------------------ FASTA on device
+// The byte map of tn93's reader: the index of a byte in "ACGTURYSWKMBDHVN?-" (either case), -1 for any other byte
+struct ByteMap {
+  signed char v[256];
+};
+
+static ByteMap make_byte_map()
+{
+  ByteMap m;
+  static const char kValid[] = "ACGTURYSWKMBDHVN?-";
+  for (int c = 0; c < 256; c++) {
+    m.v[c] = -1;
+    const int u = (c >= 'a' && c <= 'z') ? c - 32 : c;
+    if (!u) continue;
+    const char *f = strchr(kValid, u);
+    if (f) m.v[c] = (signed char)(f - kValid);
+  }
+  return m;
+}
+
+// one warp per record: how many of the bytes in its sequence range [span.x, span.y) of raw are letters of the map
+__global__ void __launch_bounds__(256) fasta_count_kernel(const unsigned char *raw, const ulonglong2 *spans, long m,
+                                                          ByteMap map, long *len)
+{
+  __shared__ signed char sm[256];
+  for (int t = threadIdx.x; t < 256; t += blockDim.x) sm[t] = map.v[t];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const long k = blockIdx.x * (long)kWarps + (threadIdx.x >> 5);
+  if (k >= m) return;
+  const unsigned long long b = spans[k].x, e = spans[k].y;
+  long n = 0;
+  for (unsigned long long p = b + lane; p < e; p += 32) n += sm[raw[p]] >= 0;
+  for (int o = 16; o; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+  if (lane == 0) len[k] = n;
+}
+
+// one warp per record: its sequence letters mapped to codes and compressed, in file order, to codes[k * L ...] (every
+// record has L letters, checked on the host before the launch)
+__global__ void __launch_bounds__(256) fasta_compress_kernel(const unsigned char *raw, const ulonglong2 *spans, long m,
+                                                             ByteMap map, long L, uint8_t *codes)
+{
+  __shared__ signed char sm[256];
+  for (int t = threadIdx.x; t < 256; t += blockDim.x) sm[t] = map.v[t];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const long k = blockIdx.x * (long)kWarps + (threadIdx.x >> 5);
+  if (k >= m) return;
+  const unsigned long long b = spans[k].x, e = spans[k].y;
+  uint8_t *row = codes + (size_t)k * L;
+  long base = 0;
+  for (unsigned long long p0 = b; p0 < e; p0 += 32) {
+    const unsigned long long p = p0 + lane;
+    const int v = p < e ? sm[raw[p]] : -1;
+    const unsigned mask = __ballot_sync(0xffffffffu, v >= 0);
+    if (v >= 0) row[base + __popc(mask & ((1u << lane) - 1u))] = (uint8_t)v;
+    base += __popc(mask);
+  }
+}
+
+// The records of a FASTA file as tn93's reader finds them (swifttn93.cpp:259-406): '>' or '#' opens a record whose
+// name runs to the end of the line, and its sequence is every byte up to the next '>' or '#'. memchr (vectorised in
+// the C library) finds those bytes, so the host does not touch the sequence letters.
+struct FastaRecords {
+  std::vector<char> names;
+  std::vector<size_t> name_off;
+  std::vector<long> name_len, counts;
+  std::vector<ulonglong2> spans;
+  int eof_state = 2;     // the reader's state at the end of the file (2: inside a sequence, the normal end)
+  std::string name_err;  // the record after the last span has an empty name (reported after the spans' lengths)
+};
+
+static void fasta_records(const char *bytes, size_t n, char counts_sep, FastaRecords &R)
+{
+  // the next '>' and '#' at or after the last search start (n: none); still the next ones for any later start that
+  // does not pass them
+  size_t ngt = 0, nhs = 0;
+  bool have = false;
+  auto next_open = [&](size_t i) -> size_t {
+    if (!have || ngt < i) {
+      const void *g = i < n ? memchr(bytes + i, '>', n - i) : nullptr;
+      ngt = g ? (size_t)((const char *)g - bytes) : n;
+    }
+    if (!have || nhs < i) {
+      const void *h = i < n ? memchr(bytes + i, '#', n - i) : nullptr;
+      nhs = h ? (size_t)((const char *)h - bytes) : n;
+    }
+    have = true;
+    return std::min(ngt, nhs);
+  };
+  size_t o = next_open(0);
+  if (o == n) {
+    R.eof_state = 0;
+    return;
+  }
+  size_t i = o + 1;
+  for (;;) {
+    size_t q = i;
+    while (q < n && bytes[q] != '\n' && bytes[q] != '\r') q++;
+    if (q == n) {
+      R.eof_state = 1;
+      return;
+    }
+    const long len = (long)(q - i);
+    if (len <= 0) {
+      R.name_err = "Sequence names must be non-empty.\n";
+      return;
+    }
+    const size_t begin = R.names.size();
+    R.names.insert(R.names.end(), bytes + i, bytes + q);
+    R.names.push_back('\0');
+    unsigned long count = 1;
+    if (len >= 3) {
+      const char *nm = R.names.data() + begin;
+      long k = len - 2;
+      while (k >= 1 && nm[k] != counts_sep) k--;
+      if (k >= 1) count = (unsigned long)(long)(int)strtol(nm + k + 1, nullptr, 10);
+      if (count < 1) count = 1;
+    }
+    R.counts.push_back((long)count);
+    R.name_off.push_back(begin);
+    R.name_len.push_back(len);
+    i = q + 1;
+    o = next_open(i);
+    R.spans.push_back(make_ulonglong2(i, o));
+    if (o == n) {
+      R.eof_state = 2;
+      return;
+    }
+    i = o + 1;
+  }
+}
+
+int tn93g_upload_fasta(tn93g_ctx *ctx, tn93g_set **out, const char *bytes, size_t nbytes, long expect_len,
+                       char counts_sep, long *n_out, long *L_out, char *msg, size_t msg_cap)
+{
+  if (!ctx || !out || (!bytes && nbytes)) return TN93G_EINVAL;
+  *out = nullptr;
+  cudaSetDevice(ctx->device);
+  const cudaStream_t st = ctx->stream;
+  FastaRecords R;
+  fasta_records(bytes, nbytes, counts_sep, R);
+  const long m = (long)R.spans.size();
+  std::vector<long> lens(m);
+  const ByteMap map = make_byte_map();
+  if (m) {
+    TRY(ensure(ctx, ctx->fraw, nbytes));
+    TRY(ensure(ctx, ctx->fspan, m * sizeof(ulonglong2)));
+    TRY(ensure(ctx, ctx->flen, m * sizeof(long)));
+    CU(cudaMemcpyAsync(ctx->fraw.p, bytes, nbytes, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(ctx->fspan.p, R.spans.data(), m * sizeof(ulonglong2), cudaMemcpyHostToDevice, st));
+    fasta_count_kernel<<<(unsigned)((m + kWarps - 1) / kWarps), 256, 0, st>>>(
+        (const unsigned char *)ctx->fraw.p, (const ulonglong2 *)ctx->fspan.p, m, map, (long *)ctx->flen.p);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(lens.data(), ctx->flen.p, m * sizeof(long), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+  }
+  // the reader's checks in its order: each record's length when its sequence closes, then what stopped the scan
+  std::string err;
+  const bool have_len = expect_len > 0;
+  long first_len = have_len ? expect_len : 0;
+  for (long k = 0; k < m && err.empty(); k++) {
+    if (k == 0 && !have_len) {
+      first_len = lens[0];
+      if (first_len <= 0) err = "First sequence length must be positive.\n";
+    } else if (lens[k] != first_len) {
+      err = "All sequences must have the same length (" + std::to_string(first_len) + "), but sequence '" +
+            std::string(R.names.data() + R.name_off[k]) + "' had length " + std::to_string(lens[k]);
+    }
+  }
+  if (err.empty() && !R.name_err.empty()) err = R.name_err;
+  if (err.empty() && R.eof_state != 2) err = "Unexpected end of file: state " + std::to_string(R.eof_state) + "\n";
+  if (!err.empty()) {
+    if (msg && msg_cap) {
+      const size_t k = err.size() < msg_cap ? err.size() : msg_cap - 1;
+      memcpy(msg, err.data(), k);
+      msg[k] = 0;
+    }
+    return TN93G_EFASTA;
+  }
+  if (msg && msg_cap) msg[0] = 0;
+  if (first_len >= (1l << 25)) return TN93G_ETOOBIG;
+  TRY(ensure(ctx, ctx->fcode, (size_t)m * first_len));
+  fasta_compress_kernel<<<(unsigned)((m + kWarps - 1) / kWarps), 256, 0, st>>>(
+      (const unsigned char *)ctx->fraw.p, (const ulonglong2 *)ctx->fspan.p, m, map, first_len, (uint8_t *)ctx->fcode.p);
+  CU(cudaGetLastError());
+  const int rc = upload_set(ctx, out, (const uint8_t *)ctx->fcode.p, cudaMemcpyDeviceToDevice, m, first_len,
+                            R.counts.data(), R.names.data(), R.name_off.data(), R.name_len.data());
+  if (rc != TN93G_OK) return rc;
+  if (n_out) *n_out = m;
+  if (L_out) *L_out = first_len;
   return TN93G_OK;
 }
 
