@@ -205,6 +205,11 @@ void tn93g_alignment_free(tn93g_alignment *a);
  * Replaces: the byte map and compression of the FASTA reader, swifttn93.cpp:259-406 (345-369 in AVX-512). */
 int tn93g_upload_fasta(tn93g_ctx *ctx, tn93g_set **out, const char *bytes, size_t nbytes, long expect_len,
                        char counts_sep, long *n_out, long *L_out, char *msg, size_t msg_cap);
+/* The host half of tn93g_upload_fasta (its record scan and the reader's checks) with the letters counted on the
+ * host: the same result and message as tn93g_upload_fasta without a device, for tests. Replaces: nothing in the
+ * reference. */
+int tn93g_fasta_check(const char *bytes, size_t nbytes, long expect_len, char counts_sep, long *n_out, long *L_out,
+                      char *msg, size_t msg_cap);
 
 /* ---- the -s mode as a service: a resident reference and batches of queries ----
  * A server keeps one reference alignment packed on the device and runs batches of query alignments against it.

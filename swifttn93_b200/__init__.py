@@ -33,7 +33,8 @@ EXPORTS = ("tn93g_create", "tn93g_destroy", "tn93g_strerror", "tn93g_last_cuda_e
            "tn93g_alignment_free", "tn93g_server_create", "tn93g_server_batch", "tn93g_server_destroy",
            "tn93g_summary_json", "tn93g_run_rows", "tn93g_batch_run", "tn93g_set_count_path",
            "tn93g_summary_certified", "tn93g_set_log_band", "tn93g_set_exact_sums", "tn93g_set_wait_limit",
-           "tn93g_inject_fault", "tn93g_selftest_division", "tn93g_upload_fasta")
+           "tn93g_inject_fault", "tn93g_selftest_division", "tn93g_upload_fasta",
+           "tn93g_fasta_check")
 
 # error codes of include/tn93g.h used by the binding
 EUNDECIDED = -10
@@ -120,6 +121,8 @@ def load_library(path: Path | str = LIB_PATH):
     lib.tn93g_selftest_division.argtypes = [C.c_void_p, C.c_long, C.c_ulonglong, C.POINTER(C.c_long)]
     lib.tn93g_upload_fasta.argtypes = [C.c_void_p, C.POINTER(C.c_void_p), C.c_char_p, C.c_size_t, C.c_long, C.c_char,
                                        C.POINTER(C.c_long), C.POINTER(C.c_long), C.c_char_p, C.c_size_t]
+    lib.tn93g_fasta_check.argtypes = [C.c_char_p, C.c_size_t, C.c_long, C.c_char, C.POINTER(C.c_long),
+                                      C.POINTER(C.c_long), C.c_char_p, C.c_size_t]
     _lib = lib
     return lib
 

@@ -2638,6 +2638,61 @@ static void fasta_records(const char *bytes, size_t n, char counts_sep, FastaRec
   }
 }
 
+// The reader's checks in its order, given each record's letter count: each length when its sequence closes, then
+// what stopped the scan. Returns the message (empty when the file is accepted) and the length in *first_len.
+static std::string fasta_check(const FastaRecords &R, const std::vector<long> &lens, long expect_len, long *first_len)
+{
+  std::string err;
+  const long m = (long)R.spans.size();
+  const bool have_len = expect_len > 0;
+  long L = have_len ? expect_len : 0;
+  for (long k = 0; k < m && err.empty(); k++) {
+    if (k == 0 && !have_len) {
+      L = lens[0];
+      if (L <= 0) err = "First sequence length must be positive.\n";
+    } else if (lens[k] != L) {
+      err = "All sequences must have the same length (" + std::to_string(L) + "), but sequence '" +
+            std::string(R.names.data() + R.name_off[k]) + "' had length " + std::to_string(lens[k]);
+    }
+  }
+  if (err.empty() && !R.name_err.empty()) err = R.name_err;
+  if (err.empty() && R.eof_state != 2) err = "Unexpected end of file: state " + std::to_string(R.eof_state) + "\n";
+  *first_len = L;
+  return err;
+}
+
+static void copy_msg(const std::string &err, char *msg, size_t msg_cap)
+{
+  if (!msg || !msg_cap) return;
+  const size_t k = err.size() < msg_cap ? err.size() : msg_cap - 1;
+  memcpy(msg, err.data(), k);
+  msg[k] = 0;
+}
+
+// The device ingest's host half with the letters counted on the host: its record scan and checks, for tests on
+// machines without a GPU. Returns TN93G_OK (with the size in n_out, L_out) or TN93G_EFASTA (message in msg).
+int tn93g_fasta_check(const char *bytes, size_t nbytes, long expect_len, char counts_sep, long *n_out, long *L_out,
+                      char *msg, size_t msg_cap)
+{
+  if (!bytes && nbytes) return TN93G_EINVAL;
+  FastaRecords R;
+  fasta_records(bytes, nbytes, counts_sep, R);
+  const ByteMap map = make_byte_map();
+  std::vector<long> lens(R.spans.size());
+  for (size_t k = 0; k < R.spans.size(); k++) {
+    long c = 0;
+    for (unsigned long long p = R.spans[k].x; p < R.spans[k].y; p++) c += map.v[(unsigned char)bytes[p]] >= 0;
+    lens[k] = c;
+  }
+  long L = 0;
+  const std::string err = fasta_check(R, lens, expect_len, &L);
+  copy_msg(err, msg, msg_cap);
+  if (!err.empty()) return TN93G_EFASTA;
+  if (n_out) *n_out = (long)R.spans.size();
+  if (L_out) *L_out = L;
+  return TN93G_OK;
+}
+
 int tn93g_upload_fasta(tn93g_ctx *ctx, tn93g_set **out, const char *bytes, size_t nbytes, long expect_len,
                        char counts_sep, long *n_out, long *L_out, char *msg, size_t msg_cap)
 {
@@ -2662,30 +2717,10 @@ int tn93g_upload_fasta(tn93g_ctx *ctx, tn93g_set **out, const char *bytes, size_
     CU(cudaMemcpyAsync(lens.data(), ctx->flen.p, m * sizeof(long), cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
   }
-  // the reader's checks in its order: each record's length when its sequence closes, then what stopped the scan
-  std::string err;
-  const bool have_len = expect_len > 0;
-  long first_len = have_len ? expect_len : 0;
-  for (long k = 0; k < m && err.empty(); k++) {
-    if (k == 0 && !have_len) {
-      first_len = lens[0];
-      if (first_len <= 0) err = "First sequence length must be positive.\n";
-    } else if (lens[k] != first_len) {
-      err = "All sequences must have the same length (" + std::to_string(first_len) + "), but sequence '" +
-            std::string(R.names.data() + R.name_off[k]) + "' had length " + std::to_string(lens[k]);
-    }
-  }
-  if (err.empty() && !R.name_err.empty()) err = R.name_err;
-  if (err.empty() && R.eof_state != 2) err = "Unexpected end of file: state " + std::to_string(R.eof_state) + "\n";
-  if (!err.empty()) {
-    if (msg && msg_cap) {
-      const size_t k = err.size() < msg_cap ? err.size() : msg_cap - 1;
-      memcpy(msg, err.data(), k);
-      msg[k] = 0;
-    }
-    return TN93G_EFASTA;
-  }
-  if (msg && msg_cap) msg[0] = 0;
+  long first_len = 0;
+  const std::string err = fasta_check(R, lens, expect_len, &first_len);
+  copy_msg(err, msg, msg_cap);
+  if (!err.empty()) return TN93G_EFASTA;
   if (first_len >= (1l << 25)) return TN93G_ETOOBIG;
   TRY(ensure(ctx, ctx->fcode, (size_t)m * first_len));
   fasta_compress_kernel<<<(unsigned)((m + kWarps - 1) / kWarps), 256, 0, st>>>(

@@ -115,3 +115,51 @@ def test_summary_json_formats_like_printf():
     assert got == want
     got2 = summ.json(30000, 17, True, False).decode()
     assert "\t\"Sequences in first file\" : 30000,\n\t\"Sequences in second file\" : 17,\n" in got2
+
+
+def _check(data, expect_len=0):
+    """tn93g_fasta_check: the device ingest's record scan and checks, letters counted on the host."""
+    import ctypes as C
+
+    from swifttn93_b200 import load_library
+
+    lib = load_library()
+    n, L = C.c_long(), C.c_long()
+    msg = C.create_string_buffer(512)
+    rc = lib.tn93g_fasta_check(data, len(data), int(expect_len), b":", C.byref(n), C.byref(L), msg, 512)
+    return rc, msg.value.decode(errors="replace"), n.value, L.value
+
+
+def _read(data, expect_len=0):
+    from swifttn93_b200 import Fasta, FastaError
+
+    try:
+        f = Fasta(data, expect_len=expect_len)
+        return 0, "", f.n, f.L
+    except FastaError as e:
+        return -9, str(e), 0, 0
+
+
+def test_device_ingest_scan_matches_reader():
+    """The device ingest (tn93g_upload_fasta) finds records with byte searches and applies the reader's checks in
+    its order from per-record letter counts; with the counts taken on the host (tn93g_fasta_check) it must accept
+    and refuse exactly what tn93g_read_fasta does, with the same message and size."""
+    from swifttn93_b200 import build
+
+    build.build_lib()
+    rng = random.Random(7400)
+    accepted = refused = 0
+    for k in range(400):
+        files, _ = cases.fuzz_case(rng)
+        data = files["in"]
+        for expect in (0, 7):
+            got, want = _check(data, expect), _read(data, expect)
+            assert got == want, (k, expect, got, want)
+            accepted += got[0] == 0
+            refused += got[0] != 0
+    extra = [b"", b"ACGT", b">", b">\n", b">a", b">a\nAC\n>\nAC\n", b"#a\nAC\n#b\nAC", b">a\r\nAC\r\n>b\nA>C\n",
+             b">a\nACGT\n>b\nAC\n>c\n", b">a b:3\nAC-?N\n>c:x:2\nnnac\n", b"\n\n>a\nA\nC\n#b\nAC"]
+    for data in extra:
+        for expect in (0, 2, 4):
+            assert _check(data, expect) == _read(data, expect), (data, expect)
+    assert accepted > 50 and refused > 20, (accepted, refused)
